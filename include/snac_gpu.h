@@ -1,0 +1,224 @@
+/*
+ * snac_gpu.h — C ABI of the B200 (sm_100a) implementation of SNAC's explicit
+ * Lagrangian time step (FLAC dynamic relaxation on a structured hex mesh,
+ * each hex split into two overlapping sets of five tetrahedra).
+ *
+ * Plain C: pointers, sizes and integer status codes only.  Every entry point
+ * returns SNAC_GPU_OK (0) or a negative SNAC_GPU_E* code; the message and the
+ * offending element/node id are kept per handle (snac_gpu_last_error /
+ * snac_gpu_error_index).  One handle owns one CUDA stream; a handle is
+ * single-threaded and non-reentrant, like the Snac_Context it stands in for
+ * (Snac/libSnac/src/Tetrahedra.c:30 notes the reference is not thread-safe).
+ *
+ * Conventions (Snac/libSnac/src/Context.c, StGermain HexaEL/BlockGeometry):
+ *   nx, ny, nz     element (hex) counts along I (x), J (y, vertical, gravity
+ *                  acts on -y) and K (z).  Node counts are nx+1, ny+1, nz+1
+ *                  (the reference's meshSizeI/J/K).
+ *   node (i,j,k)   index i + j*(nx+1) + k*(nx+1)*(ny+1)
+ *   element (i,j,k) index i + j*nx + k*nx*ny
+ *   tensors        6 components per tetrahedron in the order
+ *                  xx, yy, zz, xy, xz, yz (upper triangle of the reference's
+ *                  3x3 arrays; the lower triangle is never written there).
+ *   host arrays    element-major: stress[((e*10)+t)*6 + c],
+ *                  plastic_strain[e*10 + t], coord/velocity[n*3 + d].
+ */
+#ifndef SNAC_GPU_H
+#define SNAC_GPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SNAC_GPU_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define SNAC_GPU_OK          0
+#define SNAC_GPU_EINVAL     -1   /* bad descriptor or argument                       */
+#define SNAC_GPU_ENOMEM     -2   /* device or host allocation failed                 */
+#define SNAC_GPU_ECUDA      -3   /* CUDA runtime error                               */
+#define SNAC_GPU_ENAN       -4   /* NaN/Inf in the state (reference: Journal firewall)*/
+#define SNAC_GPU_EVOLUME    -5   /* zero tetrahedron volume (degenerate element)     */
+#define SNAC_GPU_EMATERIAL  -6   /* material index out of range                      */
+#define SNAC_GPU_EPHYSICS   -7   /* reference abort()/assert(): friction angle < 0,
+                                    dt_thermal/dt_mech <= 1, ...                      */
+#define SNAC_GPU_ETIMEDOUT  -8   /* a bounded device-side wait gave up               */
+#define SNAC_GPU_ENOTSUP    -9   /* option the reference has but this build does not  */
+#define SNAC_GPU_ESTATE    -10   /* call out of order (e.g. step before step zero)    */
+#define SNAC_GPU_ENODEV    -11   /* no CUDA device                                   */
+
+/* ---- enumerations (values follow the reference where it has them) ------ */
+/* dtType, Snac/libSnac/src/Context.c:345-391 */
+#define SNAC_DT_CONSTANT 0
+#define SNAC_DT_DYNAMIC  1
+#define SNAC_DT_WAVE     2
+
+/* Material rheology bits, Snac/libSnac/src/Material.h:46-50.  The
+ * "constitutive" field of the descriptor names the ONE constitutive plugin
+ * loaded on Snac_EP_Constitutive (SnacElastic, SnacPlastic, SnacViscoPlastic
+ * or SnacMaxwell), as in the reference configs. */
+#define SNAC_RHEOLOGY_ELASTIC      0x1
+#define SNAC_RHEOLOGY_PLASTIC      0x2
+#define SNAC_RHEOLOGY_MAXWELL      0x4
+#define SNAC_RHEOLOGY_VISCOPLASTIC 0x8
+
+/* Wall ids, StGermain/Discretisation/Utils/src/WallVC.c:49-55 */
+#define SNAC_WALL_BACK   0   /* k == 0        */
+#define SNAC_WALL_LEFT   1   /* i == 0        */
+#define SNAC_WALL_BOTTOM 2   /* j == 0        */
+#define SNAC_WALL_RIGHT  3   /* i == nx       */
+#define SNAC_WALL_TOP    4   /* j == ny       */
+#define SNAC_WALL_FRONT  5   /* k == nz       */
+#define SNAC_WALL_ALL    6   /* every node (AllNodesVC)                          */
+
+#define SNAC_MAX_SEGMENTS 8  /* softening table: nsegments <= 8, 9 break points */
+
+/* One phase, Snac/libSnac/src/Material.h:54-112 and the dictionary keys of
+ * Context.c:826-914.  Every value is taken as given (no float-literal
+ * defaults are applied here; pass what the reference would have read). */
+typedef struct snac_material {
+    double density;          /* phsDensity                    */
+    double alpha, beta;      /* thermal expansion, compressibility */
+    double lambda, mu;
+    int    nsegments;        /* piecewise-linear softening     */
+    int    yield_mohr_coulomb; /* 1 (mohrcoulomb); druckerprager is SNAC_GPU_ENOTSUP */
+    double plstrain[SNAC_MAX_SEGMENTS + 1];
+    double friction_angle[SNAC_MAX_SEGMENTS + 1];   /* degrees */
+    double dilation_angle[SNAC_MAX_SEGMENTS + 1];   /* degrees */
+    double cohesion[SNAC_MAX_SEGMENTS + 1];
+    double ten_off;
+    double vis_min, vis_max, refvisc, refsrate, reftemp;
+    double activation_e;     /* activationE (J/mol)            */
+    double srexponent;
+    double thermal_conduct, heat_capacity;
+} snac_material;
+
+/* One entry of a CompositeVC vcList (WallVC / AllNodesVC).  For velocity
+ * BCs bit d of mask fixes component d to value[d]; for temperature BCs bit 0
+ * fixes T to value[0].  When several entries fix the same component of the
+ * same node the LAST one wins (StGermain/Base/Automation/src/CompositeVC.c:599-611). */
+typedef struct snac_wall_bc {
+    int    wall;
+    int    mask;
+    double value[3];
+} snac_wall_bc;
+
+typedef struct snac_gpu_desc {
+    int    abi_version;              /* SNAC_GPU_ABI_VERSION */
+    int    nx, ny, nz;
+    double min[3], max[3];           /* BlockGeometry extent */
+    const double* node_coords;       /* optional [nn*3]; overrides the block geometry */
+
+    int    dt_type;                  /* SNAC_DT_*                     */
+    double dt;                       /* "timeStep": constant dt, or the initial value */
+    double strain_inert;
+    double gravity;
+    double demf;                     /* FLAC local damping factor     */
+
+    int    constitutive;             /* one SNAC_RHEOLOGY_* bit        */
+    int    temperature;              /* SnacTemperature loaded         */
+    int    compute_thermal_stress;
+    int    hydrostatic_ic;           /* SnacHydroStaticIC loaded       */
+    int    temperature_sweep_ic;     /* _SnacTemperature_Top2BottomSweep as the node IC */
+    double top_temp, bottom_temp;    /* for the sweep IC               */
+
+    int    n_materials;
+    const snac_material* materials;
+    const int*    element_material;  /* [ne] phase id, NULL = 0       */
+    /* Optional per-element multipliers of the phase tables: the reference
+     * expresses these as one phase per element with scaled table values. */
+    const double* element_cohesion_scale;  /* [ne] x cohesion[i]       */
+    const double* element_friction_scale;  /* [ne] x frictionAngle[i]  */
+    const double* element_visc_scale;      /* [ne] x refvisc           */
+
+    int    n_velocity_bcs;
+    const snac_wall_bc* velocity_bcs;
+    int    n_temperature_bcs;
+    const snac_wall_bc* temperature_bcs;
+
+    const double* init_velocity;     /* [nn*3] nodeICs, NULL = 0      */
+    const double* init_temperature;  /* [nn], used when temperature_sweep_ic == 0 */
+    const double* init_stress;       /* [ne*10*6] elementICs, NULL = 0 (hydrostatic_ic adds on top) */
+} snac_gpu_desc;
+
+/* Host-side view of the state for upload / download.  NULL members are
+ * skipped.  Sizes: nn*3, nn*3, ne*10*6, ne*10, ne*10, nn, nn*3, nn. */
+typedef struct snac_state_view {
+    double* coord;
+    double* velocity;
+    double* stress;
+    double* plastic_strain;
+    double* viscosity;
+    double* temperature;
+    double* force;           /* download only: damped nodal force of the last step */
+    double* inertial_mass;   /* download only */
+} snac_state_view;
+
+typedef struct snac_scalars {
+    double dt;               /* dt the NEXT step will use            */
+    double min_length_scale; /* global minimum of |V/A|              */
+    double vmax;             /* max |v| over velocity-BC nodes (floored at 3e-11f) */
+    double speed_of_sound;
+    long long time_step;     /* steps completed after step zero      */
+} snac_scalars;
+
+typedef struct snac_gpu snac_gpu;
+
+/* ---- lifetime ------------------------------------------------------------ */
+/* Builds the device state from the descriptor and applies the initial
+ * conditions in the reference's order: nodeICs, elementICs, velocity BCs
+ * (Context.c:742-774), then the plugin ICs inserted before SnacTimeStepZero
+ * (temperature, plastic / visco-plastic / Maxwell, hydrostatic).
+ * Replaces Snac_Context construction + _Snac_Context_InitialConditions. */
+int  snac_gpu_create(const snac_gpu_desc* desc, snac_gpu** out);
+void snac_gpu_destroy(snac_gpu* h);
+
+/* Snac_Context_TimeStepZero (Context.c:978-1036): element geometry from the
+ * initial coordinates, then Sync (first dt). */
+int  snac_gpu_time_step_zero(snac_gpu* h);
+
+/* nsteps x _AbstractContext_Step (AbstractContext.c:921-941) with the SNAC
+ * hooks: Solve (_Snac_Context_Solve, Context.c:1063-1099) then Sync
+ * (_Snac_Context_Sync, Context.c:1208-1268).  The step loop runs from a CUDA
+ * graph; nothing is copied to the host. */
+int  snac_gpu_step(snac_gpu* h, int nsteps);
+
+/* Loop-level entry points, one per StGermain entry point a plugin replaces
+ * with EntryPoint_Replace (StGermain/Base/Extensibility/src/EntryPoint.c:735):
+ *   Snac_EP_LoopElementsEnergy   (temperature/HeatFlux.c:47-58)
+ *   Snac_EP_LoopNodesEnergy      (temperature/Heat.c:47-62)
+ *   Snac_EP_CalcStresses         (_Snac_Context_CalcStresses, Context.c:1102-1117)
+ *   Snac_EP_LoopNodesMomentum    (_Snac_Context_LoopNodes, Context.c:1120-1154)
+ *   Snac_EP_LoopElementsMomentum (_Snac_Context_LoopElements, Context.c:1156-1184)
+ *   AbstractContext_EP_Sync      (_Snac_Context_Sync, Context.c:1208-1268)
+ * snac_gpu_begin_step advances timeStep and takes dt for the step the way
+ * _AbstractContext_Execute_Hook / _Snac_Context_Dt do (AbstractContext.c:874-890). */
+int  snac_gpu_begin_step(snac_gpu* h);
+int  snac_gpu_loop_elements_energy(snac_gpu* h);
+int  snac_gpu_loop_nodes_energy(snac_gpu* h);
+int  snac_gpu_calc_stresses(snac_gpu* h);
+int  snac_gpu_loop_nodes_momentum(snac_gpu* h);
+int  snac_gpu_loop_elements_momentum(snac_gpu* h);
+int  snac_gpu_sync(snac_gpu* h);
+
+/* ---- state transfer -------------------------------------------------------- */
+int  snac_gpu_upload(snac_gpu* h, const snac_state_view* v);
+int  snac_gpu_download(snac_gpu* h, const snac_state_view* v);
+int  snac_gpu_scalars(snac_gpu* h, snac_scalars* out);
+int  snac_gpu_set_dt(snac_gpu* h, double dt);   /* _Snac_Context_SetDt, Context.c:1047-1053 */
+
+/* ---- errors / introspection ------------------------------------------------ */
+const char* snac_gpu_last_error(const snac_gpu* h);
+long long   snac_gpu_error_index(const snac_gpu* h);   /* element/node id, -1 if none */
+int  snac_gpu_sizes(const snac_gpu* h, long long* n_elements, long long* n_nodes);
+/* Number of kernels this library launched on the handle since creation. */
+long long snac_gpu_launch_count(const snac_gpu* h);
+/* The handle's cudaStream_t, as a void* (for event timing by callers). */
+void* snac_gpu_stream(snac_gpu* h);
+int  snac_gpu_device_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SNAC_GPU_H */

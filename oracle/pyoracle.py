@@ -1,0 +1,180 @@
+"""ctypes front end of the CPU checkers.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg, never by the snac_b200 package.
+
+  Checker("port")       oracle/liboracle.so, the plain-C restatement
+  Checker("reference")  oracle/_ref/libsnacref.so, the reference's own
+                        hot-path sources compiled against oracle/refshim
+Both take the product's descriptor (snac_b200.abi.SnacConfig) and expose the
+same calls, so a test can run the GPU path and either checker side by side.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+from typing import Optional
+
+import numpy as np
+
+from snac_b200.abi import NT, Desc, Scalars, SnacConfig, State, StateView
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PATHS = {"port": os.path.join(HERE, "liboracle.so"),
+         "reference": os.path.join(HERE, "_ref", "libsnacref.so")}
+PREFIX = {"port": "so_", "reference": "ref_"}
+
+
+def build(kind: str = "port") -> str:
+    """Compile the checker with oracle/Makefile if it is missing."""
+    path = PATHS[kind]
+    if not os.path.exists(path):
+        subprocess.run(["make", "-s", "-C", HERE, "ref" if kind == "reference" else "all"], check=True)
+    return path
+
+
+def available(kind: str) -> bool:
+    return os.path.exists(PATHS[kind])
+
+
+_LIBS = {}
+
+
+def _lib(kind: str):
+    if kind not in _LIBS:
+        lib = C.CDLL(build(kind))
+        p = PREFIX[kind]
+        vp = C.c_void_p
+        lib_fn = lambda n: getattr(lib, p + n)  # noqa: E731
+        lib_fn("create").restype = vp
+        lib_fn("create").argtypes = [C.POINTER(Desc), C.POINTER(C.c_int)]
+        lib_fn("destroy").argtypes = [vp]
+        for n in ("time_step_zero", "begin_step", "loop_elements_energy", "loop_nodes_energy",
+                  "calc_stresses", "loop_nodes_momentum", "loop_elements_momentum", "sync"):
+            lib_fn(n).argtypes = [vp]
+            lib_fn(n).restype = C.c_int
+        lib_fn("step").argtypes = [vp, C.c_int]
+        lib_fn("step").restype = C.c_int
+        lib_fn("get_state").argtypes = [vp, C.POINTER(StateView)]
+        lib_fn("set_state").argtypes = [vp, C.POINTER(StateView)]
+        lib_fn("scalars").argtypes = [vp, C.POINTER(Scalars)]
+        lib_fn("set_dt").argtypes = [vp, C.c_double]
+        lib_fn("last_error").argtypes = [vp]
+        lib_fn("last_error").restype = C.c_char_p
+        dp = C.POINTER(C.c_double)
+        lib_fn("get_geometry").argtypes = [vp, dp, dp, dp]
+        lib_fn("get_element_scalars").argtypes = [vp, dp, dp, dp, dp, dp, dp]
+        lib_fn("get_tet_fields").argtypes = [vp, dp, dp, dp, dp]
+        lib_fn("get_node_fields").argtypes = [vp, dp, dp]
+        _LIBS[kind] = lib
+    return _LIBS[kind]
+
+
+def _p(a: Optional[np.ndarray]):
+    return None if a is None else a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Checker:
+    """One CPU model run (a Snac_Context)."""
+
+    def __init__(self, cfg: SnacConfig, kind: str = "port"):
+        self.kind = kind
+        self.cfg = cfg
+        self.lib = _lib(kind)
+        self._f = lambda n: getattr(self.lib, PREFIX[kind] + n)  # noqa: E731
+        self._desc = cfg.desc()
+        st = C.c_int(0)
+        self.h = self._f("create")(C.byref(self._desc), C.byref(st))
+        self.status = st.value
+        if not self.h:
+            raise RuntimeError(f"{kind} checker: create failed with status {st.value}")
+        self.ne, self.nn = cfg.n_elements, cfg.n_nodes
+
+    def close(self):
+        if self.h:
+            self._f("destroy")(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _call(self, name, *args) -> int:
+        return self._f(name)(self.h, *args)
+
+    def time_step_zero(self) -> int:
+        return self._call("time_step_zero")
+
+    def step(self, n: int = 1) -> int:
+        return self._call("step", int(n))
+
+    def begin_step(self):
+        return self._call("begin_step")
+
+    def loop_elements_energy(self):
+        return self._call("loop_elements_energy")
+
+    def loop_nodes_energy(self):
+        return self._call("loop_nodes_energy")
+
+    def calc_stresses(self):
+        return self._call("calc_stresses")
+
+    def loop_nodes_momentum(self):
+        return self._call("loop_nodes_momentum")
+
+    def loop_elements_momentum(self):
+        return self._call("loop_elements_momentum")
+
+    def sync(self):
+        return self._call("sync")
+
+    def set_dt(self, dt: float):
+        self._f("set_dt")(self.h, C.c_double(dt))
+
+    def last_error(self) -> str:
+        return self._f("last_error")(self.h).decode()
+
+    def state(self) -> State:
+        s = State.empty(self.ne, self.nn)
+        v = s.view()
+        self._f("get_state")(self.h, C.byref(v))
+        return s
+
+    def set_state(self, s: State, fields=None):
+        v = s.view(fields)
+        self._f("set_state")(self.h, C.byref(v))
+
+    def scalars(self) -> Scalars:
+        o = Scalars()
+        self._f("scalars")(self.h, C.byref(o))
+        return o
+
+    def geometry(self):
+        vol = np.zeros((self.ne, NT))
+        area = np.zeros((self.ne, NT, 4))
+        nrm = np.zeros((self.ne, NT, 4, 3))
+        self._f("get_geometry")(self.h, _p(vol), _p(area), _p(nrm))
+        return vol, area, nrm
+
+    def element_scalars(self):
+        out = [np.zeros(self.ne) for _ in range(6)]
+        self._f("get_element_scalars")(self.h, *[_p(a) for a in out])
+        return dict(zip(("volume", "strain_rate", "stress", "hydro_pressure", "aps", "min_length_scale"), out))
+
+    def tet_fields(self):
+        sr = np.zeros((self.ne, NT, 6))
+        sn = np.zeros((self.ne, NT, 6))
+        den = np.zeros((self.ne, NT))
+        at = np.zeros((self.ne, NT))
+        self._f("get_tet_fields")(self.h, _p(sr), _p(sn), _p(den), _p(at))
+        return {"strain_rate": sr, "strain": sn, "density": den, "avg_temp": at}
+
+    def node_fields(self):
+        mass = np.zeros(self.nn)
+        bal = np.zeros((self.nn, 3))
+        self._f("get_node_fields")(self.h, _p(mass), _p(bal))
+        return {"mass": mass, "balance": bal}
