@@ -1,0 +1,387 @@
+"""Benchmark of the SNAC explicit step on B200 (one JSON line on stdout).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3]
+    python bench.py --impl reference ...      # the reference's CPU code on the host cores
+
+A "step" is one _AbstractContext_Step of the model (Solve + Sync) over the
+whole mesh.  The default workload is configs[1]: 64 x 32(y) x 64 hex
+Mohr-Coulomb strain-softening (131,072 hex, 1.31 M tets), synthetic seeded
+inputs (snac_b200/workloads.py).  Its state (~0.1 GB) fits in the 126 MB L2,
+so a 512 MiB buffer is written between timed steps to flush L2.
+
+Timing: W untimed steps, then K steps, each bracketed by CUDA events
+recorded on the library's own stream; barrier + synchronize around the timed
+region; the max over ranks is taken.  With --gpus N (torchrun) every rank
+advances its own replica of the model (the single-model path is not
+sharded): value = all ranks' element-steps / slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "element-steps/s FP64 plain vs batched vs adjoint cost ratio, 1 B200, at stated tol"
+UNIT = "element-steps/s"
+
+# Algorithmic (compulsory) HBM bytes per element-step: persistent state read
+# once and written once.  Tet stress 10 x 6 x 8 B x 2 = 960 B; node x and v
+# 6 x 8 B x 2 = 96 B per node (nodes per hex below); plastic strain
+# 10 x 8 B x 2 = 160 B; per-element parameter 8 B; node temperature 8 B read.
+NODES_PER_HEX = {"c1": 2601 / 2048, "c2": 139425 / 131072, "c3": 1081665 / 1048576}
+
+
+def algorithmic_bytes(workload: str) -> float:
+    nph = NODES_PER_HEX[workload]
+    b = 960.0 + 96.0 * nph
+    if workload in ("c2", "c3"):
+        b += 160.0 + 8.0
+    if workload == "c3":
+        b += 8.0 * nph
+    return b
+
+
+def make_workload(name: str):
+    from snac_b200 import workloads as W
+    return {"c1": W.c1_elastic, "c2": W.c2_plastic, "c3": W.c3_viscoplastic}[name]()
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, reasons)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": len(self.rows)}
+        try:
+            sm = [float(r[1]) for r in self.rows if len(r) >= 9]
+            if sm:
+                out["sm_mhz"] = statistics.median(sm)
+                out["sm_max_mhz"] = max(float(r[2]) for r in self.rows if len(r) >= 9)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            seen = set()
+            for r in self.rows:
+                for k, nm in enumerate(names):
+                    if len(r) > 5 + k and r[5 + k].lower().startswith("active"):
+                        seen.add(nm)
+            out["reasons"] = sorted(seen)
+        except Exception:
+            pass
+        return out
+
+
+def dist_setup():
+    import torch
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def allmax(ws, x: float) -> float:
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ---------------------------------------------------------------------------------------------
+def cpu_sample(workload: str, steps: int, kind: str):
+    """Time the CPU checker on `steps` SNAC steps of the full workload (one core)."""
+    from oracle.pyoracle import Checker, available
+    if kind == "reference" and not available("reference"):
+        kind = "port"
+    cfg = make_workload(workload)
+    ck = Checker(cfg, kind)
+    ck.time_step_zero()
+    t = time.perf_counter()
+    ck.step(steps)
+    dt = time.perf_counter() - t
+    return cfg.n_elements * steps / dt, kind, dt
+
+
+def _cpu_worker(args):
+    workload, steps, kind = args
+    return cpu_sample(workload, steps, kind)
+
+
+def run_reference(args, ws, rank):
+    """--impl reference: the reference's own hot-path C code (oracle/_ref, or
+    the port when the reference could not be compiled) on the host cores, one
+    independent model copy per process (the reference is single-threaded and
+    not thread-safe)."""
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    from oracle.pyoracle import available
+    kind = "reference" if available("reference") else "port"
+    cfg = make_workload(args.workload)
+    ne = cfg.n_elements
+    ncpu = os.cpu_count() or 1
+    procs = max(1, min(ncpu, args.cpu_procs))
+    ctx = mp.get_context("spawn")
+    per_step = []
+    with ctx.Pool(procs) as pool:
+        for s in range(args.warmup + args.steps):
+            t = time.perf_counter()
+            res = pool.map(_cpu_worker, [(args.workload, 1, kind)] * procs)
+            dt = time.perf_counter() - t
+            if s >= args.warmup:
+                per_step.append(dt)
+    total = sum(per_step)
+    value = procs * ne * args.steps / total
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded, snac_b200/workloads.py)",
+        "config": {"workload": workload_name(args.workload), "hex": ne, "cpu_processes": procs},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+                         "sample": f"each step: {procs} processes x 1 SNAC step of the full {args.workload} mesh "
+                                   f"(includes per-process model construction)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def workload_name(w):
+    return {"c1": "configs[0] elastic 16x8(y)x16 hex over 100x30x100 km",
+            "c2": "configs[1] Mohr-Coulomb strain-softening 64x32(y)x64 hex over 200x40x200 km, lithostatic IC",
+            "c3": "configs[2] Maxwell visco-plastic + temperature 128x64(y)x128 hex over 400x100x400 km"}[w]
+
+
+# ---------------------------------------------------------------------------------------------
+def run_ours(args, ws, rank, local):
+    import numpy as np
+    import torch
+    from snac_b200.context import SnacContext
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfg = make_workload(args.workload)
+    ne = cfg.n_elements
+    ctx = SnacContext(cfg)
+    ctx.time_step_zero()
+    stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    # warm-up (also captures the CUDA graphs)
+    ctx.step(max(2, args.warmup))
+    torch.cuda.synchronize()
+
+    # ---- device-timed steps ------------------------------------------------------------
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    l0 = ctx.launches
+    barrier(ws)
+    torch.cuda.synchronize()
+    wall0 = time.perf_counter()
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.fill_(float(k))  # 512 MiB write: evicts the model state from L2
+            ev[k][0].record(stream)
+        ctx.lib.snac_gpu_step(ctx.h, 1)  # graph launch + status read
+        with torch.cuda.stream(stream):
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    barrier(ws)
+    wall = time.perf_counter() - wall0
+    launches = ctx.launches - l0
+    clocks = sampler.stop() if sampler else None
+    step_ms = [a.elapsed_time(b) for a, b in ev]
+    t_dev = sum(step_ms) / 1e3
+    t_max = allmax(ws, t_dev)
+    value = ws * ne * args.steps / t_max
+
+    # ---- per-kernel breakdown (hook by hook, events on the library stream) -------------
+    kern = {}
+    hooks = [("k_heat_flux", ctx.loop_elements_energy), ("k_heat_nodes", ctx.loop_nodes_energy),
+             ("k_calc_stresses", ctx.calc_stresses), ("k_loop_nodes", ctx.loop_nodes_momentum),
+             ("k_update_elements", ctx.loop_elements_momentum), ("k_sync", ctx.sync)]
+    nb = max(3, min(10, args.steps))
+    for _ in range(nb):
+        ctx.begin_step()
+        for name, fn in hooks:
+            with torch.cuda.stream(stream):
+                flush.fill_(1.0)
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+            fn()
+            with torch.cuda.stream(stream):
+                b.record(stream)
+            torch.cuda.synchronize()
+            kern.setdefault(name, []).append(a.elapsed_time(b))
+    kern_ms = {k: statistics.mean(v) for k, v in kern.items() if not (k.startswith("k_heat") and not cfg.temperature)}
+    top = max(kern_ms, key=kern_ms.get)
+    peak, peak_kind = load_peaks()
+    alg = algorithmic_bytes(args.workload)
+    step_ms_mean = 1e3 * t_dev / args.steps
+    achieved_step = alg * ne / (step_ms_mean / 1e3) / 1e9
+    kb = KERNEL_BYTES.get(top, lambda w: alg)(args.workload)
+    achieved_kernel = kb * ne / (kern_ms[top] / 1e3) / 1e9
+
+    # ---- end to end through the C ABI with host buffers --------------------------------
+    e2e = None
+    if not args.no_e2e:
+        from snac_b200.abi import State
+        st = ctx.state()
+        fields = ["coord", "velocity", "stress", "plastic_strain"]
+        host = State.empty(ctx.ne, ctx.nn)
+        pinned = {}
+        for f in fields:
+            t = torch.from_numpy(getattr(st, f)).pin_memory()
+            pinned[f] = t
+            setattr(host, f, t.numpy())
+        h2d = sum(pinned[f].numel() * 8 for f in fields)
+        ke = max(3, min(args.steps, 10))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            ctx.set_state(host, fields)          # host -> device, the step's inputs
+            ctx.step(1)
+            out = ctx.state()                    # device -> host, the step's result
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - t0) / ke
+        d2h = sum(getattr(out, f).nbytes for f in ("coord", "velocity", "stress", "plastic_strain", "viscosity",
+                                                    "temperature", "force", "inertial_mass"))
+        e2e = {"value": ws * ne / allmax(ws, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "note": "per step: snac_gpu_upload of the state from pinned host buffers, snac_gpu_step(1), "
+                       "snac_gpu_download of the state"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle.pyoracle import available
+        kind = "reference" if available("reference") else "port"
+        v, kind, dt = cpu_sample(args.workload, args.cpu_steps, kind)
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"{args.cpu_steps} SNAC steps of the full {args.workload} mesh ({ne} hex) on one host core, "
+                         f"{dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms_mean, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, snac_b200/workloads.py)",
+            "config": {"workload": workload_name(args.workload), "hex": ne, "tets": ne * 10, "nodes": cfg.n_nodes,
+                       "l2": "512 MiB flush written between timed steps",
+                       "parallelism": "replicas" if ws > 1 else "single model",
+                       "arithmetic": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle"},
+            "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
+                         "frac": achieved_kernel / peak, "traffic": None, "kernel": top,
+                         "kernel_ms": kern_ms[top], "algorithmic_bytes_per_hex": kb,
+                         "peak_source": peak_kind,
+                         "step": {"achieved": achieved_step, "frac": achieved_step / peak,
+                                  "algorithmic_bytes_per_hex": alg}},
+            "kernels_ms": kern_ms,
+            "gpu_launches": int(launches),
+            "wall_s": wall,
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+# Algorithmic bytes per hex of one launch of each kernel (state it must read / write once).
+KERNEL_BYTES = {
+    "k_calc_stresses": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
+                                 + (8.0 * NODES_PER_HEX[w] if w == "c3" else 0.0),
+    "k_loop_nodes": lambda w: 480.0 + 96.0 * NODES_PER_HEX[w],
+    "k_update_elements": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w],
+}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-procs", type=int, default=32)
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        ws = int(os.environ.get("WORLD_SIZE", "1"))
+        rank = int(os.environ.get("RANK", "0"))
+        run_reference(args, ws, rank)
+        return
+    ws, rank, local = dist_setup()
+    try:
+        run_ours(args, ws, rank, local)
+    finally:
+        if ws > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

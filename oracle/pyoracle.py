@@ -54,6 +54,9 @@ def _lib(kind: str):
                   "calc_stresses", "loop_nodes_momentum", "loop_elements_momentum", "sync"):
             lib_fn(n).argtypes = [vp]
             lib_fn(n).restype = C.c_int
+        if kind == "port":
+            lib_fn("node_forces").argtypes = [vp]
+            lib_fn("node_forces").restype = C.c_int
         lib_fn("step").argtypes = [vp, C.c_int]
         lib_fn("step").restype = C.c_int
         lib_fn("get_state").argtypes = [vp, C.POINTER(StateView)]
@@ -131,6 +134,10 @@ class Checker:
 
     def sync(self):
         return self._call("sync")
+
+    def node_forces(self):
+        """Snac_Force for every node, without the node update (port only)."""
+        return self._call("node_forces")
 
     def set_dt(self, dt: float):
         self._f("set_dt")(self.h, C.c_double(dt))

@@ -981,6 +981,13 @@ int so_calc_stresses(so_ctx* s) {
     return s->status;
 }
 
+/* Snac_Force for every node without the node update (the force loop of
+ * _Snac_Context_LoopNodes, Context.c:1129-1140) */
+int so_node_forces(so_ctx* s) {
+    for (long n = 0; n < s->nn; n++) node_force(s, n);
+    return s->status;
+}
+
 int so_loop_nodes_momentum(so_ctx* s) {
     for (long n = 0; n < s->nn; n++) node_force(s, n);
     for (long n = 0; n < s->nn; n++) node_update(s, n);

@@ -36,6 +36,7 @@ int so_loop_elements_energy(so_ctx* s);
 int so_loop_nodes_energy(so_ctx* s);
 int so_calc_stresses(so_ctx* s);
 int so_loop_nodes_momentum(so_ctx* s);
+int so_node_forces(so_ctx* s);   /* force loop only, no node update */
 int so_loop_elements_momentum(so_ctx* s);
 int so_sync(so_ctx* s);
 

@@ -1,0 +1,180 @@
+"""Python front end of the CUDA library (libsnac_b200.so) through its C ABI.
+
+SnacContext mirrors the reference's Snac_Context life cycle
+(Snac/libSnac/src/Context.c): construction applies the initial conditions,
+time_step_zero() is Snac_Context_TimeStepZero, step(n) runs n
+_AbstractContext_Step's (Solve + Sync), and the loop-level methods are the
+entry points a StGermain plugin replaces.  Every call goes to the CUDA
+library; there is no CPU path here.  If the library is missing or no GPU is
+visible, construction raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+from .abi import NT, STATUS_NAMES, Desc, Scalars, SnacConfig, State, StateView
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libsnac_b200.so")
+
+
+class SnacError(RuntimeError):
+    def __init__(self, code: int, msg: str, index: int = -1):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+        self.index = index
+
+
+_LIB = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Load libsnac_b200.so (raises OSError if it was not built)."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(path):
+        raise OSError(f"{path} is missing: run __graft_entry__.build() (or python -m snac_b200.build)")
+    lib = C.CDLL(path)
+    vp = C.c_void_p
+    lib.snac_gpu_create.argtypes = [C.POINTER(Desc), C.POINTER(vp)]
+    lib.snac_gpu_create.restype = C.c_int
+    lib.snac_gpu_destroy.argtypes = [vp]
+    lib.snac_gpu_destroy.restype = None
+    for n in ("time_step_zero", "begin_step", "loop_elements_energy", "loop_nodes_energy", "calc_stresses",
+              "loop_nodes_momentum", "loop_elements_momentum", "sync"):
+        f = getattr(lib, "snac_gpu_" + n)
+        f.argtypes = [vp]
+        f.restype = C.c_int
+    lib.snac_gpu_step.argtypes = [vp, C.c_int]
+    lib.snac_gpu_step.restype = C.c_int
+    lib.snac_gpu_upload.argtypes = [vp, C.POINTER(StateView)]
+    lib.snac_gpu_upload.restype = C.c_int
+    lib.snac_gpu_download.argtypes = [vp, C.POINTER(StateView)]
+    lib.snac_gpu_download.restype = C.c_int
+    lib.snac_gpu_scalars.argtypes = [vp, C.POINTER(Scalars)]
+    lib.snac_gpu_scalars.restype = C.c_int
+    lib.snac_gpu_set_dt.argtypes = [vp, C.c_double]
+    lib.snac_gpu_set_dt.restype = C.c_int
+    lib.snac_gpu_last_error.argtypes = [vp]
+    lib.snac_gpu_last_error.restype = C.c_char_p
+    lib.snac_gpu_error_index.argtypes = [vp]
+    lib.snac_gpu_error_index.restype = C.c_longlong
+    lib.snac_gpu_sizes.argtypes = [vp, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)]
+    lib.snac_gpu_sizes.restype = C.c_int
+    lib.snac_gpu_launch_count.argtypes = [vp]
+    lib.snac_gpu_launch_count.restype = C.c_longlong
+    lib.snac_gpu_stream.argtypes = [vp]
+    lib.snac_gpu_stream.restype = vp
+    lib.snac_gpu_device_count.argtypes = []
+    lib.snac_gpu_device_count.restype = C.c_int
+    _LIB = lib
+    return lib
+
+
+class SnacContext:
+    """One model on the GPU (one snac_gpu handle)."""
+
+    def __init__(self, cfg: SnacConfig):
+        self.lib = load_library()
+        self.cfg = cfg
+        self._desc = cfg.desc()
+        self.h = C.c_void_p()
+        rc = self.lib.snac_gpu_create(C.byref(self._desc), C.byref(self.h))
+        if rc != 0:
+            msg = self.lib.snac_gpu_last_error(self.h).decode() if self.h else ""
+            if self.h:
+                self.lib.snac_gpu_destroy(self.h)
+                self.h = C.c_void_p()
+            raise SnacError(rc, msg or "snac_gpu_create failed")
+        self.ne, self.nn = cfg.n_elements, cfg.n_nodes
+
+    # -- lifetime ---------------------------------------------------------------------
+    def close(self):
+        if self.h:
+            self.lib.snac_gpu_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _check(self, rc: int) -> int:
+        if rc != 0:
+            raise SnacError(rc, self.lib.snac_gpu_last_error(self.h).decode(), self.lib.snac_gpu_error_index(self.h))
+        return rc
+
+    # -- the reference's step structure ------------------------------------------------
+    def time_step_zero(self):
+        return self._check(self.lib.snac_gpu_time_step_zero(self.h))
+
+    def step(self, n: int = 1):
+        return self._check(self.lib.snac_gpu_step(self.h, int(n)))
+
+    def begin_step(self):
+        return self._check(self.lib.snac_gpu_begin_step(self.h))
+
+    def loop_elements_energy(self):
+        return self._check(self.lib.snac_gpu_loop_elements_energy(self.h))
+
+    def loop_nodes_energy(self):
+        return self._check(self.lib.snac_gpu_loop_nodes_energy(self.h))
+
+    def calc_stresses(self):
+        return self._check(self.lib.snac_gpu_calc_stresses(self.h))
+
+    def loop_nodes_momentum(self):
+        return self._check(self.lib.snac_gpu_loop_nodes_momentum(self.h))
+
+    def loop_elements_momentum(self):
+        return self._check(self.lib.snac_gpu_loop_elements_momentum(self.h))
+
+    def sync(self):
+        return self._check(self.lib.snac_gpu_sync(self.h))
+
+    def solve(self):
+        """_Snac_Context_Solve + Sync for one step, hook by hook."""
+        self.begin_step()
+        self.loop_elements_energy()
+        self.loop_nodes_energy()
+        self.calc_stresses()
+        self.loop_nodes_momentum()
+        self.loop_elements_momentum()
+        self.sync()
+
+    # -- state --------------------------------------------------------------------------
+    def state(self) -> State:
+        s = State.empty(self.ne, self.nn)
+        v = s.view()
+        self._check(self.lib.snac_gpu_download(self.h, C.byref(v)))
+        return s
+
+    def set_state(self, s: State, fields: Optional[list] = None):
+        v = s.view(fields)
+        self._check(self.lib.snac_gpu_upload(self.h, C.byref(v)))
+
+    def scalars(self) -> Scalars:
+        o = Scalars()
+        self._check(self.lib.snac_gpu_scalars(self.h, C.byref(o)))
+        return o
+
+    def set_dt(self, dt: float):
+        self._check(self.lib.snac_gpu_set_dt(self.h, C.c_double(dt)))
+
+    @property
+    def launches(self) -> int:
+        return int(self.lib.snac_gpu_launch_count(self.h))
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.snac_gpu_stream(self.h) or 0)

@@ -1,0 +1,426 @@
+// snac_device.cuh — device-side building blocks of the SNAC step for sm_100a.
+//
+// Everything here is FP64.  The translation unit that includes this file is
+// compiled with -fmad=false, so every expression below rounds exactly like
+// the reference's x86-64 build (no FMA contraction, IEEE division and square
+// root); the expressions keep the reference's evaluation order, and each
+// function cites the reference lines it computes.  Paths are relative to the
+// SNAC source tree.
+#pragma once
+
+#include <cstdint>
+
+#include "snac_gpu.h"
+
+namespace snac {
+
+constexpr int NT = 10;        // Tetrahedra_Count
+constexpr int MAX_PHASES = 32;
+
+// TetrahedraTables.c:42-84 (tets 0-4 are the first five-tet set, 5-9 the second).
+// Face f of a tet is the triangle opposite its local node (3,0,1,2)[f].
+// The tables are compile-time functions: inside unrolled loops every index
+// folds to a constant and the corner coordinates stay in registers.
+__host__ __device__ constexpr int tet_node(int t, int q) {
+    constexpr int tab[NT][4] = {{7, 2, 3, 0}, {0, 5, 4, 7}, {2, 5, 1, 0}, {5, 2, 6, 7}, {2, 5, 0, 7},
+                                {3, 4, 7, 6}, {4, 3, 0, 1}, {6, 1, 2, 3}, {1, 6, 5, 4}, {1, 3, 6, 4}};
+    return tab[t][q];
+}
+__host__ __device__ constexpr int face_node(int f, int k) {
+    constexpr int tab[4][3] = {{0, 1, 2}, {1, 3, 2}, {0, 2, 3}, {3, 1, 0}};
+    return tab[f][k];
+}
+__host__ __device__ constexpr int node_tet(int ne, int i) {
+    constexpr int tab[8][5] = {{3, 5, 7, 8, 9}, {0, 1, 3, 4, 5}, {1, 2, 3, 4, 8}, {1, 5, 6, 8, 9},
+                               {0, 2, 3, 4, 7}, {0, 5, 6, 7, 9}, {2, 6, 7, 8, 9}, {0, 1, 2, 4, 6}};
+    return tab[ne][i];
+}
+__host__ __device__ constexpr int node_face(int ne, int i) {
+    constexpr int tab[8][5] = {{3, 0, 1, 2, 3}, {1, 0, 0, 0, 3}, {2, 2, 1, 2, 3}, {3, 2, 1, 0, 0},
+                               {2, 1, 2, 1, 3}, {3, 1, 2, 0, 2}, {3, 0, 2, 1, 1}, {0, 1, 0, 3, 3}};
+    return tab[ne][i];
+}
+// element-local corner -> (di,dj,dk), HexaEL.c:456-471: corners 1,2,5,6 have di=1 ...
+__host__ __device__ constexpr int corner_di(int c) { return (c == 1 || c == 2 || c == 5 || c == 6) ? 1 : 0; }
+__host__ __device__ constexpr int corner_dj(int c) { return (c == 2 || c == 3 || c == 6 || c == 7) ? 1 : 0; }
+__host__ __device__ constexpr int corner_dk(int c) { return c >= 4 ? 1 : 0; }
+
+// tet_node for a per-lane (run-time) tet index, from two packed 64-bit words
+// (3 bits per corner): no constant-memory lookups that would serialise.
+__host__ __device__ constexpr unsigned long long pack_tets(int t0) {
+    unsigned long long w = 0;
+    for (int t = 0; t < 5; t++)
+        for (int q = 0; q < 4; q++) w |= (unsigned long long)tet_node(t0 + t, q) << (t * 12 + q * 3);
+    return w;
+}
+__device__ __forceinline__ int tet_node_rt(int t, int q) {
+    constexpr unsigned long long lo = pack_tets(0), hi = pack_tets(5);
+    unsigned long long w = t < 5 ? lo : hi;
+    int sh = (t < 5 ? t : t - 5) * 12 + q * 3;
+    return (int)((w >> sh) & 7ull);
+}
+
+// One phase on the device.  The transcendental values of a softening table
+// whose angles do not vary are evaluated once on the host with the host C
+// library (the reference's libm), so that a constant-angle Mohr-Coulomb run
+// rounds like the reference.
+struct DevMaterial {
+    double density, alpha, beta, lambda, mu;
+    int nsegments, yield_mc;
+    double plstrain[SNAC_MAX_SEGMENTS + 1];
+    double fric[SNAC_MAX_SEGMENTS + 1];
+    double dil[SNAC_MAX_SEGMENTS + 1];
+    double coh[SNAC_MAX_SEGMENTS + 1];
+    double ten_off;
+    double vis_min, vis_max, refvisc, refsrate, reftemp, H, srexponent;
+    double thermal_conduct, heat_capacity;
+    // host-evaluated transcendentals (valid when the *_const flag is set)
+    int fric_const, dil_const;
+    double fric0, sin_fric0, tan_fric0;
+    double dil0, sin_dil0;
+};
+
+// Device-resident scalars of one model (everything a captured step reads).
+struct DevScalars {
+    double dt;
+    double speed_of_sound;
+    double min_length_scale;
+    double vmax;
+    double init_min_length_scale;
+    unsigned long long minls_bits;   // running min of |V/A| (non-negative doubles order as integers)
+    unsigned long long vmax_bits;    // running max of |v| over velocity-BC nodes
+    long long time_step;
+    int pos_parity;                  // which of the two coordinate buffers is current
+    int status;                      // first error (SNAC_GPU_E*), 0 if none
+    long long err_index;
+    long long launches;
+};
+
+__device__ __forceinline__ void report(DevScalars* sc, int code, long long index) {
+    if (atomicCAS(&sc->status, 0, code) == 0) sc->err_index = index;
+}
+
+struct V3 {
+    double x, y, z;
+};
+
+// ---- Tetrahedra.c:44-113 ------------------------------------------------------------
+__device__ __forceinline__ double tet_volume(const V3& c1, const V3& c2, const V3& c3, const V3& c4) {
+    double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
+    double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
+    double x4 = c4.x - c1.x, y4 = c4.y - c1.y, z4 = c4.z - c1.z;
+    double v = (x4 * (y2 * z3 - z2 * y3) + y4 * (z2 * x3 - x2 * z3) + z4 * (x2 * y3 - x3 * y2)) / 6.0;
+    return fabs(v);
+}
+
+// Tetrahedra_SurfaceArea and Tetrahedra_SurfaceNormal evaluate the same cross
+// product and the same square root; computing it once gives the same bits.
+__device__ __forceinline__ void tet_face(const V3& c1, const V3& c2, const V3& c3, double& area, V3& n) {
+    double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
+    double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
+    double a = y2 * z3 - z2 * y3;
+    double b = z2 * x3 - x2 * z3;
+    double c = x2 * y3 - y2 * x3;
+    double s = sqrt(a * a + b * b + c * c);
+    area = s / 2.0;
+    n.x = a / s;
+    n.y = b / s;
+    n.z = c / s;
+}
+
+struct TetGeom {
+    double V;
+    double A[4];
+    V3 n[4];
+};
+
+__device__ __forceinline__ void tet_geometry(const V3 c[4], TetGeom& g) {
+    g.V = tet_volume(c[0], c[1], c[2], c[3]);
+#pragma unroll
+    for (int f = 0; f < 4; f++)
+        tet_face(c[face_node(f, 0)], c[face_node(f, 1)], c[face_node(f, 2)], g.A[f], g.n[f]);
+}
+
+__device__ __forceinline__ double comp(const V3& v, int d) { return d == 0 ? v.x : (d == 1 ? v.y : v.z); }
+
+// sum_k w_k,a * n_face(k),b * A_face(k) over the tet's nodes k (node k pairs
+// with face (1,2,3,0)[k]), StrainRate.c:65-184 / UpdateElement.c:145-219
+__device__ __forceinline__ double face_sum(const V3 w[4], int a, const TetGeom& g, int b) {
+    return comp(w[0], a) * comp(g.n[1], b) * g.A[1] + comp(w[1], a) * comp(g.n[2], b) * g.A[2] +
+           comp(w[2], a) * comp(g.n[3], b) * g.A[3] + comp(w[3], a) * comp(g.n[0], b) * g.A[0];
+}
+
+// The reference writes the spin and shear sums as one left-to-right chain
+// a0+a1+a2+a3 -/+ b0 -/+ b1 -/+ b2 -/+ b3 (UpdateElement.c:145-219,
+// StrainRate.c:101-184); these keep that chain.
+__device__ __forceinline__ double spin_sum(const V3 v[4], const TetGeom& g, int a, int b) {
+    return comp(v[0], a) * comp(g.n[1], b) * g.A[1] + comp(v[1], a) * comp(g.n[2], b) * g.A[2] +
+           comp(v[2], a) * comp(g.n[3], b) * g.A[3] + comp(v[3], a) * comp(g.n[0], b) * g.A[0] -
+           comp(v[0], b) * comp(g.n[1], a) * g.A[1] - comp(v[1], b) * comp(g.n[2], a) * g.A[2] -
+           comp(v[2], b) * comp(g.n[3], a) * g.A[3] - comp(v[3], b) * comp(g.n[0], a) * g.A[0];
+}
+__device__ __forceinline__ double shear_sum(const V3 v[4], const TetGeom& g, int a, int b) {
+    return comp(v[0], a) * comp(g.n[1], b) * g.A[1] + comp(v[1], a) * comp(g.n[2], b) * g.A[2] +
+           comp(v[2], a) * comp(g.n[3], b) * g.A[3] + comp(v[3], a) * comp(g.n[0], b) * g.A[0] +
+           comp(v[0], b) * comp(g.n[1], a) * g.A[1] + comp(v[1], b) * comp(g.n[2], a) * g.A[2] +
+           comp(v[2], b) * comp(g.n[3], a) * g.A[3] + comp(v[3], b) * comp(g.n[0], a) * g.A[0];
+}
+
+// StrainRate.c:65-184, before the mixed-discretisation correction;
+// sr = (xx, yy, zz, xy, xz, yz)
+__device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g, double sr[6]) {
+    sr[0] = -1.0f * (face_sum(v, 0, g, 0)) / 3.0f / g.V;
+    sr[1] = -1.0f * (face_sum(v, 1, g, 1)) / 3.0f / g.V;
+    sr[2] = -1.0f * (face_sum(v, 2, g, 2)) / 3.0f / g.V;
+    sr[3] = -0.5f * (shear_sum(v, g, 0, 1)) / 3.0f / g.V;
+    sr[4] = -0.5f * (shear_sum(v, g, 0, 2)) / 3.0f / g.V;
+    sr[5] = -0.5f * (shear_sum(v, g, 1, 2)) / 3.0f / g.V;
+}
+
+// Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
+// zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
+__device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
+    double r01 = -(0.5f / g.V) * (spin_sum(v, g, 0, 1)) / 3.0f;
+    double r02 = -(0.5f / g.V) * (spin_sum(v, g, 0, 2)) / 3.0f;
+    double r12 = -(0.5 / g.V) * (spin_sum(v, g, 1, 2)) / 3.0f;
+    s[0] += (2.0f * r01 * s[3] + 2.0f * r02 * s[4]) * dt;
+    s[1] += (2.0f * (-1.0f * r01) * s[3] + 2.0f * r12 * s[5]) * dt;
+    s[2] += (2.0f * (-1.0f * r02) * s[4] + 2.0f * (-1.0f * r12) * s[5]) * dt;
+    s[3] += (r01 * (s[1] - s[0])) * dt + (r02 * s[5] + r12 * s[4]) * dt;
+    s[4] += (r02 * (s[2] - s[0])) * dt + (r01 * s[5] - r12 * s[3]) * dt;
+    s[5] += (r12 * (s[2] - s[1])) * dt + ((-1.0f * r01) * s[4] - r02 * s[3]) * dt;
+}
+
+// ---- plastic/Constitutive.c:249-410: cyclic Jacobi (Numerical Recipes
+// jacobi/eigsrt) on the symmetric stress, then principal values ascending
+// (most compressive first) and their directions cn[k] = eigenvector k.
+// The three (ip,iq) pairs and their rotate loops are spelled out so that the
+// whole solver lives in registers.
+__host__ __device__ __forceinline__ void jrot(double& aij, double& akl, double s, double tau) {
+    double g = aij, h = akl;
+    aij = g - s * (h + g * tau);
+    akl = h + s * (g - h * tau);
+}
+
+struct Jac {
+    double a01, a02, a12;  // off-diagonal part (the diagonal lives in d/b)
+    double d[3], b[3], z[3];
+    double v[3][3];
+};
+
+template <int IP, int IQ>
+__host__ __device__ __forceinline__ void jac_pair(Jac& J, int i, double tresh) {
+    double& apq = (IP == 0 && IQ == 1) ? J.a01 : (IP == 0 && IQ == 2) ? J.a02 : J.a12;
+    double g = 100.0f * fabs(apq);
+    if ((i > 4) && (double)(fabs(J.d[IP]) + g) == (double)fabs(J.d[IP]) &&
+        (double)(fabs(J.d[IQ]) + g) == (double)fabs(J.d[IQ])) {
+        apq = 0.0f;
+    } else if (fabs(apq) > tresh) {
+        double h = J.d[IQ] - J.d[IP], t;
+        if ((fabs(h) + g) == fabs(h)) {
+            t = apq / h;
+        } else {
+            double theta = 0.5f * h / (apq);
+            t = 1.0f / (fabs(theta) + sqrt(1.0f + theta * theta));
+            if (theta < 0.0f) t *= -1.0f;
+        }
+        double c = 1.0f / sqrt(1.0f + t * t);
+        double s = t * c;
+        double tau = s / (1.0f + c);
+        h = t * apq;
+        J.z[IP] -= h;
+        J.z[IQ] += h;
+        J.d[IP] -= h;
+        J.d[IQ] += h;
+        apq = 0.0f;
+        // the reference's three rotate loops for this pair (j < ip, ip < j < iq, j > iq)
+        if (IP == 0 && IQ == 1) jrot(J.a02, J.a12, s, tau);          // j = 2 > iq
+        if (IP == 0 && IQ == 2) jrot(J.a01, J.a12, s, tau);          // j = 1 between
+        if (IP == 1 && IQ == 2) jrot(J.a01, J.a02, s, tau);          // j = 0 < ip
+#pragma unroll
+        for (int j = 0; j < 3; j++) jrot(J.v[j][IP], J.v[j][IQ], s, tau);
+    }
+}
+
+__host__ __device__ void principal_stresses(const double st[6], double sp[3], double cn[3][3]) {
+    Jac J;
+    J.a01 = st[3];
+    J.a02 = st[4];
+    J.a12 = st[5];
+#pragma unroll
+    for (int ip = 0; ip < 3; ip++) {
+#pragma unroll
+        for (int iq = 0; iq < 3; iq++) J.v[ip][iq] = 0.0f;
+        J.v[ip][ip] = 1.0f;
+    }
+#pragma unroll
+    for (int ip = 0; ip < 3; ip++) {
+        J.b[ip] = J.d[ip] = st[ip];
+        J.z[ip] = 0.0f;
+    }
+    for (int i = 1; i <= 50; i++) {
+        double sm = 0.0f;
+        sm += fabs(J.a01);
+        sm += fabs(J.a02);
+        sm += fabs(J.a12);
+        if (sm == 0.0f) break;
+        double tresh = (i < 4) ? 0.2f * sm / (3u * 3u) : 0.0f;
+        jac_pair<0, 1>(J, i, tresh);
+        jac_pair<0, 2>(J, i, tresh);
+        jac_pair<1, 2>(J, i, tresh);
+#pragma unroll
+        for (int ip = 0; ip < 3; ip++) {
+            J.b[ip] += J.z[ip];
+            J.d[ip] = J.b[ip];
+            J.z[ip] = 0.0f;
+        }
+    }
+    double d[3] = {J.d[0] * -1.0f, J.d[1] * -1.0f, J.d[2] * -1.0f};
+    // eigsrt: descending, ">=" keeps the later index on ties
+#pragma unroll
+    for (int i = 0; i < 2; i++) {
+        int k = i;
+        double p = d[i];
+#pragma unroll
+        for (int j = i + 1; j < 3; j++)
+            if (d[j] >= p) {
+                k = j;
+                p = d[j];
+            }
+        if (k != i) {
+            // swap entry i with entry k (k > i), columns of v likewise
+#pragma unroll
+            for (int kk = i + 1; kk < 3; kk++)
+                if (kk == k) {
+                    d[kk] = d[i];
+                    d[i] = p;
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        double q = J.v[j][i];
+                        J.v[j][i] = J.v[j][kk];
+                        J.v[j][kk] = q;
+                    }
+                }
+        }
+    }
+#pragma unroll
+    for (int i = 0; i < 3; i++) {
+        sp[i] = d[i] * -1.0f;
+#pragma unroll
+        for (int j = 0; j < 3; j++) cn[i][j] = J.v[j][i];
+    }
+}
+
+// True when the tet provably does not reach the Mohr-Coulomb or tension
+// surface, so the reference would leave its trial stress untouched: the
+// exact eigenvalues lie in the Gershgorin interval [lo, hi], the Jacobi
+// values are within ~1e-15 of the stress scale of them, and the margin asked
+// for is 1e-9 of that scale.  Skipping the eigen-solve then changes no bit.
+__host__ __device__ __forceinline__ bool surely_elastic(const double st[6], double cohesion, double anphi, double stc) {
+    double r0 = fabs(st[3]) + fabs(st[4]);
+    double r1 = fabs(st[3]) + fabs(st[5]);
+    double r2 = fabs(st[4]) + fabs(st[5]);
+    double hi = fmax(st[0] + r0, fmax(st[1] + r1, st[2] + r2));
+    double lo = fmin(st[0] - r0, fmin(st[1] - r1, st[2] - r2));
+    double scale = fabs(st[0]) + fabs(st[1]) + fabs(st[2]) + 2.0 * (r0 + r1 + r2);
+    double cterm = 2.0 * cohesion * sqrt(anphi);
+    double tol_t = 1e-9 * (scale + fabs(stc)) + 1e-300;
+    double tol_s = 1e-9 * (scale * (1.0 + anphi) + fabs(cterm)) + 1e-300;
+    bool no_tension = hi - stc < -tol_t;
+    bool no_shear = (lo - hi * anphi + cterm) > tol_s;
+    return no_tension && no_shear && anphi > 0.0;
+}
+
+// PI/180 with PI = M_PI, plastic/Constitutive.c:44-55
+__device__ __forceinline__ double degrad() { return 3.14159265358979323846 / 180.0f; }
+
+__device__ __forceinline__ double sin_fric(const DevMaterial& m, double phi) {
+    return (m.fric_const && phi == m.fric0) ? m.sin_fric0 : sin(phi * degrad());
+}
+__device__ __forceinline__ double tan_fric(const DevMaterial& m, double phi) {
+    return (m.fric_const && phi == m.fric0) ? m.tan_fric0 : tan(phi * degrad());
+}
+__device__ __forceinline__ double sin_dil(const DevMaterial& m, double psi) {
+    return (m.dil_const && psi == m.dil0) ? m.sin_dil0 : sin(psi * degrad());
+}
+
+// Mohr-Coulomb composite yield + return map in principal space, shared by
+// plastic/Constitutive.c:180-237 and viscoplastic/Constitutive.c:305-370.
+// Returns 1 when the tet yielded (stress resolved back, plastic strain grown).
+__device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3], double st6[6], double& eps_p,
+                                             double cohesion, double hardening, double anphi, double anpsi,
+                                             double st, double a1, double a2) {
+    double alam, dep1, dep2, dep3, depm;
+    double fs = sp[0] - sp[2] * anphi + 2 * cohesion * sqrt(anphi);
+    double ft = sp[2] - st;
+    if (!(fs < 0.0f || ft > 0.0f)) return 0;
+    double aP = sqrt(1.0f + anphi * anphi) + anphi;
+    double sP = st * anphi - 2 * cohesion * sqrt(anphi);
+    double h = sp[2] - st + aP * (sp[0] - sP);
+    if (h < 0.0f) {
+        alam = fs / (a1 - a2 * anpsi + a1 * anphi * anpsi - a2 * anphi + 2.0 * sqrt(anphi) * hardening);
+        sp[0] -= alam * (a1 - a2 * anpsi);
+        sp[1] -= alam * a2 * (1.0f - anpsi);
+        sp[2] -= alam * (a2 - a1 * anpsi);
+        dep1 = alam;
+        dep2 = 0.0f;
+        dep3 = -alam * anpsi;
+    } else {
+        alam = ft / a1;
+        sp[0] -= alam * a2;
+        sp[1] -= alam * a2;
+        sp[2] -= alam * a1;
+        dep1 = 0.0f;
+        dep2 = 0.0f;
+        dep3 = alam;
+    }
+    depm = (dep1 + dep2 + dep3) / 3.0f;
+    eps_p += sqrt(0.5f * ((dep1 - depm) * (dep1 - depm) + (dep2 - depm) * (dep2 - depm) +
+                          (dep3 - depm) * (dep3 - depm) + depm * depm));
+    double r[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    for (int m = 0; m < 3; m++)
+        for (int n = m; n < 3; n++)
+            for (int k = 0; k < 3; k++) r[m][n] += cn[k][m] * cn[k][n] * sp[k];
+    st6[0] = r[0][0];
+    st6[1] = r[1][1];
+    st6[2] = r[2][2];
+    st6[3] = r[0][1];
+    st6[4] = r[0][2];
+    st6[5] = r[1][2];
+    return 1;
+}
+
+// Power-law / Arrhenius viscosity, viscoplastic/Constitutive.c:186-210 and
+// maxwell/Constitutive.c:122-142, clipped to [vis_min, vis_max].
+__device__ __forceinline__ double arrhenius_viscosity(double refvisc, double srJ2, double rstrainrate,
+                                                      double srexponent, double H, double avgTemp, double rTemp,
+                                                      double vis_min, double vis_max) {
+    const double R = 8.31448;
+    double eta = refvisc * pow((srJ2 / rstrainrate), (1. / srexponent - 1.)) *
+                 exp(H / R * (1. / (avgTemp + 273.15) - 1. / (rTemp + 273.15)));
+    if (eta < vis_min) eta = vis_min;
+    if (eta > vis_max) eta = vis_max;
+    return eta;
+}
+
+// Maxwell visco-elastic update of one tet, viscoplastic/Constitutive.c:211-257
+// and maxwell/Constitutive.c:146-183 (identical arithmetic).
+__device__ __forceinline__ void maxwell_update(double s[6], const double e[6], double stressd[3],
+                                               const double straind[3], double trace_stress, double trace_strain,
+                                               double rmu, double eta, double dt, double bulkm) {
+    double temp = rmu / (2.0f * (eta)) * dt;
+    double vic1 = 1.0f - temp;
+    double vic2 = 1.0f / (1.0f + temp);
+    stressd[0] = (stressd[0] * vic1 + 2.0f * rmu * straind[0]) * vic2;
+    stressd[1] = (stressd[1] * vic1 + 2.0f * rmu * straind[1]) * vic2;
+    stressd[2] = (stressd[2] * vic1 + 2.0f * rmu * straind[2]) * vic2;
+    s[3] = (s[3] * vic1 + 2.0f * rmu * e[3]) * vic2;
+    s[4] = (s[4] * vic1 + 2.0f * rmu * e[4]) * vic2;
+    s[5] = (s[5] * vic1 + 2.0f * rmu * e[5]) * vic2;
+    double VolumicStress = trace_stress / 3.0f + bulkm * trace_strain;
+    s[0] = stressd[0] + VolumicStress;
+    s[1] = stressd[1] + VolumicStress;
+    s[2] = stressd[2] + VolumicStress;
+}
+
+}  // namespace snac

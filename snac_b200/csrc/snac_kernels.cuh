@@ -1,0 +1,707 @@
+// snac_kernels.cuh — the kernels of one SNAC step (reference rounding).
+//
+// Per step, in _Snac_Context_Solve order (Snac/libSnac/src/Context.c:1063-1099):
+//   k_heat_flux      Snac_EP_LoopElementsEnergy  temperature/HeatFlux.c:47-200 + HeatFluxBC
+//   k_heat_nodes     Snac_EP_LoopNodesEnergy     temperature/Heat.c:47-140
+//   k_calc_stresses  Snac_EP_CalcStresses        StrainRate.c + Stress.c + the constitutive hook
+//   k_loop_nodes     Snac_EP_LoopNodesMomentum   Force.c + UpdateNode.c
+//   k_update_elements Snac_EP_LoopElementsMomentum UpdateElement.c
+//   k_sync           AbstractContext_EP_Sync     Context.c:1208-1268
+//
+// Element kernels run one thread per tetrahedron: a warp holds three
+// elements in lanes 0-9, 10-19, 20-29 (lanes 30-31 idle).  Element sums
+// (volume, traces) are gathered lane by lane with shuffles and added in the
+// reference's tet order, so they round like the reference's loops.  Node
+// kernels run one thread per node and gather the 8 adjacent hexes x 5 tets in
+// the reference's fixed order (Force.c:87-181): no atomics, bit-reproducible.
+//
+// Geometry (volumes, face areas and normals) is never stored: each kernel
+// recomputes it from the coordinates with the reference's formulas, which
+// gives the same bits the reference stored in its element structs.
+#pragma once
+
+#include "snac_device.cuh"
+
+namespace snac {
+
+struct Mesh {
+    int nx, ny, nz, nnx, nny, nnz;
+    long long ne, nn;
+};
+
+struct Fields {
+    const double4* pos;      // current coordinates (x, y, z) and temperature (w)
+    double4* pos_next;       // written by k_loop_nodes (coordinates are double-buffered)
+    double4* vel;            // velocity (x, y, z) and temperature0 (w)
+    double4* force;          // damped force (x, y, z) and inertial mass (w)
+    double* stress;          // [ne*10][6]
+    double* eps_p;           // [ne*10]  plastic strain (plastic, visco-plastic)
+    double* visc;            // [ne*10]  viscosity (visco-plastic, Maxwell)
+    double* density;         // [ne*10]  only when some phase has alpha or beta != 0
+    double* vol;             // [ne*10][2] volume, old volume (Maxwell)
+    double* hflux;           // [ne*10][4] heat flux x, y, z and thermal stress
+    double* tpre;            // [nn] temperature before the BCs (temperature + density)
+    const uchar4* bc;        // per node: velocity-VC index of x, y, z and temperature-VC index (255 = free)
+    const double* vbc_val;   // [n_vc][3]
+    const double* tbc_val;   // [n_tc]
+    const unsigned char* mat;        // [ne] phase, NULL = 0
+    const DevMaterial* mats;         // phase table of this model
+    const double* coh_scale;         // [ne] or NULL
+    const double* fric_scale;        // [ne] or NULL
+    const double* visc_scale;        // [ne] or NULL
+    DevScalars* sc;
+};
+
+struct Config {
+    int dt_type, constitutive, temperature, thermal_stress, has_density, time_step_zero;
+    double gravity, demf;
+    double strain_inert;
+};
+
+constexpr int ELEM_WARPS = 4;                  // warps per block in the element kernels
+constexpr int ELEM_PER_BLOCK = ELEM_WARPS * 3;  // 12 elements per block
+constexpr unsigned FULL = 0xffffffffu;
+
+__device__ __forceinline__ long long node_id(const Mesh& m, int i, int j, int k) {
+    return (long long)i + (long long)j * m.nnx + (long long)k * m.nnx * m.nny;
+}
+
+__device__ __forceinline__ void elem_ijk(const Mesh& m, long long e, int& i, int& j, int& k) {
+    i = (int)(e % m.nx);
+    j = (int)((e / m.nx) % m.ny);
+    k = (int)(e / ((long long)m.nx * m.ny));
+}
+
+__device__ __forceinline__ long long corner_node(const Mesh& m, int i, int j, int k, int corner) {
+    return node_id(m, i + corner_di(corner), j + corner_dj(corner), k + corner_dk(corner));
+}
+
+__device__ __forceinline__ int phase_of(const Fields& F, long long e) { return F.mat ? (int)F.mat[e] : 0; }
+
+// The value of lane (base + u) of this lane's element group.
+__device__ __forceinline__ double grp(double v, int base, int u) { return __shfl_sync(FULL, v, base + u); }
+
+// Sum over the 10 tets of the group, added in tet order starting from 0.
+__device__ __forceinline__ double grp_sum(double v, int base) {
+    double s = 0.0f;
+#pragma unroll
+    for (int u = 0; u < NT; u++) s += grp(v, base, u);
+    return s;
+}
+
+struct TetSlot {
+    int lane, base, t;
+    long long e, q;
+    bool active;
+    int i, j, k;
+};
+
+__device__ __forceinline__ TetSlot tet_slot(const Mesh& m) {
+    TetSlot s;
+    s.lane = threadIdx.x & 31;
+    int g = s.lane / 10;
+    s.base = g * 10;
+    s.t = s.lane - s.base;
+    long long warp = (long long)blockIdx.x * ELEM_WARPS + (threadIdx.x >> 5);
+    s.e = warp * 3 + g;
+    s.active = (g < 3) && (s.e < m.ne);
+    if (g >= 3) {  // lanes 30, 31 mirror lane 0-9 group 0 slots so shuffles stay in range
+        s.base = 0;
+        s.t = s.lane - 30;
+    }
+    s.q = s.e * NT + s.t;
+    if (s.active)
+        elem_ijk(m, s.e, s.i, s.j, s.k);
+    else
+        s.i = s.j = s.k = 0;
+    return s;
+}
+
+// loads the tet's 4 corners (coordinates, velocities, temperatures)
+__device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const TetSlot& s, V3 c[4], V3 v[4],
+                                         double T[4], double T0[4]) {
+#pragma unroll
+    for (int qn = 0; qn < 4; qn++) {
+        if (s.active) {
+            long long n = corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn));
+            double4 p = F.pos[n];
+            double4 w = F.vel[n];
+            c[qn] = {p.x, p.y, p.z};
+            T[qn] = p.w;
+            v[qn] = {w.x, w.y, w.z};
+            T0[qn] = w.w;
+        } else {  // a regular dummy tet keeps inactive lanes finite
+            c[qn] = {qn == 1 ? 1.0 : 0.0, qn == 2 ? 1.0 : 0.0, qn == 3 ? 1.0 : 0.0};
+            v[qn] = {0.0, 0.0, 0.0};
+            T[qn] = T0[qn] = 0.0;
+        }
+    }
+}
+
+// ======================================================================================
+// Snac_EP_CalcStresses: StrainRate.c:49-305, Stress.c:53-172 and the constitutive hook
+// ======================================================================================
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32) k_calc_stresses(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    const double dt = F.sc->dt;
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    double sr[6];
+    tet_strain_rate(v, g, sr);
+
+    // element volume: UpdateElement.c:141,267 then 2*volume (StrainRate.c:62)
+    double vsum = grp_sum(g.V, s.base);
+    double elemVolume = 2.0 * (vsum * 0.5);
+    // mixed discretisation, StrainRate.c:272-289
+    double trace = (sr[0] + sr[1] + sr[2]) / 3.0f;
+    double partial = 0.0f;
+#pragma unroll
+    for (int u = 0; u < NT; u++) partial += grp(trace, s.base, u) * grp(g.V, s.base, u);
+    double corr = -1.0f * trace + partial / elemVolume;
+    sr[0] += corr;
+    sr[1] += corr;
+    sr[2] += corr;
+
+    // strain, Stress.c:71-82
+    double e[6];
+#pragma unroll
+    for (int a = 0; a < 6; a++) e[a] = sr[a] * dt;
+
+    const int ph = s.active ? phase_of(F, s.e) : 0;
+    const DevMaterial& M = F.mats[ph];
+    double st[6] = {0, 0, 0, 0, 0, 0};
+    if (s.active) {
+#pragma unroll
+        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+    }
+    double eps_p = 0.0, eta = 0.0;
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
+        eps_p = s.active ? F.eps_p[s.q] : 0.0;
+
+    double sp[3] = {0, 0, 0}, cn[3][3];
+    // softening-table lookup results of this tet (for the carry-over between tets)
+    double fa = 0.0f, da = 0.0f, co = 0.0f, hd = 0.0f;
+    int matched = 0;
+
+    if (PLUGIN == SNAC_RHEOLOGY_ELASTIC) {
+        // elastic/Constitutive.c:40-66
+        const double a2 = M.lambda;
+        const double sh2 = 2.0 * M.mu;
+        double tr = e[0] + e[1] + e[2];
+        st[0] += sh2 * e[0] + a2 * (tr);
+        st[1] += sh2 * e[1] + a2 * (tr);
+        st[2] += sh2 * e[2] + a2 * (tr);
+        st[3] += sh2 * e[3];
+        st[4] += sh2 * e[4];
+        st[5] += sh2 * e[5];
+    } else if (PLUGIN == SNAC_RHEOLOGY_MAXWELL) {
+        // maxwell/Constitutive.c:47-184
+        const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+        double vold = s.active ? F.vol[s.q * 2 + 1] : 1.0;
+        double vcur = s.active ? F.vol[s.q * 2 + 0] : 1.0;
+        double trace_stress = st[0] + st[1] + st[2];
+        double trace_strain = vcur / vold - 1.0f;
+        double straind[3], stressd[3];
+        for (int a = 0; a < 3; a++) straind[a] = e[a] - (trace_strain) / 3.0f;
+        for (int a = 0; a < 3; a++) stressd[a] = st[a] - (trace_stress) / 3.0f;
+        double srJ2 = sqrt(fabs(straind[1] * straind[2] + straind[2] * straind[0] + straind[0] * straind[1] -
+                                e[3] * e[3] - e[4] * e[4] - e[5] * e[5])) /
+                      dt;
+        if (srJ2 == 0.0f) srJ2 = M.refsrate;
+        double avgTemp = 0.0;
+        for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
+        eta = arrhenius_viscosity(M.refvisc, srJ2, M.refsrate, M.srexponent, M.H, avgTemp, M.reftemp, M.vis_min,
+                                  M.vis_max);
+        if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
+        if (ph == 0) maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
+    } else {
+        const double a1 = M.lambda + 2.0f * M.mu;
+        const double a2 = M.lambda;
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) {
+            // elastic trial, plastic/Constitutive.c:114-121
+            double tr = e[0] + e[1] + e[2];
+            st[0] += (2.0f * M.mu) * e[0] + M.lambda * (tr);
+            st[1] += (2.0f * M.mu) * e[1] + M.lambda * (tr);
+            st[2] += (2.0f * M.mu) * e[2] + M.lambda * (tr);
+            st[3] += (2.0f * M.mu) * e[3];
+            st[4] += (2.0f * M.mu) * e[4];
+            st[5] += (2.0f * M.mu) * e[5];
+            if (s.active && M.plstrain[0] != 0.0) report(F.sc, SNAC_GPU_EINVAL, s.e);
+        } else {
+            // visco-plastic Maxwell step, viscoplastic/Constitutive.c:158-257
+            const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+            if (cfg.thermal_stress) {
+                double ts = s.active ? F.hflux[s.q * 4 + 3] : 0.0;
+                st[0] += ts;
+                st[1] += ts;
+                st[2] += ts;
+            }
+            double trace_stress = st[0] + st[1] + st[2];
+            double trace_strain = e[0] + e[1] + e[2];
+            double straind[3], stressd[3];
+            for (int a = 0; a < 3; a++) straind[a] = e[a] - (trace_strain) / 3.0f;
+            for (int a = 0; a < 3; a++) stressd[a] = st[a] - (trace_stress) / 3.0f;
+            // viscoplastic/Constitutive.c:189 reads strain[1][0], strain[2][0] and stress[2][0]
+            // (the pointer, not the tensor, is indexed); those entries are always zero.
+            const double lower = 0.0;
+            double srJ2 = sqrt(fabs(straind[1] * straind[2] + straind[2] * straind[0] + straind[0] * straind[1] -
+                                    (lower) * (lower) - (lower) * (lower) - (lower) * (lower))) /
+                          dt;
+            if (srJ2 == 0.0f) srJ2 = M.refsrate;
+            double avgTemp = 0.0;
+            for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
+            double refvisc = M.refvisc;
+            if (F.visc_scale && s.active) refvisc = M.refvisc * F.visc_scale[s.e];
+            eta = arrhenius_viscosity(refvisc, srJ2, M.refsrate, M.srexponent, M.H, avgTemp, M.reftemp, M.vis_min,
+                                      M.vis_max);
+            if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
+            maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
+        }
+        // piecewise-linear softening (plastic/Constitutive.c:133-159 with break and
+        // clamp; viscoplastic/Constitutive.c:279-293 without either: the last
+        // matching segment wins)
+        const double cs = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
+        const double fsc = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
+        for (int i = 0; i < M.nsegments; i++) {
+            const double pl1 = M.plstrain[i];
+            const double pl2 = M.plstrain[i + 1];
+            double f0 = F.fric_scale ? M.fric[i] * fsc : M.fric[i];
+            double f1 = F.fric_scale ? M.fric[i + 1] * fsc : M.fric[i + 1];
+            double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
+            double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
+            if (eps_p >= pl1 && eps_p <= pl2) {
+                const double tgf = (f1 - f0) / (pl2 - pl1);
+                const double tgd = (M.dil[i + 1] - M.dil[i]) / (pl2 - pl1);
+                const double tgc = (c1 - c0) / (pl2 - pl1);
+                fa = f0 + tgf * (eps_p - pl1);
+                da = M.dil[i] + tgd * (eps_p - pl1);
+                co = c0 + tgc * (eps_p - pl1);
+                hd = tgc;
+                matched = 1;
+                if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) break;
+            } else if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && i == M.nsegments - 1 && eps_p > pl2) {
+                fa = F.fric_scale ? M.fric[M.nsegments] * fsc : M.fric[M.nsegments];
+                da = M.dil[M.nsegments];
+                co = F.coh_scale ? M.coh[M.nsegments] * cs : M.coh[M.nsegments];
+                hd = 0.0;
+                matched = 1;
+                break;
+            }
+        }
+    }
+
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC) {
+        // The reference keeps the table values (and the tension cutoff) in
+        // variables that outlive the tet loop: a tet whose lookup matched no
+        // segment reuses the previous tet's values, 0 before the first match.
+        unsigned mb = __ballot_sync(FULL, matched && s.active);
+        unsigned mine = (mb >> s.base) & ((1u << (s.t + 1)) - 1u);
+        int src = mine ? (31 - __clz(mine)) : -1;
+        double src_fa = __shfl_sync(FULL, fa, s.base + (src < 0 ? 0 : src));
+        double src_da = __shfl_sync(FULL, da, s.base + (src < 0 ? 0 : src));
+        double src_co = __shfl_sync(FULL, co, s.base + (src < 0 ? 0 : src));
+        double src_hd = __shfl_sync(FULL, hd, s.base + (src < 0 ? 0 : src));
+        double frictionAngle = src < 0 ? 0.0f : src_fa;
+        double dilationAngle = src < 0 ? 0.0f : src_da;
+        double cohesion = src < 0 ? 0.0f : src_co;
+        double hardening = src < 0 ? 0.0f : src_hd;
+        // tension cutoff st = min(ten_off, c / tan(phi)) when phi > 0, else carried over
+        bool phi_ok = (PLUGIN == SNAC_RHEOLOGY_PLASTIC) ? (frictionAngle >= 0.0f) : (frictionAngle > 0.0f);
+        double st_own = 0.0;
+        if (phi_ok) {
+            st_own = M.ten_off;
+            if (frictionAngle > 0.0) {
+                double tmp = cohesion / tan_fric(M, frictionAngle);
+                if (tmp < st_own) st_own = tmp;
+            }
+        }
+        unsigned pb = __ballot_sync(FULL, phi_ok && s.active);
+        unsigned pm = (pb >> s.base) & ((1u << (s.t + 1)) - 1u);
+        int psrc = pm ? (31 - __clz(pm)) : -1;
+        double st_c = __shfl_sync(FULL, st_own, s.base + (psrc < 0 ? 0 : psrc));
+        double stc = psrc < 0 ? 0.0 : st_c;
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && s.active && frictionAngle < 0.0f)
+            report(F.sc, SNAC_GPU_EPHYSICS, s.e);  // plastic/Constitutive.c:175 abort()
+        double sphi = sin_fric(M, frictionAngle);
+        double spsi = sin_dil(M, dilationAngle);
+        double anphi = (1.0f + sphi) / (1.0f - sphi);
+        double anpsi = (1.0f + spsi) / (1.0f - spsi);
+        const double a1 = M.lambda + 2.0f * M.mu;
+        const double a2 = M.lambda;
+        // The reference always computes the principal stresses; they only
+        // matter when the tet yields.  A tet that provably stays inside the
+        // yield surface keeps its trial stress without the eigen-solve.
+        if (!surely_elastic(st, cohesion, anphi, stc)) {
+            principal_stresses(st, sp, cn);
+            mc_return_map(sp, cn, st, eps_p, cohesion, hardening, anphi, anpsi, stc, a1, a2);
+        }
+    }
+
+    // trace averaging over the 10 tets, Stress.c:87-137
+    double traceS = (st[0] + st[1] + st[2]) / 3.0f;
+    double partialS = 0.0f;
+#pragma unroll
+    for (int u = 0; u < NT; u++) partialS += grp(traceS, s.base, u) * grp(g.V, s.base, u);
+    const double avgTrace = partialS / elemVolume;
+    double cs2 = -1.0f * traceS + avgTrace;
+    st[0] += cs2;
+    st[1] += cs2;
+    st[2] += cs2;
+
+    if (cfg.has_density) {
+        // Stress.c:125-170: pressure = mean tet trace/3, density update
+        double ptet = (st[0] + st[1] + st[2]) / 3.0f;
+        double pressure = 0.0f;
+#pragma unroll
+        for (int u = 0; u < NT; u++) pressure += grp(ptet, s.base, u);
+        pressure /= NT;
+        double avgT = 0.0;
+        if (cfg.temperature) {
+            // UpdateAverageTemp_LoopElements (Heat.c:143-172) ran before the
+            // temperature BCs were re-applied: use the pre-BC temperatures
+            avgT = 0.0;
+            for (int qn = 0; qn < 4; qn++) {
+                long long n = s.active ? corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn)) : 0;
+                avgT += F.tpre[n] / (1.0f * 4);
+            }
+        }
+        if (s.active) F.density[s.q] = M.density * (1.0 - M.alpha * (avgT - M.reftemp) + M.beta * pressure);
+    }
+
+    if (s.active) {
+        bool ok = true;
+#pragma unroll
+        for (int a = 0; a < 6; a++) {
+            F.stress[s.q * 6 + a] = st[a];
+            ok = ok && isfinite(st[a]);
+        }
+        if (!ok) report(F.sc, SNAC_GPU_ENAN, s.e);  // Stress.c:161-166
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC) F.eps_p[s.q] = eps_p;
+        if (PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC || (PLUGIN == SNAC_RHEOLOGY_MAXWELL && ph == 0)) F.visc[s.q] = eta;
+    }
+}
+
+// ======================================================================================
+// Snac_EP_LoopElementsMomentum: UpdateElement.c:54-269 and the minLengthScale
+// reduction of _Snac_Context_LoopElements (Context.c:1156-1184)
+// ======================================================================================
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32) k_update_elements(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    const double dt = F.sc->dt;
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    double ls = 1.0e+27f;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        double l = g.A[f];
+        if (l) {
+            l = fabs(g.V / l);
+            if (ls > l) ls = l;
+        }
+    }
+    if (!s.active) ls = 1.0e+27f;
+    if (s.active && g.V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, s.e);
+    if (PLUGIN == SNAC_RHEOLOGY_MAXWELL && s.active) {
+        double vc = F.vol[s.q * 2 + 0];
+        F.vol[s.q * 2 + 1] = cfg.time_step_zero ? g.V : vc;
+        F.vol[s.q * 2 + 0] = g.V;
+    }
+    if (s.active) {
+        double st[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+        rotate_stress(v, g, dt, st);
+#pragma unroll
+        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
+    }
+    // global minimum (exact: min does not round)
+    for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
+}
+
+// ======================================================================================
+// Snac_EP_LoopNodesMomentum: Snac_Force (Force.c:53-188), then
+// Snac_UpdateNodeMomentum_PreProcess (UpdateNode.c:74-158) and
+// Snac_UpdateNodeMomentum (UpdateNode.c:60-72) for every node.  Coordinates
+// are read from pos and written to pos_next, so every force sees the old
+// geometry, as in the reference where all forces are summed before any node moves.
+// ======================================================================================
+template <int DTTYPE>
+__global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool active = n < m.nn;
+    double vcand = 0.0;
+    if (active) {
+        const double dt = F.sc->dt;
+        const double sos = F.sc->speed_of_sound;
+        int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
+        const double factor4 = 1.0f / 4.0f;
+        double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
+#pragma unroll
+        for (int ne = 0; ne < 8; ne++) {
+            int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
+            if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
+            long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
+            const DevMaterial& M = F.mats[phase_of(F, e)];
+            const double inertialDensity = (M.lambda + 2.0f * M.mu) / (sos * sos);
+            V3 corner[8];
+#pragma unroll
+            for (int cc = 0; cc < 8; cc++) {
+                double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
+                corner[cc] = {p.x, p.y, p.z};
+            }
+#pragma unroll
+            for (int idx = 0; idx < 5; idx++) {
+                const int t = node_tet(ne, idx);
+                const int f = node_face(ne, idx);
+                V3 tc[4];
+#pragma unroll
+                for (int qn = 0; qn < 4; qn++) tc[qn] = corner[tet_node(t, qn)];
+                double V = tet_volume(tc[0], tc[1], tc[2], tc[3]);
+                double A;
+                V3 nr;
+                tet_face(tc[face_node(f, 0)], tc[face_node(f, 1)], tc[face_node(f, 2)], A, nr);
+                const long long q = e * NT + t;
+                const double* sq = F.stress + q * 6;
+                double s00 = sq[0], s11 = sq[1], s22 = sq[2], s01 = sq[3], s02 = sq[4], s12 = sq[5];
+                const double effDensity = cfg.has_density ? F.density[q] : M.density;
+                if (DTTYPE == SNAC_DT_DYNAMIC) {
+                    imass += factor4 * inertialDensity * V;
+                } else if (DTTYPE == SNAC_DT_CONSTANT) {
+                    double alpha1 = (M.lambda + 2.0f * M.mu), area_sum = 0.0, temp;
+                    temp = (nr.x * A) * (nr.x * A);
+                    if (temp > area_sum) area_sum = temp;
+                    temp = (nr.y * A) * (nr.y * A);
+                    if (temp > area_sum) area_sum = temp;
+                    temp = (nr.z * A) * (nr.z * A);
+                    if (temp > area_sum) area_sum = temp;
+                    imass += alpha1 * area_sum / (9.0f * V) * (dt * dt);
+                } else {
+                    imass += factor4 * effDensity * V;
+                }
+                fx += (s00 * nr.x + s01 * nr.y + s02 * nr.z) * A / 6.0f;
+                fy += (s01 * nr.x + s11 * nr.y + s12 * nr.z) * A / 6.0f;
+                fz += (s02 * nr.x + s12 * nr.y + s22 * nr.z) * A / 6.0f;
+                fy -= cfg.gravity * effDensity * V / 8.0f;
+            }
+        }
+        // FLAC local damping with the pre-update velocity, then v and x
+        double4 w = F.vel[n];
+        const double demf = cfg.demf;
+        auto sgn = [](double x) { return x < 0 ? -1.0f : x > 0 ? +1.0f : 0.0f; };
+        fx -= demf * sgn(w.x) * fabs(fx);
+        fy -= demf * sgn(w.y) * fabs(fy);
+        fz -= demf * sgn(w.z) * fabs(fz);
+        w.x += dt * fx / imass;
+        w.y += dt * fy / imass;
+        w.z += dt * fz / imass;
+        uchar4 b = F.bc[n];
+        if (b.x != 255) w.x = F.vbc_val[b.x * 3 + 0];
+        if (b.y != 255) w.y = F.vbc_val[b.y * 3 + 1];
+        if (b.z != 255) w.z = F.vbc_val[b.z * 3 + 2];
+        double4 p = F.pos[n];
+        p.x += dt * w.x;
+        p.y += dt * w.y;
+        p.z += dt * w.z;
+        F.pos_next[n] = p;
+        F.vel[n] = w;
+        F.force[n] = make_double4(fx, fy, fz, imass);
+        if (!(isfinite(w.x) && isfinite(w.y) && isfinite(w.z))) report(F.sc, SNAC_GPU_ENAN, n);
+        if (b.x != 255 || b.y != 255 || b.z != 255) vcand = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
+    }
+    // max |v| over velocity-BC nodes for Sync (exact: max does not round)
+    for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
+    if ((threadIdx.x & 31) == 0 && vcand > 0.0)
+        atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
+}
+
+// ======================================================================================
+// Snac_EP_LoopElementsEnergy: Snac_HeatFlux (temperature/HeatFlux.c:60-200) and
+// SnacTemperature_HeatFluxBC (temperature/VariableConditions.c:280-413)
+// ======================================================================================
+__global__ void __launch_bounds__(ELEM_WARPS * 32) k_heat_flux(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
+    double q[3], tsr = 0.0;
+    for (int d = 0; d < 3; d++)
+        q[d] = 1.0f * M.thermal_conduct *
+               (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
+                T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0]) /
+               3.0f / g.V;
+    if (cfg.thermal_stress) {
+        const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+        double temp = 0.25f * (T[0] + T[1] + T[2] + T[3]);
+        double temp0 = 0.25f * (T0[0] + T0[1] + T0[2] + T0[3]);
+        tsr = -1.0f * M.alpha * bulkm * (temp - temp0);
+    }
+    // flux BC on the x and z walls: remove the wall-normal part of grad T
+    double nrm[4][3];
+    // (tet, face) pairs averaged for each wall, VariableConditions.c:311-367
+    const int W[4][4][2] = {{{0, 2}, {1, 2}, {5, 0}, {6, 0}},
+                            {{2, 0}, {3, 0}, {7, 0}, {8, 0}},
+                            {{0, 1}, {2, 2}, {6, 1}, {7, 1}},
+                            {{1, 1}, {3, 2}, {5, 1}, {8, 1}}};
+#pragma unroll
+    for (int w = 0; w < 4; w++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double a[4];
+#pragma unroll
+            for (int r = 0; r < 4; r++) {
+                const int f = W[w][r][1];
+                double val = f == 0 ? comp(g.n[0], d) : f == 1 ? comp(g.n[1], d) : f == 2 ? comp(g.n[2], d) : comp(g.n[3], d);
+                a[r] = __shfl_sync(FULL, val, s.base + W[w][r][0]);
+            }
+            nrm[w][d] = 0.25f * (a[0] + a[1] + a[2] + a[3]);
+        }
+    if (s.active && (s.i == 0 || s.i == m.nx - 1 || s.k == 0 || s.k == m.nz - 1)) {
+        double normal[3];
+        if (s.i == 0)
+            for (int d = 0; d < 3; d++) normal[d] = nrm[0][d];
+        if (s.i == m.nx - 1)
+            for (int d = 0; d < 3; d++) normal[d] = nrm[1][d];
+        if (s.k == 0)
+            for (int d = 0; d < 3; d++) normal[d] = nrm[2][d];
+        if (s.k == m.nz - 1)
+            for (int d = 0; d < 3; d++) normal[d] = nrm[3][d];
+        double gd[3];
+        for (int d = 0; d < 3; d++)
+            gd[d] = -1.0f *
+                    (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
+                     T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0]) /
+                    3.0f / g.V;
+        double Fn = 0.0f;
+        for (int d = 0; d < 3; d++) Fn += gd[d] * normal[d];
+        for (int d = 0; d < 3; d++) q[d] -= Fn * normal[d];
+    }
+    if (s.active) {
+        double* h = F.hflux + s.q * 4;
+        h[0] = q[0];
+        h[1] = q[1];
+        h[2] = q[2];
+        if (cfg.thermal_stress) h[3] = tsr;
+    }
+}
+
+// ======================================================================================
+// Snac_EP_LoopNodesEnergy: Snac_Heat for every node (temperature/Heat.c:64-140),
+// the tet mean temperatures and the temperature BCs (Heat.c:47-62)
+// ======================================================================================
+__global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= m.nn) return;
+    const double dt = F.sc->dt;
+    const double minLS = F.sc->min_length_scale;
+    int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
+    double energy = 0.0f, source = 0.0f, lumpVolume = 0.0f;
+    const double sourceterm = 0.0;
+#pragma unroll
+    for (int ne = 0; ne < 8; ne++) {
+        int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
+        if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
+        long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
+        const DevMaterial& M = F.mats[phase_of(F, e)];
+        V3 corner[8];
+#pragma unroll
+        for (int cc = 0; cc < 8; cc++) {
+            double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
+            corner[cc] = {p.x, p.y, p.z};
+        }
+#pragma unroll
+        for (int idx = 0; idx < 5; idx++) {
+            const int t = node_tet(ne, idx);
+            const int f = node_face(ne, idx);
+            V3 tc[4];
+#pragma unroll
+            for (int qn = 0; qn < 4; qn++) tc[qn] = corner[tet_node(t, qn)];
+            double V = tet_volume(tc[0], tc[1], tc[2], tc[3]);
+            double A;
+            V3 nr;
+            tet_face(tc[face_node(f, 0)], tc[face_node(f, 1)], tc[face_node(f, 2)], A, nr);
+            const long long q = e * NT + t;
+            const double* h = F.hflux + q * 4;
+            energy += (h[0] * nr.x + h[1] * nr.y + h[2] * nr.z) * A / 6.0f;
+            source += sourceterm * V / 4.0f;
+            // tetra density is set from TimeStepZero on, so the reference's
+            // "density == 0" fallback (Heat.c:120-125) is never taken
+            double rho = cfg.has_density ? F.density[q] : M.density;
+            lumpVolume += M.heat_capacity * ((rho)*V) / 8.0f;
+        }
+        double dt_thermal_to_mech = sqrt((M.lambda + 2.0f * M.mu) / M.density) * minLS /
+                                    (M.thermal_conduct / (M.heat_capacity * M.density));
+        if (!(dt_thermal_to_mech > 1.0)) report(F.sc, SNAC_GPU_EPHYSICS, n);
+    }
+    // only the w slots are written: other threads read this node's x, y, z
+    double* pw = reinterpret_cast<double*>(const_cast<double4*>(F.pos) + n) + 3;
+    double Told = *pw;
+    double Tnew = Told + (energy + source) * -1.0f * dt / lumpVolume;
+    if (F.tpre) F.tpre[n] = Tnew;
+    uchar4 b = F.bc[n];
+    if (b.w != 255) Tnew = F.tbc_val[b.w];
+    reinterpret_cast<double*>(F.vel + n)[3] = Told;
+    *pw = Tnew;
+    if (!isfinite(Tnew)) report(F.sc, SNAC_GPU_ENAN, n);
+}
+
+// ======================================================================================
+// AbstractContext_EP_Sync: _Snac_Context_Sync (Context.c:1208-1268), one thread
+// ======================================================================================
+__global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double vmax = __longlong_as_double((long long)sc->vmax_bits);
+    const double vlb = 3.0e-11f;
+    if (vmax < vlb) vmax = vlb;
+    sc->vmax = vmax;
+    double minLS = __longlong_as_double((long long)sc->minls_bits);
+    sc->min_length_scale = minLS;
+    if (sc->time_step == 0) sc->init_min_length_scale = minLS;
+    if (cfg.dt_type == SNAC_DT_DYNAMIC) {
+        sc->dt = minLS * 0.45f * cfg.strain_inert / vmax;
+        sc->speed_of_sound = minLS * 0.5f / sc->dt;
+    } else if (cfg.dt_type == SNAC_DT_WAVE) {
+        sc->speed_of_sound = wave_speed;
+        sc->dt = 0.5f * minLS / sc->speed_of_sound;
+    }
+    sc->vmax_bits = 0ull;
+    sc->minls_bits = 0x7ff0000000000000ull;  // +inf
+}
+
+// max |v| over the velocity-BC nodes from the current velocities, for a
+// Sync that does not follow the node loop (step zero, hook-by-hook callers)
+__global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double vcand = 0.0;
+    if (n < m.nn) {
+        uchar4 b = F.bc[n];
+        if (b.x != 255 || b.y != 255 || b.z != 255) {
+            double4 w = F.vel[n];
+            vcand = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
+    if ((threadIdx.x & 31) == 0 && vcand > 0.0)
+        atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
+}
+
+// _AbstractContext_Execute_Hook: timeStep++ and dt = dtFactor * dt (AbstractContext.c:874-890)
+__global__ void k_begin_step(DevScalars* sc) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        sc->time_step += 1;
+        sc->dt = 1.0 * sc->dt;
+    }
+}
+
+}  // namespace snac

@@ -1,0 +1,246 @@
+"""The CUDA path against the CPU oracle, through the C ABI.
+
+Elastic and constant-friction plastic runs must agree with the oracle to the
+last bit (the kernels keep the reference's operation order, without FMA
+contraction; sin/tan of a constant friction angle come from the host C
+library).  Runs that evaluate pow/exp on the device (visco-plastic, Maxwell)
+are compared with a normwise relative tolerance: max|gpu - cpu| / max|cpu|
+per field <= 1e-9 (elastic bar of the target) or <= 1e-6 (plastic bar).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle.pyoracle import Checker
+from snac_b200 import workloads as W
+from snac_b200.abi import State
+from snac_b200.context import SnacContext, SnacError
+from tests import scenarios as S
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("coord", "velocity", "stress", "plastic_strain", "viscosity", "temperature", "force", "inertial_mass")
+
+
+def relerr(a, b):
+    den = np.max(np.abs(b))
+    return float(np.max(np.abs(a - b)) / den) if den > 0 else float(np.max(np.abs(a - b)))
+
+
+def run_both(cfg, steps, chunks=1):
+    g = SnacContext(cfg)
+    c = Checker(cfg, "port")
+    g.time_step_zero()
+    c.time_step_zero()
+    for _ in range(chunks):
+        g.step(steps // chunks)
+        c.step(steps // chunks)
+    return g, c
+
+
+def assert_bitwise(g, c):
+    sg, sc = g.state(), c.state()
+    for f in FIELDS:
+        x, y = getattr(sg, f), getattr(sc, f)
+        assert np.array_equal(x, y), (f, relerr(x, y), int(np.sum(x != y)))
+    a, b = g.scalars(), c.scalars()
+    assert a.dt == b.dt and a.min_length_scale == b.min_length_scale and a.vmax == b.vmax
+    assert a.time_step == b.time_step
+
+
+@pytest.mark.parametrize("case", ["elastic", "plastic", "lithostatic"])
+def test_bitwise_equal_to_oracle(case):
+    make, steps = S.CASES[case]
+    g, c = run_both(make(), steps, chunks=2)
+    assert_bitwise(g, c)
+
+
+def test_plastic_case_yields_on_gpu():
+    make, steps = S.CASES["plastic"]
+    g = SnacContext(make())
+    g.time_step_zero()
+    g.step(steps)
+    assert np.count_nonzero(g.state().plastic_strain) > 100
+
+
+# pow/exp on the device differ from the host libm in the last bit; through the
+# yield branch the difference stays far below the plastic bar (1e-6), and
+# without plasticity (Maxwell) below the elastic bar (1e-9).
+@pytest.mark.parametrize("case,tol", [("viscoplastic", 1e-6), ("maxwell", 1e-9), ("density", 1e-6)])
+def test_device_transcendentals_within_tolerance(case, tol):
+    make, steps = S.CASES[case]
+    g, c = run_both(make(), steps)
+    sg, sc = g.state(), c.state()
+    for f in ("velocity", "stress", "plastic_strain", "viscosity", "temperature", "coord"):
+        e = relerr(getattr(sg, f), getattr(sc, f))
+        assert e <= tol, (case, f, e)
+
+
+def test_elastic_c1_full_1000_steps():
+    """configs[0] in full: 16 x 8 x 16 hex, 1000 elastic steps."""
+    g, c = run_both(W.c1_elastic(), 1000)
+    sg, sc = g.state(), c.state()
+    assert relerr(sg.velocity, sc.velocity) <= 1e-9
+    assert relerr(sg.stress, sc.stress) <= 1e-9
+    assert np.array_equal(sg.velocity, sc.velocity) and np.array_equal(sg.stress, sc.stress)
+
+
+@pytest.mark.parametrize("dt_type", ["constant", "wave"])
+def test_other_dt_types_bitwise(dt_type):
+    cfg = S.elastic_small(6, 4, 6)
+    if dt_type == "constant":
+        S.constant_dt(cfg, 2.0e7)
+    else:
+        cfg.dtType = "wave"
+    g, c = run_both(cfg, 30)
+    assert_bitwise(g, c)
+
+
+def test_hook_by_hook_equals_graph_step():
+    """the loop-level entry points a plugin would call give the same bits as
+    the graph-captured step"""
+    make, steps = S.CASES["viscoplastic"]
+    a = SnacContext(make())
+    b = SnacContext(make())
+    a.time_step_zero()
+    b.time_step_zero()
+    a.step(10)
+    for _ in range(10):
+        b.solve()
+    sa, sb = a.state(), b.state()
+    for f in FIELDS:
+        assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
+
+
+def test_run_to_run_bit_reproducible():
+    make, steps = S.CASES["plastic"]
+    out = []
+    for _ in range(2):
+        g = SnacContext(make())
+        g.time_step_zero()
+        g.step(steps)
+        out.append(g.state())
+    for f in FIELDS:
+        assert np.array_equal(getattr(out[0], f), getattr(out[1], f)), f
+
+
+def test_pull_test_known_answer_on_gpu():
+    """testUpdateNode-velocity-4-4-4: 10 hook-by-hook iterations of the unit cube."""
+    cfg = W.libsnac_unit_cube()
+    g = SnacContext(cfg)
+    c = Checker(cfg)
+    g.time_step_zero()
+    c.time_step_zero()
+    S.pull_test_10(g)
+    S.pull_test_10(c)
+    v = g.state().velocity
+    assert np.array_equal(v, c.state().velocity)
+    for n in (1, 4, 13, 25):
+        assert abs(v[n, 0] - 0.00834447) <= 5e-6 * 0.00834447
+
+
+def test_upload_download_roundtrip():
+    cfg = S.plastic_small()
+    g = SnacContext(cfg)
+    g.time_step_zero()
+    g.step(20)
+    s = g.state()
+    h = SnacContext(cfg)
+    h.time_step_zero()
+    h.set_state(s, ["coord", "velocity", "stress", "plastic_strain"])
+    s2 = h.state()
+    for f in ("coord", "velocity", "stress", "plastic_strain"):
+        assert np.array_equal(getattr(s, f), getattr(s2, f)), f
+
+
+# ---- failure detection: every fault is made on the host, none on the GPU ----------------
+
+def test_nan_velocity_is_reported_with_its_node():
+    cfg = S.elastic_small(4, 2, 4)
+    v = np.zeros((cfg.n_nodes, 3))
+    v[7, 1] = float("nan")
+    cfg.init_velocity = v.reshape(-1)
+    g = SnacContext(cfg)
+    g.time_step_zero()
+    with pytest.raises(SnacError) as ei:
+        g.step(3)
+    assert ei.value.code in (-4,)  # ENAN
+    assert ei.value.index >= 0
+
+
+def test_collapsed_element_is_reported():
+    cfg = S.elastic_small(4, 2, 4)
+    nnx, nny = 5, 3
+    coords = np.zeros((cfg.n_nodes, 3))
+    for n in range(cfg.n_nodes):
+        i, j, k = n % nnx, (n // nnx) % nny, n // (nnx * nny)
+        coords[n] = (i * 1000.0, -2000.0 + j * 1000.0, k * 1000.0)
+    coords[1 + 1 * nnx + 1 * nnx * nny] = coords[0 + 0 * nnx + 0 * nnx * nny]  # fold element 0
+    cfg.node_coords = coords.reshape(-1)
+    g = SnacContext(cfg)
+    with pytest.raises(SnacError) as ei:
+        g.time_step_zero()
+    assert ei.value.code == -5  # EVOLUME
+
+
+def test_bad_phase_index_is_rejected_at_create():
+    cfg = S.elastic_small(4, 2, 4)
+    cfg.element_material = np.full(cfg.n_elements, 3, dtype=np.int32)
+    with pytest.raises(SnacError) as ei:
+        SnacContext(cfg)
+    assert ei.value.code in (-6, -1)
+
+
+def test_negative_friction_angle_is_reported():
+    cfg = S.plastic_small(4, 2, 4)
+    m = W.mc_phase(phi=-5.0)
+    cfg.materials = [m]
+    g = SnacContext(cfg)
+    g.time_step_zero()
+    with pytest.raises(SnacError) as ei:
+        g.step(2)
+    assert ei.value.code == -7  # EPHYSICS (the reference calls abort())
+
+
+def test_step_before_step_zero_is_refused():
+    g = SnacContext(S.elastic_small(2, 2, 2))
+    with pytest.raises(SnacError) as ei:
+        g.step(1)
+    assert ei.value.code == -10
+
+
+# ---- full-size configurations: bounded CPU comparisons and size-free properties ------------
+
+def test_c2_full_size_first_steps_bitwise():
+    """configs[1] at full size (64 x 32 x 64): three steps against the oracle."""
+    g, c = run_both(W.c2_plastic(), 3)
+    assert_bitwise(g, c)
+
+
+def test_c3_full_size_first_step_within_tolerance():
+    """configs[2] at full size (128 x 64 x 128, ~1M hex): one step against the oracle."""
+    g, c = run_both(W.c3_viscoplastic(), 1)
+    sg, sc = g.state(), c.state()
+    for f in ("velocity", "stress", "viscosity", "temperature"):
+        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, f
+
+
+def test_full_size_c3_bit_reproducible_and_hooks_match():
+    """configs[2] at full size: two graph runs agree to the bit, and the
+    hook-by-hook path gives the same bits as the graph path"""
+    cfg = W.c3_viscoplastic()
+    runs = []
+    for mode in ("graph", "graph", "hooks"):
+        g = SnacContext(cfg)
+        g.time_step_zero()
+        if mode == "graph":
+            g.step(3)
+        else:
+            for _ in range(3):
+                g.solve()
+        runs.append(g.state())
+        g.close()
+    for f in ("velocity", "stress", "plastic_strain", "viscosity", "temperature"):
+        assert np.array_equal(getattr(runs[0], f), getattr(runs[1], f)), f
+        assert np.array_equal(getattr(runs[0], f), getattr(runs[2], f)), f

@@ -1,0 +1,65 @@
+"""The plain-C restatement against the reference's own hot-path sources,
+compiled here from the SNAC tree against oracle/refshim (oracle/_ref).
+Every field must agree to the last bit, for every rheology and IC path."""
+import os
+
+import numpy as np
+import pytest
+
+from oracle import pyoracle
+from tests import scenarios as S
+
+REF_TREE = "/root/reference/Snac"
+
+
+def _reference_available():
+    if pyoracle.available("reference"):
+        return True
+    if os.path.isdir(REF_TREE):
+        try:
+            pyoracle.build("reference")
+            return True
+        except Exception:
+            return False
+    return False
+
+
+pytestmark = pytest.mark.skipif(not _reference_available(), reason="reference checker not built (no SNAC tree)")
+
+FIELDS = ("coord", "velocity", "stress", "plastic_strain", "viscosity", "temperature", "force", "inertial_mass")
+
+
+@pytest.mark.parametrize("case", sorted(S.CASES))
+def test_restatement_is_bitwise_equal_to_reference(case):
+    make, steps = S.CASES[case]
+    cfg = make()
+    a = pyoracle.Checker(cfg, "port")
+    b = pyoracle.Checker(cfg, "reference")
+    assert a.time_step_zero() == 0 and b.time_step_zero() == 0
+    for _ in range(2):
+        a.step(steps // 2)
+        b.step(steps // 2)
+        sa, sb = a.state(), b.state()
+        for f in FIELDS:
+            x, y = getattr(sa, f), getattr(sb, f)
+            assert np.array_equal(x, y), (case, f, np.max(np.abs(x - y)))
+        assert a.scalars().dt == b.scalars().dt
+        assert a.scalars().min_length_scale == b.scalars().min_length_scale
+
+
+def test_plastic_case_actually_yields():
+    a = pyoracle.Checker(S.plastic_small(), "port")
+    a.time_step_zero()
+    a.step(S.CASES["plastic"][1])
+    assert np.count_nonzero(a.state().plastic_strain) > 100
+
+
+def test_pull_test_bitwise():
+    from snac_b200 import workloads as W
+    a = pyoracle.Checker(W.libsnac_unit_cube(), "port")
+    b = pyoracle.Checker(W.libsnac_unit_cube(), "reference")
+    a.time_step_zero()
+    b.time_step_zero()
+    S.pull_test_10(a)
+    S.pull_test_10(b)
+    assert np.array_equal(a.state().velocity, b.state().velocity)
