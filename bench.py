@@ -254,25 +254,15 @@ def run_ours(args, ws, rank, local):
     t_max = allmax(ws, t_dev)
     value = ws * ne * args.steps / t_max
 
-    # ---- per-kernel breakdown (hook by hook, events on the library stream) -------------
+    # ---- per-kernel breakdown: one step kernel by kernel, events on the library stream -----
     kern = {}
-    hooks = [("k_heat_flux", ctx.loop_elements_energy), ("k_heat_nodes", ctx.loop_nodes_energy),
-             ("k_calc_stresses", ctx.calc_stresses), ("k_loop_nodes", ctx.loop_nodes_momentum),
-             ("k_update_elements", ctx.loop_elements_momentum), ("k_sync", ctx.sync)]
     nb = max(3, min(10, args.steps))
     for _ in range(nb):
-        ctx.begin_step()
-        for name, fn in hooks:
-            with torch.cuda.stream(stream):
-                flush.fill_(1.0)
-                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-                a.record(stream)
-            fn()
-            with torch.cuda.stream(stream):
-                b.record(stream)
-            torch.cuda.synchronize()
-            kern.setdefault(name, []).append(a.elapsed_time(b))
-    kern_ms = {k: statistics.mean(v) for k, v in kern.items() if not (k.startswith("k_heat") and not cfg.temperature)}
+        with torch.cuda.stream(stream):
+            flush.fill_(1.0)
+        for name, ms in ctx.profile_step():
+            kern.setdefault(name, []).append(ms)
+    kern_ms = {k: statistics.mean(v) for k, v in kern.items()}
     top = max(kern_ms, key=kern_ms.get)
     peak, peak_kind = load_peaks()
     alg = algorithmic_bytes(args.workload)
@@ -348,6 +338,8 @@ def run_ours(args, ws, rank, local):
 
 # Algorithmic bytes per hex of one launch of each kernel (state it must read / write once).
 KERNEL_BYTES = {
+    "k_fused_step": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0),
+    "k_fused_heat": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + 8.0 * NODES_PER_HEX[w],
     "k_calc_stresses": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
                                  + (8.0 * NODES_PER_HEX[w] if w == "c3" else 0.0),
     "k_loop_nodes": lambda w: 480.0 + 96.0 * NODES_PER_HEX[w],

@@ -208,6 +208,18 @@ int  snac_gpu_download(snac_gpu* h, const snac_state_view* v);
 int  snac_gpu_scalars(snac_gpu* h, snac_scalars* out);
 int  snac_gpu_set_dt(snac_gpu* h, double dt);   /* _Snac_Context_SetDt, Context.c:1047-1053 */
 
+/* ---- profiling ---------------------------------------------------------------- */
+/* One step launched kernel by kernel (no graph), with CUDA events recorded
+ * around every launch on the handle's stream: names[i] / ms[i] for the
+ * kernels of the step, in launch order.  Returns the number of kernels
+ * (<= max) or a negative status.  The step advances the model like
+ * snac_gpu_step(h, 1). */
+typedef struct snac_kernel_time {
+    char   name[40];
+    double ms;
+} snac_kernel_time;
+int  snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max);
+
 /* ---- errors / introspection ------------------------------------------------ */
 const char* snac_gpu_last_error(const snac_gpu* h);
 long long   snac_gpu_error_index(const snac_gpu* h);   /* element/node id, -1 if none */

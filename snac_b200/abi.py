@@ -114,6 +114,10 @@ class StateView(C.Structure):
                 ("viscosity", _DP), ("temperature", _DP), ("force", _DP), ("inertial_mass", _DP)]
 
 
+class KernelTime(C.Structure):
+    _fields_ = [("name", C.c_char * 40), ("ms", C.c_double)]
+
+
 class Scalars(C.Structure):
     _fields_ = [("dt", C.c_double), ("min_length_scale", C.c_double), ("vmax", C.c_double),
                 ("speed_of_sound", C.c_double), ("time_step", C.c_longlong)]

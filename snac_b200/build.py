@@ -40,18 +40,18 @@ def stale() -> bool:
     return any(os.path.getmtime(s) > t for s in sources())
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    if not force and not stale():
+def build(force: bool = False, verbose: bool = False, defines=(), out: str = LIB) -> str:
+    if not force and not stale() and out == LIB:
         return LIB
-    cmd = [nvcc(), *ARCH, "-lineinfo", "-O3", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
-           "-shared", "-I" + os.path.join(ROOT, "include"), "-o", LIB + ".tmp",
+    cmd = [nvcc(), *ARCH, *["-D" + d for d in defines], "-lineinfo", "-O3", "-fmad=false", "-std=c++17", "-Xcompiler", "-fPIC,-O2",
+           "-shared", "-I" + os.path.join(ROOT, "include"), "-o", out + ".tmp",
            os.path.join(CSRC, "snac_api.cu")]
     if verbose:
         cmd.insert(1, "-Xptxas=-v")
         print(" ".join(cmd))
     subprocess.run(cmd, check=True)
-    os.replace(LIB + ".tmp", LIB)
-    return LIB
+    os.replace(out + ".tmp", out)
+    return out
 
 
 def ensure_built() -> str:

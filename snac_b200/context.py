@@ -14,7 +14,7 @@ import ctypes as C
 import os
 from typing import Optional
 
-from .abi import NT, STATUS_NAMES, Desc, Scalars, SnacConfig, State, StateView
+from .abi import NT, STATUS_NAMES, Desc, KernelTime, Scalars, SnacConfig, State, StateView
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsnac_b200.so")
@@ -68,6 +68,8 @@ def load_library(path: str = LIB_PATH):
     lib.snac_gpu_launch_count.restype = C.c_longlong
     lib.snac_gpu_stream.argtypes = [vp]
     lib.snac_gpu_stream.restype = vp
+    lib.snac_gpu_profile_step.argtypes = [vp, C.POINTER(KernelTime), C.c_int]
+    lib.snac_gpu_profile_step.restype = C.c_int
     lib.snac_gpu_device_count.argtypes = []
     lib.snac_gpu_device_count.restype = C.c_int
     _LIB = lib
@@ -170,6 +172,14 @@ class SnacContext:
 
     def set_dt(self, dt: float):
         self._check(self.lib.snac_gpu_set_dt(self.h, C.c_double(dt)))
+
+    def profile_step(self):
+        """One step kernel by kernel with CUDA events: [(kernel name, ms)]."""
+        buf = (KernelTime * 32)()
+        n = self.lib.snac_gpu_profile_step(self.h, buf, 32)
+        if n < 0:
+            self._check(n)
+        return [(buf[i].name.decode(), buf[i].ms) for i in range(n)]
 
     @property
     def launches(self) -> int:

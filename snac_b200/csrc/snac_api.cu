@@ -40,6 +40,9 @@ struct snac_gpu {
     double* vol = nullptr;
     double* hflux = nullptr;
     double* tpre = nullptr;
+    double* fterm = nullptr;
+    double* fgrav = nullptr;
+    double* fmass = nullptr;
     uchar4* bc = nullptr;
     double* vbc_val = nullptr;
     double* tbc_val = nullptr;
@@ -53,9 +56,14 @@ struct snac_gpu {
     int parity = 0;
     long long time_step = 0;
     bool zero_done = false;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [fused][parity]
+    bool pending = false;  // the element update of the last step is deferred into the next kernel
+    // kernel-by-kernel timing (snac_gpu_profile_step)
+    snac_kernel_time* prof = nullptr;
+    int prof_n = 0, prof_max = 0;
+    cudaEvent_t prof_ev[64];
     long long launches = 0;
-    int kernels_per_step = 0;
+    int steps_kernels[2] = {0, 0};
     char err[512] = {0};
     long long err_index = -1;
 };
@@ -158,6 +166,9 @@ Fields fields(snac_gpu* h) {
     F.vol = h->vol;
     F.hflux = h->hflux;
     F.tpre = h->tpre;
+    F.fterm = h->fterm;
+    F.fgrav = h->fgrav;
+    F.fmass = h->fmass;
     F.bc = h->bc;
     F.vbc_val = h->vbc_val;
     F.tbc_val = h->tbc_val;
@@ -173,33 +184,49 @@ Fields fields(snac_gpu* h) {
 unsigned elem_blocks(const Mesh& m) { return (unsigned)((m.ne + ELEM_PER_BLOCK - 1) / ELEM_PER_BLOCK); }
 unsigned node_blocks(const Mesh& m) { return (unsigned)((m.nn + 127) / 128); }
 
-int launch_check(snac_gpu* h) {
+// called right after each launch: checks it and, when profiling, records an
+// event behind it (the event before the first launch is recorded by the caller)
+int launch_check_named(snac_gpu* h, const char* name) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "kernel launch: %s", cudaGetErrorString(e));
+    if (h->prof && h->prof_n < h->prof_max && h->prof_n < 63) {
+        cudaEventRecord(h->prof_ev[h->prof_n + 1], h->stream);
+        snprintf(h->prof[h->prof_n].name, sizeof h->prof[h->prof_n].name, "%s", name);
+        h->prof_n++;
+    }
     return 0;
 }
+#define launch_check(h) launch_check_named((h), __func__)
 
 template <int P>
 void launch_stress(snac_gpu* h, const Fields& F, const Config& c) {
     k_calc_stresses<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
 template <int P>
-void launch_update(snac_gpu* h, const Fields& F, const Config& c) {
-    k_update_elements<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+void launch_update(snac_gpu* h, const Fields& F, const Config& c, int pending) {
+    k_update_elements<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c, pending);
+}
+template <int P>
+void launch_fused(snac_gpu* h, const Fields& F, const Config& c) {
+    k_fused_step<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+}
+template <int P>
+void launch_fused_heat(snac_gpu* h, const Fields& F, const Config& c) {
+    k_fused_heat<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
 
 int op_energy_elements(snac_gpu* h) {
     if (!h->temperature) return 0;
     k_heat_flux<<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
     h->launches++;
-    return launch_check(h);
+    return launch_check_named(h, "k_heat_flux");
 }
 
 int op_energy_nodes(snac_gpu* h) {
     if (!h->temperature) return 0;
     k_heat_nodes<<<node_blocks(h->mesh), 128, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
     h->launches++;
-    return launch_check(h);
+    return launch_check_named(h, "k_heat_nodes");
 }
 
 int op_calc_stresses(snac_gpu* h) {
@@ -211,7 +238,7 @@ int op_calc_stresses(snac_gpu* h) {
         case SNAC_RHEOLOGY_MAXWELL: launch_stress<SNAC_RHEOLOGY_MAXWELL>(h, F, h->cfg); break;
     }
     h->launches++;
-    return launch_check(h);
+    return launch_check_named(h, "k_calc_stresses");
 }
 
 int op_loop_nodes(snac_gpu* h) {
@@ -224,32 +251,61 @@ int op_loop_nodes(snac_gpu* h) {
     }
     h->launches++;
     h->parity ^= 1;  // the new coordinates are current from here on
-    return launch_check(h);
+    return launch_check_named(h, "k_loop_nodes");
 }
 
-int op_update_elements(snac_gpu* h, bool step_zero) {
+int op_update_elements(snac_gpu* h, bool step_zero, int pending = 0) {
     Fields F = fields(h);
     Config c = h->cfg;
     c.time_step_zero = step_zero ? 1 : 0;
     switch (h->constitutive) {
-        case SNAC_RHEOLOGY_MAXWELL: launch_update<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
-        default: launch_update<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_MAXWELL: launch_update<SNAC_RHEOLOGY_MAXWELL>(h, F, c, pending); break;
+        default: launch_update<SNAC_RHEOLOGY_ELASTIC>(h, F, c, pending); break;
     }
     h->launches++;
-    return launch_check(h);
+    return launch_check_named(h, "k_update_elements");
+}
+
+// the end of the previous step fused with the start of this one
+int op_fused(snac_gpu* h) {
+    Fields F = fields(h);
+    Config c = h->cfg;
+    c.time_step_zero = 0;
+    if (h->temperature) {
+        switch (h->constitutive) {
+            case SNAC_RHEOLOGY_MAXWELL: launch_fused_heat<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
+            default: launch_fused_heat<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
+        }
+    } else {
+        switch (h->constitutive) {
+            case SNAC_RHEOLOGY_ELASTIC: launch_fused<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
+            case SNAC_RHEOLOGY_PLASTIC: launch_fused<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
+            case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
+            case SNAC_RHEOLOGY_MAXWELL: launch_fused<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
+        }
+    }
+    h->launches++;
+    h->time_step++;
+    return launch_check_named(h, h->temperature ? "k_fused_heat" : "k_fused_step");
+}
+
+int op_min_length_scale(snac_gpu* h) {
+    k_min_length_scale<<<(unsigned)((h->mesh.ne * NT + 255) / 256), 256, 0, h->stream>>>(h->mesh, fields(h));
+    h->launches++;
+    return launch_check_named(h, "k_min_length_scale");
 }
 
 int op_sync(snac_gpu* h) {
     k_sync<<<1, 32, 0, h->stream>>>(h->cfg, h->sc, h->wave_speed);
     h->launches++;
-    return launch_check(h);
+    return launch_check_named(h, "k_sync");
 }
 
 // Sync when the node loop did not just reduce max |v| (step zero, hook by hook)
 int op_sync_full(snac_gpu* h) {
     k_vmax<<<(unsigned)((h->mesh.nn + 255) / 256), 256, 0, h->stream>>>(h->mesh, fields(h));
     h->launches++;
-    int rc = launch_check(h);
+    int rc = launch_check_named(h, "k_vmax");
     return rc ? rc : op_sync(h);
 }
 
@@ -257,18 +313,38 @@ int op_begin(snac_gpu* h) {
     k_begin_step<<<1, 32, 0, h->stream>>>(h->sc);
     h->launches++;
     h->time_step++;
-    return launch_check(h);
+    return launch_check_named(h, "k_begin_step");
 }
 
-int record_step(snac_gpu* h) {
+// One step as a chain of launches.  Element update of step n and the first
+// element kernel of step n+1 share one launch when the previous step's
+// update is pending (fused), otherwise the step starts from scratch.
+int record_step(snac_gpu* h, bool fused) {
     int rc;
-    if ((rc = op_begin(h))) return rc;
-    if ((rc = op_energy_elements(h))) return rc;
+    if (fused) {
+        if ((rc = op_fused(h))) return rc;
+    } else {
+        if ((rc = op_begin(h))) return rc;
+        if ((rc = op_energy_elements(h))) return rc;
+    }
     if ((rc = op_energy_nodes(h))) return rc;
-    if ((rc = op_calc_stresses(h))) return rc;
+    if (fused && !h->temperature) {
+        // stress already updated by the fused kernel
+    } else if ((rc = op_calc_stresses(h))) {
+        return rc;
+    }
     if ((rc = op_loop_nodes(h))) return rc;
-    if ((rc = op_update_elements(h, false))) return rc;
+    if ((rc = op_min_length_scale(h))) return rc;
     return op_sync(h);
+}
+
+// apply a deferred element update so that the state matches the reference's
+// end of step (before any transfer or hook-by-hook call)
+int flush_pending(snac_gpu* h) {
+    if (!h->pending) return 0;
+    int rc = op_update_elements(h, false, 1);
+    h->pending = false;
+    return rc;
 }
 
 int read_status(snac_gpu* h) {
@@ -391,7 +467,9 @@ int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
     int rc = 0;
     if ((rc = dalloc(h, &h->pos[0], nn)) || (rc = dalloc(h, &h->pos[1], nn)) || (rc = dalloc(h, &h->vel, nn)) ||
         (rc = dalloc(h, &h->force, nn)) || (rc = dalloc(h, &h->stress, nq * 6)) || (rc = dalloc(h, &h->bc, nn)) ||
-        (rc = dalloc(h, &h->sc, 1)) || (rc = dalloc(h, &h->mats, MAX_PHASES)))
+        (rc = dalloc(h, &h->sc, 1)) || (rc = dalloc(h, &h->mats, MAX_PHASES)) ||
+        (rc = dalloc(h, &h->fterm, nq * 12)) || (rc = dalloc(h, &h->fgrav, nq)) ||
+        (rc = dalloc(h, &h->fmass, d->dt_type == SNAC_DT_CONSTANT ? nq * 4 : nq)))
         return rc;
     if (d->constitutive == SNAC_RHEOLOGY_PLASTIC || d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC)
         if ((rc = dalloc(h, &h->eps_p, nq))) return rc;
@@ -529,10 +607,11 @@ int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
 void snac_gpu_destroy(snac_gpu* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (auto& g : h->graph)
-        if (g) cudaGraphExecDestroy(g);
+    for (auto& gf : h->graph)
+        for (auto& g : gf)
+            if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
-                    h->hflux, h->tpre, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
+                    h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
                     h->visc_scale, h->sc};
     for (void* b : bufs)
         if (b) cudaFree(b);
@@ -568,27 +647,27 @@ int snac_gpu_step(snac_gpu* h, int nsteps) {
     if (!h || nsteps < 0) return SNAC_GPU_EINVAL;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
     for (int s = 0; s < nsteps; s++) {
-        int p = h->parity;
-        if (!h->graph[p]) {
+        int p = h->parity, f = h->pending ? 1 : 0;
+        if (!h->graph[f][p]) {
             cudaGraph_t g;
-            long long l0 = h->launches;
-            long long ts0 = h->time_step;
+            long long l0 = h->launches, ts0 = h->time_step;
             CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            int rc = record_step(h);
+            int rc = record_step(h, f == 1);
             cudaError_t e = cudaStreamEndCapture(h->stream, &g);
             if (rc) return rc;
             if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "graph capture: %s", cudaGetErrorString(e));
-            CK(cudaGraphInstantiate(&h->graph[p], g, 0));
+            CK(cudaGraphInstantiate(&h->graph[f][p], g, 0));
             cudaGraphDestroy(g);
-            h->kernels_per_step = (int)(h->launches - l0);
+            h->steps_kernels[f] = (int)(h->launches - l0);
             h->launches = l0;  // counted again below, when the graph actually runs
             h->time_step = ts0;
             h->parity = p;
         }
-        CK(cudaGraphLaunch(h->graph[p], h->stream));
-        h->launches += h->kernels_per_step;
+        CK(cudaGraphLaunch(h->graph[f][p], h->stream));
+        h->launches += h->steps_kernels[f];
         h->time_step++;
         h->parity ^= 1;
+        h->pending = true;
     }
     return read_status(h);
 }
@@ -596,33 +675,47 @@ int snac_gpu_step(snac_gpu* h, int nsteps) {
 int snac_gpu_begin_step(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
-    return op_begin(h);
+    int rc = flush_pending(h);
+    return rc ? rc : op_begin(h);
 }
-int snac_gpu_loop_elements_energy(snac_gpu* h) { return h ? op_energy_elements(h) : SNAC_GPU_EINVAL; }
-int snac_gpu_loop_nodes_energy(snac_gpu* h) { return h ? op_energy_nodes(h) : SNAC_GPU_EINVAL; }
+int snac_gpu_loop_elements_energy(snac_gpu* h) {
+    if (!h) return SNAC_GPU_EINVAL;
+    int rc = flush_pending(h);
+    return rc ? rc : op_energy_elements(h);
+}
+int snac_gpu_loop_nodes_energy(snac_gpu* h) {
+    if (!h) return SNAC_GPU_EINVAL;
+    int rc = flush_pending(h);
+    return rc ? rc : op_energy_nodes(h);
+}
 int snac_gpu_calc_stresses(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
-    int rc = op_calc_stresses(h);
+    int rc = flush_pending(h);
+    if (!rc) rc = op_calc_stresses(h);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_loop_nodes_momentum(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
-    int rc = op_loop_nodes(h);
+    int rc = flush_pending(h);
+    if (!rc) rc = op_loop_nodes(h);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_loop_elements_momentum(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
-    int rc = op_update_elements(h, h->time_step == 0);
+    int rc = flush_pending(h);
+    if (!rc) rc = op_update_elements(h, h->time_step == 0);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_sync(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
-    int rc = op_sync_full(h);
+    int rc = flush_pending(h);
+    if (!rc) rc = op_sync_full(h);
     return rc ? rc : read_status(h);
 }
 
 int snac_gpu_upload(snac_gpu* h, const snac_state_view* v) {
     if (!h || !v) return SNAC_GPU_EINVAL;
+    if (int rc = flush_pending(h)) return rc;
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
     if (v->coord || v->velocity || v->temperature) {
         std::vector<double4> p(nn), w(nn);
@@ -644,6 +737,7 @@ int snac_gpu_upload(snac_gpu* h, const snac_state_view* v) {
 
 int snac_gpu_download(snac_gpu* h, const snac_state_view* v) {
     if (!h || !v) return SNAC_GPU_EINVAL;
+    if (int rc = flush_pending(h)) return rc;
     CK(cudaStreamSynchronize(h->stream));
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
     if (v->coord || v->velocity || v->temperature || v->force || v->inertial_mass) {
@@ -716,6 +810,33 @@ int snac_gpu_sizes(const snac_gpu* h, long long* ne, long long* nn) {
     return 0;
 }
 long long snac_gpu_launch_count(const snac_gpu* h) { return h ? h->launches : 0; }
+
+int snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max) {
+    if (!h || !out || max < 1) return SNAC_GPU_EINVAL;
+    if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
+    for (auto& e : h->prof_ev) CK(cudaEventCreate(&e));
+    h->prof = out;
+    h->prof_n = 0;
+    h->prof_max = max;
+    CK(cudaEventRecord(h->prof_ev[0], h->stream));
+    bool fused = h->pending;
+    int rc = record_step(h, fused);
+    h->prof = nullptr;
+    if (!rc) {
+        h->parity ^= 0;  // record_step already flipped the parity in the node loop
+        h->pending = true;
+        CK(cudaStreamSynchronize(h->stream));
+        for (int i = 0; i < h->prof_n; i++) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->prof_ev[i], h->prof_ev[i + 1]);
+            out[i].ms = ms;
+        }
+    }
+    for (auto& e : h->prof_ev) cudaEventDestroy(e);
+    if (rc) return rc;
+    rc = read_status(h);
+    return rc ? rc : h->prof_n;
+}
 void* snac_gpu_stream(snac_gpu* h) { return h ? (void*)h->stream : nullptr; }
 
 }  // extern "C"

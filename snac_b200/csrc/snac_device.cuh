@@ -83,6 +83,7 @@ struct DevMaterial {
 // Device-resident scalars of one model (everything a captured step reads).
 struct DevScalars {
     double dt;
+    double dt_rot;                   // dt of the element update still to apply (fused pipeline)
     double speed_of_sound;
     double min_length_scale;
     double vmax;

@@ -41,6 +41,9 @@ struct Fields {
     double* vol;             // [ne*10][2] volume, old volume (Maxwell)
     double* hflux;           // [ne*10][4] heat flux x, y, z and thermal stress
     double* tpre;            // [nn] temperature before the BCs (temperature + density)
+    double* fterm;           // [ne*10][4 faces][3] stress.n.A/6 of each face (Force.c:154-165)
+    double* fgrav;           // [ne*10] g rho V / 8 (Force.c:173)
+    double* fmass;           // [ne*10][4] (constant dt) or [ne*10] inertial-mass term (Force.c:107-140)
     const uchar4* bc;        // per node: velocity-VC index of x, y, z and temperature-VC index (255 = free)
     const double* vbc_val;   // [n_vc][3]
     const double* tbc_val;   // [n_tc]
@@ -58,7 +61,13 @@ struct Config {
     double strain_inert;
 };
 
-constexpr int ELEM_WARPS = 4;                  // warps per block in the element kernels
+#ifndef SNAC_ELEM_MINB
+#define SNAC_ELEM_MINB 4  // resident blocks per SM asked of the compiler (register budget, measured best)
+#endif
+#ifndef SNAC_ELEM_WARPS
+#define SNAC_ELEM_WARPS 4
+#endif
+constexpr int ELEM_WARPS = SNAC_ELEM_WARPS;    // warps per block in the element kernels
 constexpr int ELEM_PER_BLOCK = ELEM_WARPS * 3;  // 12 elements per block
 constexpr unsigned FULL = 0xffffffffu;
 
@@ -141,15 +150,13 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
 // ======================================================================================
 // Snac_EP_CalcStresses: StrainRate.c:49-305, Stress.c:53-172 and the constitutive hook
 // ======================================================================================
+// st holds the tet's stress on entry (already rotated when fused with the
+// element update); the new stress, plastic strain, viscosity, density and
+// the Force terms are stored.
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32) k_calc_stresses(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
-    const double dt = F.sc->dt;
-    V3 c[4], v[4];
-    double T[4], T0[4];
-    load_tet(m, F, s, c, v, T, T0);
-    TetGeom g;
-    tet_geometry(c, g);
+__device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
+                                              const V3 v[4], const double T[4], const TetGeom& g, double st[6],
+                                              const double dt) {
     double sr[6];
     tet_strain_rate(v, g, sr);
 
@@ -173,11 +180,6 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32) k_calc_stresses(Mesh m, Field
 
     const int ph = s.active ? phase_of(F, s.e) : 0;
     const DevMaterial& M = F.mats[ph];
-    double st[6] = {0, 0, 0, 0, 0, 0};
-    if (s.active) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
-    }
     double eps_p = 0.0, eta = 0.0;
     if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
         eps_p = s.active ? F.eps_p[s.q] : 0.0;
@@ -372,6 +374,46 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32) k_calc_stresses(Mesh m, Field
         if (s.active) F.density[s.q] = M.density * (1.0 - M.alpha * (avgT - M.reftemp) + M.beta * pressure);
     }
 
+    // Per-tet terms of Snac_Force (Force.c:107-180), evaluated here where the
+    // tet's geometry and new stress already are.  k_loop_nodes adds them in
+    // the reference's node-centred order, so the sums keep their bits.
+    if (s.active) {
+        const double rho = cfg.has_density ? F.density[s.q] : M.density;
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            const V3& nr = g.n[f];
+            const double A = g.A[f];
+            double* o = F.fterm + s.q * 12 + f * 3;
+            o[0] = (st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A / 6.0f;
+            o[1] = (st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A / 6.0f;
+            o[2] = (st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A / 6.0f;
+        }
+        F.fgrav[s.q] = cfg.gravity * rho * g.V / 8.0f;
+        const double factor4 = 1.0f / 4.0f;
+        if (cfg.dt_type == SNAC_DT_DYNAMIC) {
+            const double sos = F.sc->speed_of_sound;
+            const double inertialDensity = (M.lambda + 2.0f * M.mu) / (sos * sos);
+            F.fmass[s.q] = factor4 * inertialDensity * g.V;
+        } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
+            const double alpha1 = (M.lambda + 2.0f * M.mu);
+#pragma unroll
+            for (int f = 0; f < 4; f++) {
+                const V3& nr = g.n[f];
+                const double A = g.A[f];
+                double area_sum = 0.0, temp;
+                temp = (nr.x * A) * (nr.x * A);
+                if (temp > area_sum) area_sum = temp;
+                temp = (nr.y * A) * (nr.y * A);
+                if (temp > area_sum) area_sum = temp;
+                temp = (nr.z * A) * (nr.z * A);
+                if (temp > area_sum) area_sum = temp;
+                F.fmass[s.q * 4 + f] = alpha1 * area_sum / (9.0f * g.V) * (dt * dt);
+            }
+        } else {
+            F.fmass[s.q] = factor4 * rho * g.V;
+        }
+    }
+
     if (s.active) {
         bool ok = true;
 #pragma unroll
@@ -385,19 +427,77 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32) k_calc_stresses(Mesh m, Field
     }
 }
 
-// ======================================================================================
-// Snac_EP_LoopElementsMomentum: UpdateElement.c:54-269 and the minLengthScale
-// reduction of _Snac_Context_LoopElements (Context.c:1156-1184)
-// ======================================================================================
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32) k_update_elements(Mesh m, Fields F, Config cfg) {
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stresses(Mesh m, Fields F, Config cfg) {
     TetSlot s = tet_slot(m);
-    const double dt = F.sc->dt;
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
     TetGeom g;
     tet_geometry(c, g);
+    double st[6] = {0, 0, 0, 0, 0, 0};
+    if (s.active) {
+#pragma unroll
+        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+    }
+    stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+}
+
+// UpdateElement.c:84-91 volume bookkeeping (Maxwell reads V/V_old) and the
+// Jaumann rotation of the stress (:145-265) of one tet; returns the rotated stress.
+template <int PLUGIN>
+__device__ __forceinline__ void element_update_tet(const Fields& F, const Config& cfg, const TetSlot& s, const V3 v[4],
+                                                   const TetGeom& g, double dt, double st[6]) {
+    if (PLUGIN == SNAC_RHEOLOGY_MAXWELL && s.active) {
+        double vc = F.vol[s.q * 2 + 0];
+        F.vol[s.q * 2 + 1] = cfg.time_step_zero ? g.V : vc;
+        F.vol[s.q * 2 + 0] = g.V;
+    }
+    if (s.active) {
+#pragma unroll
+        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+        rotate_stress(v, g, dt, st);
+    }
+}
+
+// The end of step n (element update with dt_n, whose geometry and velocities
+// are already final) fused with the stress update of step n+1 (dt_{n+1},
+// same geometry and velocities): one geometry evaluation, one stress
+// read-modify-write.  Used when no energy hook sits between the two.
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    if (blockIdx.x == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    double st[6] = {0, 0, 0, 0, 0, 0};
+    element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
+    stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+}
+
+// ======================================================================================
+// Snac_EP_LoopElementsMomentum: UpdateElement.c:54-269 and the minLengthScale
+// reduction of _Snac_Context_LoopElements (Context.c:1156-1184)
+// ======================================================================================
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elements(Mesh m, Fields F, Config cfg,
+                                                                                     int pending) {
+    TetSlot s = tet_slot(m);
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    double st[6];
+    element_update_tet<PLUGIN>(F, cfg, s, v, g, pending ? F.sc->dt_rot : F.sc->dt, st);
+    if (s.active) {
+#pragma unroll
+        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
+    }
+    if (pending) return;  // the minimum length scale of this geometry is already known
     double ls = 1.0e+27f;
 #pragma unroll
     for (int f = 0; f < 4; f++) {
@@ -409,20 +509,46 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32) k_update_elements(Mesh m, Fie
     }
     if (!s.active) ls = 1.0e+27f;
     if (s.active && g.V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, s.e);
-    if (PLUGIN == SNAC_RHEOLOGY_MAXWELL && s.active) {
-        double vc = F.vol[s.q * 2 + 0];
-        F.vol[s.q * 2 + 1] = cfg.time_step_zero ? g.V : vc;
-        F.vol[s.q * 2 + 0] = g.V;
-    }
-    if (s.active) {
-        double st[6];
-#pragma unroll
-        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
-        rotate_stress(v, g, dt, st);
-#pragma unroll
-        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
-    }
     // global minimum (exact: min does not round)
+    for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
+}
+
+// The minimum over all tets and faces of |V/A| (UpdateElement.c:109-139) for
+// the current coordinates, without the rest of the element update.  For a
+// tet, min_f RN(V/A_f) = RN(V / max_f A_f) because correctly rounded
+// division is monotonic, and max_f A_f = RN(sqrt(max_f s_f))/2 for the same
+// reason; faces with A = 0 are skipped as in the reference.
+__global__ void __launch_bounds__(256) k_min_length_scale(Mesh m, Fields F) {
+    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double ls = 1.0e+27f;
+    if (q < m.ne * NT) {
+        long long e = q / NT;
+        int t = (int)(q - e * NT), i, j, k;
+        elem_ijk(m, e, i, j, k);
+        V3 c[4];
+#pragma unroll
+        for (int qn = 0; qn < 4; qn++) {
+            double4 p = F.pos[corner_node(m, i, j, k, tet_node_rt(t, qn))];
+            c[qn] = {p.x, p.y, p.z};
+        }
+        double V = tet_volume(c[0], c[1], c[2], c[3]);
+        double smax = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; f++) {
+            const V3 &c1 = c[face_node(f, 0)], &c2 = c[face_node(f, 1)], &c3 = c[face_node(f, 2)];
+            double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
+            double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
+            double a = y2 * z3 - z2 * y3;
+            double b = z2 * x3 - x2 * z3;
+            double cc = x2 * y3 - y2 * x3;
+            double sq = a * a + b * b + cc * cc;
+            if (sq > smax) smax = sq;
+        }
+        double A = sqrt(smax) / 2.0;
+        if (A) ls = fabs(V / A);
+        if (V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, e);
+    }
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
@@ -441,56 +567,26 @@ __global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg
     double vcand = 0.0;
     if (active) {
         const double dt = F.sc->dt;
-        const double sos = F.sc->speed_of_sound;
         int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
-        const double factor4 = 1.0f / 4.0f;
         double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
+        // Snac_Force: the 8 incident hexes in HexaEL.c:529-573 order, 5 tets each
+        // (NodeToTetra/NodeToSurface); absent hexes are skipped (Force.c:92)
 #pragma unroll
         for (int ne = 0; ne < 8; ne++) {
             int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
             if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
             long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
-            const DevMaterial& M = F.mats[phase_of(F, e)];
-            const double inertialDensity = (M.lambda + 2.0f * M.mu) / (sos * sos);
-            V3 corner[8];
-#pragma unroll
-            for (int cc = 0; cc < 8; cc++) {
-                double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
-                corner[cc] = {p.x, p.y, p.z};
-            }
 #pragma unroll
             for (int idx = 0; idx < 5; idx++) {
                 const int t = node_tet(ne, idx);
                 const int f = node_face(ne, idx);
-                V3 tc[4];
-#pragma unroll
-                for (int qn = 0; qn < 4; qn++) tc[qn] = corner[tet_node(t, qn)];
-                double V = tet_volume(tc[0], tc[1], tc[2], tc[3]);
-                double A;
-                V3 nr;
-                tet_face(tc[face_node(f, 0)], tc[face_node(f, 1)], tc[face_node(f, 2)], A, nr);
                 const long long q = e * NT + t;
-                const double* sq = F.stress + q * 6;
-                double s00 = sq[0], s11 = sq[1], s22 = sq[2], s01 = sq[3], s02 = sq[4], s12 = sq[5];
-                const double effDensity = cfg.has_density ? F.density[q] : M.density;
-                if (DTTYPE == SNAC_DT_DYNAMIC) {
-                    imass += factor4 * inertialDensity * V;
-                } else if (DTTYPE == SNAC_DT_CONSTANT) {
-                    double alpha1 = (M.lambda + 2.0f * M.mu), area_sum = 0.0, temp;
-                    temp = (nr.x * A) * (nr.x * A);
-                    if (temp > area_sum) area_sum = temp;
-                    temp = (nr.y * A) * (nr.y * A);
-                    if (temp > area_sum) area_sum = temp;
-                    temp = (nr.z * A) * (nr.z * A);
-                    if (temp > area_sum) area_sum = temp;
-                    imass += alpha1 * area_sum / (9.0f * V) * (dt * dt);
-                } else {
-                    imass += factor4 * effDensity * V;
-                }
-                fx += (s00 * nr.x + s01 * nr.y + s02 * nr.z) * A / 6.0f;
-                fy += (s01 * nr.x + s11 * nr.y + s12 * nr.z) * A / 6.0f;
-                fz += (s02 * nr.x + s12 * nr.y + s22 * nr.z) * A / 6.0f;
-                fy -= cfg.gravity * effDensity * V / 8.0f;
+                imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[q * 4 + f] : F.fmass[q];
+                const double* o = F.fterm + q * 12 + f * 3;
+                fx += o[0];
+                fy += o[1];
+                fz += o[2];
+                fy -= F.fgrav[q];
             }
         }
         // FLAC local damping with the pre-update velocity, then v and x
@@ -527,13 +623,8 @@ __global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg
 // Snac_EP_LoopElementsEnergy: Snac_HeatFlux (temperature/HeatFlux.c:60-200) and
 // SnacTemperature_HeatFluxBC (temperature/VariableConditions.c:280-413)
 // ======================================================================================
-__global__ void __launch_bounds__(ELEM_WARPS * 32) k_heat_flux(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
-    V3 c[4], v[4];
-    double T[4], T0[4];
-    load_tet(m, F, s, c, v, T, T0);
-    TetGeom g;
-    tet_geometry(c, g);
+__device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
+                                              const double T[4], const double T0[4], const TetGeom& g) {
     const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
     double q[3], tsr = 0.0;
     for (int d = 0; d < 3; d++)
@@ -594,6 +685,36 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32) k_heat_flux(Mesh m, Fields F,
         h[2] = q[2];
         if (cfg.thermal_stress) h[3] = tsr;
     }
+}
+
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    heat_flux_tet(m, F, cfg, s, T, T0, g);
+}
+
+// End of step n (element update) fused with the heat flux of step n+1: both
+// need the geometry of the same coordinates.
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m);
+    if (blockIdx.x == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    double st[6];
+    element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
+    if (s.active) {
+#pragma unroll
+        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
+    }
+    heat_flux_tet(m, F, cfg, s, T, T0, g);
 }
 
 // ======================================================================================
@@ -668,6 +789,7 @@ __global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {
     double minLS = __longlong_as_double((long long)sc->minls_bits);
     sc->min_length_scale = minLS;
     if (sc->time_step == 0) sc->init_min_length_scale = minLS;
+    sc->dt_rot = sc->dt;  // the element update of this step (done now, or deferred into the next kernel) used this dt
     if (cfg.dt_type == SNAC_DT_DYNAMIC) {
         sc->dt = minLS * 0.45f * cfg.strain_inert / vmax;
         sc->speed_of_sound = minLS * 0.5f / sc->dt;
