@@ -229,6 +229,11 @@ long long snac_gpu_launch_count(const snac_gpu* h);
 /* The handle's cudaStream_t, as a void* (for event timing by callers). */
 void* snac_gpu_stream(snac_gpu* h);
 int  snac_gpu_device_count(void);
+/* Self-test of the straight-line correctly rounded division the kernels use
+ * (csrc/snac_device.cuh): n random operand pairs (wide exponent range,
+ * signed zeros, exact quotients and ties) compared bit for bit with the
+ * IEEE quotient of the GPU; *mismatches receives the count (expected 0). */
+int  snac_gpu_selftest_division(long long n, unsigned long long seed, long long* mismatches);
 
 #ifdef __cplusplus
 }

@@ -70,6 +70,8 @@ def load_library(path: str = LIB_PATH):
     lib.snac_gpu_stream.restype = vp
     lib.snac_gpu_profile_step.argtypes = [vp, C.POINTER(KernelTime), C.c_int]
     lib.snac_gpu_profile_step.restype = C.c_int
+    lib.snac_gpu_selftest_division.argtypes = [C.c_longlong, C.c_ulonglong, C.POINTER(C.c_longlong)]
+    lib.snac_gpu_selftest_division.restype = C.c_int
     lib.snac_gpu_device_count.argtypes = []
     lib.snac_gpu_device_count.restype = C.c_int
     _LIB = lib

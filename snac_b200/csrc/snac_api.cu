@@ -290,7 +290,7 @@ int op_fused(snac_gpu* h) {
 }
 
 int op_min_length_scale(snac_gpu* h) {
-    k_min_length_scale<<<(unsigned)((h->mesh.ne * NT + 255) / 256), 256, 0, h->stream>>>(h->mesh, fields(h));
+    k_min_length_scale<<<(unsigned)((h->mesh.ne + 127) / 128), 128, 0, h->stream>>>(h->mesh, fields(h));
     h->launches++;
     return launch_check_named(h, "k_min_length_scale");
 }
@@ -403,6 +403,20 @@ void hydrostatic_ic(const snac_gpu_desc* d, const std::vector<double>& coord, st
 
 extern "C" {
 
+int snac_gpu_selftest_division(long long n, unsigned long long seed, long long* mismatches) {
+    if (!mismatches || n < 0) return SNAC_GPU_EINVAL;
+    unsigned long long* d = nullptr;
+    if (cudaMalloc(&d, sizeof *d) != cudaSuccess) return SNAC_GPU_ENOMEM;
+    cudaMemset(d, 0, sizeof *d);
+    k_selftest_division<<<148 * 8, 256>>>(n, seed, d);
+    unsigned long long h = 0;
+    cudaError_t e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return SNAC_GPU_ECUDA;
+    *mismatches = (long long)h;
+    return 0;
+}
+
 int snac_gpu_device_count(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
@@ -480,7 +494,7 @@ int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
     if (h->has_density)
         if ((rc = dalloc(h, &h->density, nq))) return rc;
     if (d->temperature) {
-        if ((rc = dalloc(h, &h->hflux, nq * 4))) return rc;
+        if ((rc = dalloc(h, &h->hflux, nq * HF_STRIDE))) return rc;
         if (h->has_density && (rc = dalloc(h, &h->tpre, nn))) return rc;
     }
 

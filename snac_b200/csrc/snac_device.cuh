@@ -9,6 +9,8 @@
 #pragma once
 
 #include <cstdint>
+#include <cstring>
+#include <cmath>
 
 #include "snac_gpu.h"
 
@@ -101,6 +103,95 @@ __device__ __forceinline__ void report(DevScalars* sc, int code, long long index
     if (atomicCAS(&sc->status, 0, code) == 0) sc->err_index = index;
 }
 
+#ifndef SNAC_FAST_DIV
+#define SNAC_FAST_DIV 0  // measured slower than the hardware IEEE division on B200; kept switchable
+#endif
+
+// ---- correctly rounded division without the slow-path branch -----------------
+// dv(x, y) returns the same bits as the IEEE quotient x / y (round to
+// nearest even) for operands in the normal range, as a straight-line
+// sequence the compiler can interleave with other work:
+//   1. a reciprocal seed z0 ~ 1/y from the single-precision approximate
+//      reciprocal (relative error < 2^-22 after the conversions),
+//   2. two Newton-Raphson steps z <- z + z (1 - y z), each fused, which leave
+//      |1 - y z| ~ 2^-52,
+//   3. q = x z corrected once with the exact remainder, q <- q + (x - q y) z;
+//      q is then within one ulp of x / y (faithful),
+//   4. the rounding decision from the exact remainder r = x - q y (one FMA,
+//      exact because q is faithful): the correctly rounded quotient is q or
+//      its neighbour qn towards x / y, whichever is nearer; nearer is decided
+//      by comparing 2|r| with |qn - q| |y| (both exact: |qn - q| is a power of
+//      two), ties to the even significand.
+// This is the Newton-Raphson division with Markstein's remainder-based
+// correction: P. Markstein, "Computation of elementary functions on the IBM
+// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; J.-M. Muller
+// et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018, ch. 4.
+// Divisors outside [2^-120, 2^120], non-finite operands and quotients
+// outside [2^-800, 2^800] (other than zero) take the IEEE division instead.
+// The device self-test (snac_gpu_selftest_division) compares it with the
+// hardware-rounded '/' on random operands.
+__host__ __device__ __forceinline__ double approx_recip(double y) {
+#ifdef __CUDA_ARCH__
+    float r, yf = (float)y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(yf));
+    return (double)r;
+#else
+    return (double)(1.0f / (float)y);
+#endif
+}
+
+// ~1/y, |1 - y z| ~ 2^-52 (only meaningful when 2^-120 <= |y| <= 2^120)
+__host__ __device__ __forceinline__ double recip(double y) {
+    double z = approx_recip(y);
+    double e = fma(-y, z, 1.0);
+    z = fma(z, e, z);
+    e = fma(-y, z, 1.0);
+    return fma(z, e, z);
+}
+
+__host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
+#if SNAC_FAST_DIV
+    const double q0 = x * z;  // for x = +-0 this is already the IEEE zero with the right sign
+    double r = fma(-q0, y, x);
+    double q = fma(r, z, q0);
+    r = fma(-q, y, x);
+    const bool up = (r > 0.0) == (y > 0.0);  // x / y lies above q
+#ifdef __CUDA_ARCH__
+    long long b = __double_as_longlong(q);
+    double qn = __longlong_as_double(b + (((q > 0.0) == up) ? 1 : -1));
+#else
+    long long b;
+    memcpy(&b, &q, 8);
+    long long bn = b + (((q > 0.0) == up) ? 1 : -1);
+    double qn;
+    memcpy(&qn, &bn, 8);
+#endif
+    const double tr = 2.0 * fabs(r);
+    const double h = fabs(qn - q) * fabs(y);
+    double res = (tr < h) ? q : (tr > h ? qn : ((b & 1) ? qn : q));
+    if (r == 0.0) res = q;
+    if (x == 0.0) res = q0;
+    const double ay = fabs(y), aq = fabs(q);
+    const bool ok = ay >= 0x1p-120 && ay <= 0x1p120 && (x == 0.0 || (aq >= 0x1p-800 && aq <= 0x1p800));
+    return ok ? res : x / y;
+#else
+    (void)z;
+    return x / y;
+#endif
+}
+__host__ __device__ __forceinline__ double dv(double x, double y) {
+#if SNAC_FAST_DIV
+    return dvz(x, y, recip(y));
+#else
+    return x / y;
+#endif
+}
+// division by the constants the reference uses; the reciprocal is RN(1/c)
+__host__ __device__ __forceinline__ double dv3(double x) { return dvz(x, 3.0, 0x1.5555555555555p-2); }
+__host__ __device__ __forceinline__ double dv6(double x) { return dvz(x, 6.0, 0x1.5555555555555p-3); }
+__host__ __device__ __forceinline__ double dv9(double x) { return dvz(x, 9.0, 0x1.c71c71c71c71cp-4); }
+__host__ __device__ __forceinline__ double dv10(double x) { return dvz(x, 10.0, 0x1.999999999999ap-4); }
+
 struct V3 {
     double x, y, z;
 };
@@ -110,7 +201,7 @@ __device__ __forceinline__ double tet_volume(const V3& c1, const V3& c2, const V
     double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
     double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
     double x4 = c4.x - c1.x, y4 = c4.y - c1.y, z4 = c4.z - c1.z;
-    double v = (x4 * (y2 * z3 - z2 * y3) + y4 * (z2 * x3 - x2 * z3) + z4 * (x2 * y3 - x3 * y2)) / 6.0;
+    double v = dv6(x4 * (y2 * z3 - z2 * y3) + y4 * (z2 * x3 - x2 * z3) + z4 * (x2 * y3 - x3 * y2));
     return fabs(v);
 }
 
@@ -124,9 +215,10 @@ __device__ __forceinline__ void tet_face(const V3& c1, const V3& c2, const V3& c
     double c = x2 * y3 - y2 * x3;
     double s = sqrt(a * a + b * b + c * c);
     area = s / 2.0;
-    n.x = a / s;
-    n.y = b / s;
-    n.z = c / s;
+    const double zs = recip(s);
+    n.x = dvz(a, s, zs);
+    n.y = dvz(b, s, zs);
+    n.z = dvz(c, s, zs);
 }
 
 struct TetGeom {
@@ -170,20 +262,22 @@ __device__ __forceinline__ double shear_sum(const V3 v[4], const TetGeom& g, int
 // StrainRate.c:65-184, before the mixed-discretisation correction;
 // sr = (xx, yy, zz, xy, xz, yz)
 __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g, double sr[6]) {
-    sr[0] = -1.0f * (face_sum(v, 0, g, 0)) / 3.0f / g.V;
-    sr[1] = -1.0f * (face_sum(v, 1, g, 1)) / 3.0f / g.V;
-    sr[2] = -1.0f * (face_sum(v, 2, g, 2)) / 3.0f / g.V;
-    sr[3] = -0.5f * (shear_sum(v, g, 0, 1)) / 3.0f / g.V;
-    sr[4] = -0.5f * (shear_sum(v, g, 0, 2)) / 3.0f / g.V;
-    sr[5] = -0.5f * (shear_sum(v, g, 1, 2)) / 3.0f / g.V;
+    const double zV = recip(g.V);
+    sr[0] = dvz(dv3(-1.0f * (face_sum(v, 0, g, 0))), g.V, zV);
+    sr[1] = dvz(dv3(-1.0f * (face_sum(v, 1, g, 1))), g.V, zV);
+    sr[2] = dvz(dv3(-1.0f * (face_sum(v, 2, g, 2))), g.V, zV);
+    sr[3] = dvz(dv3(-0.5f * (shear_sum(v, g, 0, 1))), g.V, zV);
+    sr[4] = dvz(dv3(-0.5f * (shear_sum(v, g, 0, 2))), g.V, zV);
+    sr[5] = dvz(dv3(-0.5f * (shear_sum(v, g, 1, 2))), g.V, zV);
 }
 
 // Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
 // zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
-    double r01 = -(0.5f / g.V) * (spin_sum(v, g, 0, 1)) / 3.0f;
-    double r02 = -(0.5f / g.V) * (spin_sum(v, g, 0, 2)) / 3.0f;
-    double r12 = -(0.5 / g.V) * (spin_sum(v, g, 1, 2)) / 3.0f;
+    const double hV = dv(0.5, g.V);
+    double r01 = dv3(-(hV) * (spin_sum(v, g, 0, 1)));
+    double r02 = dv3(-(hV) * (spin_sum(v, g, 0, 2)));
+    double r12 = dv3(-(hV) * (spin_sum(v, g, 1, 2)));
     s[0] += (2.0f * r01 * s[3] + 2.0f * r02 * s[4]) * dt;
     s[1] += (2.0f * (-1.0f * r01) * s[3] + 2.0f * r12 * s[5]) * dt;
     s[2] += (2.0f * (-1.0f * r02) * s[4] + 2.0f * (-1.0f * r12) * s[5]) * dt;
@@ -219,15 +313,15 @@ __host__ __device__ __forceinline__ void jac_pair(Jac& J, int i, double tresh) {
     } else if (fabs(apq) > tresh) {
         double h = J.d[IQ] - J.d[IP], t;
         if ((fabs(h) + g) == fabs(h)) {
-            t = apq / h;
+            t = dv(apq, h);
         } else {
-            double theta = 0.5f * h / (apq);
-            t = 1.0f / (fabs(theta) + sqrt(1.0f + theta * theta));
+            double theta = dv(0.5f * h, apq);
+            t = dv(1.0f, fabs(theta) + sqrt(1.0f + theta * theta));
             if (theta < 0.0f) t *= -1.0f;
         }
-        double c = 1.0f / sqrt(1.0f + t * t);
+        double c = dv(1.0f, sqrt(1.0f + t * t));
         double s = t * c;
-        double tau = s / (1.0f + c);
+        double tau = dv(s, 1.0f + c);
         h = t * apq;
         J.z[IP] -= h;
         J.z[IQ] += h;
@@ -265,7 +359,7 @@ __host__ __device__ void principal_stresses(const double st[6], double sp[3], do
         sm += fabs(J.a02);
         sm += fabs(J.a12);
         if (sm == 0.0f) break;
-        double tresh = (i < 4) ? 0.2f * sm / (3u * 3u) : 0.0f;
+        double tresh = (i < 4) ? dv9(0.2f * sm) : 0.0f;
         jac_pair<0, 1>(J, i, tresh);
         jac_pair<0, 2>(J, i, tresh);
         jac_pair<1, 2>(J, i, tresh);
@@ -359,7 +453,7 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
     double sP = st * anphi - 2 * cohesion * sqrt(anphi);
     double h = sp[2] - st + aP * (sp[0] - sP);
     if (h < 0.0f) {
-        alam = fs / (a1 - a2 * anpsi + a1 * anphi * anpsi - a2 * anphi + 2.0 * sqrt(anphi) * hardening);
+        alam = dv(fs, a1 - a2 * anpsi + a1 * anphi * anpsi - a2 * anphi + 2.0 * sqrt(anphi) * hardening);
         sp[0] -= alam * (a1 - a2 * anpsi);
         sp[1] -= alam * a2 * (1.0f - anpsi);
         sp[2] -= alam * (a2 - a1 * anpsi);
@@ -367,7 +461,7 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
         dep2 = 0.0f;
         dep3 = -alam * anpsi;
     } else {
-        alam = ft / a1;
+        alam = dv(ft, a1);
         sp[0] -= alam * a2;
         sp[1] -= alam * a2;
         sp[2] -= alam * a1;
@@ -375,7 +469,7 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
         dep2 = 0.0f;
         dep3 = alam;
     }
-    depm = (dep1 + dep2 + dep3) / 3.0f;
+    depm = dv3(dep1 + dep2 + dep3);
     eps_p += sqrt(0.5f * ((dep1 - depm) * (dep1 - depm) + (dep2 - depm) * (dep2 - depm) +
                           (dep3 - depm) * (dep3 - depm) + depm * depm));
     double r[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -397,8 +491,8 @@ __device__ __forceinline__ double arrhenius_viscosity(double refvisc, double srJ
                                                       double srexponent, double H, double avgTemp, double rTemp,
                                                       double vis_min, double vis_max) {
     const double R = 8.31448;
-    double eta = refvisc * pow((srJ2 / rstrainrate), (1. / srexponent - 1.)) *
-                 exp(H / R * (1. / (avgTemp + 273.15) - 1. / (rTemp + 273.15)));
+    double eta = refvisc * pow((dv(srJ2, rstrainrate)), (dv(1., srexponent) - 1.)) *
+                 exp(dv(H, R) * (dv(1., avgTemp + 273.15) - dv(1., rTemp + 273.15)));
     if (eta < vis_min) eta = vis_min;
     if (eta > vis_max) eta = vis_max;
     return eta;
@@ -409,16 +503,16 @@ __device__ __forceinline__ double arrhenius_viscosity(double refvisc, double srJ
 __device__ __forceinline__ void maxwell_update(double s[6], const double e[6], double stressd[3],
                                                const double straind[3], double trace_stress, double trace_strain,
                                                double rmu, double eta, double dt, double bulkm) {
-    double temp = rmu / (2.0f * (eta)) * dt;
+    double temp = dv(rmu, 2.0f * (eta)) * dt;
     double vic1 = 1.0f - temp;
-    double vic2 = 1.0f / (1.0f + temp);
+    double vic2 = dv(1.0f, 1.0f + temp);
     stressd[0] = (stressd[0] * vic1 + 2.0f * rmu * straind[0]) * vic2;
     stressd[1] = (stressd[1] * vic1 + 2.0f * rmu * straind[1]) * vic2;
     stressd[2] = (stressd[2] * vic1 + 2.0f * rmu * straind[2]) * vic2;
     s[3] = (s[3] * vic1 + 2.0f * rmu * e[3]) * vic2;
     s[4] = (s[4] * vic1 + 2.0f * rmu * e[4]) * vic2;
     s[5] = (s[5] * vic1 + 2.0f * rmu * e[5]) * vic2;
-    double VolumicStress = trace_stress / 3.0f + bulkm * trace_strain;
+    double VolumicStress = dv3(trace_stress) + bulkm * trace_strain;
     s[0] = stressd[0] + VolumicStress;
     s[1] = stressd[1] + VolumicStress;
     s[2] = stressd[2] + VolumicStress;

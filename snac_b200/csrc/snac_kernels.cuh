@@ -39,7 +39,7 @@ struct Fields {
     double* visc;            // [ne*10]  viscosity (visco-plastic, Maxwell)
     double* density;         // [ne*10]  only when some phase has alpha or beta != 0
     double* vol;             // [ne*10][2] volume, old volume (Maxwell)
-    double* hflux;           // [ne*10][4] heat flux x, y, z and thermal stress
+    double* hflux;           // [ne*10][6] face energy terms (q.n A/6), Cp rho V/8, thermal stress
     double* tpre;            // [nn] temperature before the BCs (temperature + density)
     double* fterm;           // [ne*10][4 faces][3] stress.n.A/6 of each face (Force.c:154-165)
     double* fgrav;           // [ne*10] g rho V / 8 (Force.c:173)
@@ -70,6 +70,7 @@ struct Config {
 constexpr int ELEM_WARPS = SNAC_ELEM_WARPS;    // warps per block in the element kernels
 constexpr int ELEM_PER_BLOCK = ELEM_WARPS * 3;  // 12 elements per block
 constexpr unsigned FULL = 0xffffffffu;
+constexpr int HF_STRIDE = 6;  // per-tet heat record: 4 face energy terms, lumped capacity, thermal stress
 
 __device__ __forceinline__ long long node_id(const Mesh& m, int i, int j, int k) {
     return (long long)i + (long long)j * m.nnx + (long long)k * m.nnx * m.nny;
@@ -164,11 +165,11 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     double vsum = grp_sum(g.V, s.base);
     double elemVolume = 2.0 * (vsum * 0.5);
     // mixed discretisation, StrainRate.c:272-289
-    double trace = (sr[0] + sr[1] + sr[2]) / 3.0f;
+    double trace = dv3(sr[0] + sr[1] + sr[2]);
     double partial = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) partial += grp(trace, s.base, u) * grp(g.V, s.base, u);
-    double corr = -1.0f * trace + partial / elemVolume;
+    double corr = -1.0f * trace + dv(partial, elemVolume);
     sr[0] += corr;
     sr[1] += corr;
     sr[2] += corr;
@@ -202,14 +203,14 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         st[5] += sh2 * e[5];
     } else if (PLUGIN == SNAC_RHEOLOGY_MAXWELL) {
         // maxwell/Constitutive.c:47-184
-        const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+        const double bulkm = M.lambda + dv3(2.0f * M.mu);
         double vold = s.active ? F.vol[s.q * 2 + 1] : 1.0;
         double vcur = s.active ? F.vol[s.q * 2 + 0] : 1.0;
         double trace_stress = st[0] + st[1] + st[2];
-        double trace_strain = vcur / vold - 1.0f;
+        double trace_strain = dv(vcur, vold) - 1.0f;
         double straind[3], stressd[3];
-        for (int a = 0; a < 3; a++) straind[a] = e[a] - (trace_strain) / 3.0f;
-        for (int a = 0; a < 3; a++) stressd[a] = st[a] - (trace_stress) / 3.0f;
+        for (int a = 0; a < 3; a++) straind[a] = e[a] - dv3(trace_strain);
+        for (int a = 0; a < 3; a++) stressd[a] = st[a] - dv3(trace_stress);
         double srJ2 = sqrt(fabs(straind[1] * straind[2] + straind[2] * straind[0] + straind[0] * straind[1] -
                                 e[3] * e[3] - e[4] * e[4] - e[5] * e[5])) /
                       dt;
@@ -235,9 +236,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             if (s.active && M.plstrain[0] != 0.0) report(F.sc, SNAC_GPU_EINVAL, s.e);
         } else {
             // visco-plastic Maxwell step, viscoplastic/Constitutive.c:158-257
-            const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+            const double bulkm = M.lambda + dv3(2.0f * M.mu);
             if (cfg.thermal_stress) {
-                double ts = s.active ? F.hflux[s.q * 4 + 3] : 0.0;
+                double ts = s.active ? F.hflux[s.q * HF_STRIDE + 5] : 0.0;
                 st[0] += ts;
                 st[1] += ts;
                 st[2] += ts;
@@ -245,8 +246,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double trace_stress = st[0] + st[1] + st[2];
             double trace_strain = e[0] + e[1] + e[2];
             double straind[3], stressd[3];
-            for (int a = 0; a < 3; a++) straind[a] = e[a] - (trace_strain) / 3.0f;
-            for (int a = 0; a < 3; a++) stressd[a] = st[a] - (trace_stress) / 3.0f;
+            for (int a = 0; a < 3; a++) straind[a] = e[a] - dv3(trace_strain);
+            for (int a = 0; a < 3; a++) stressd[a] = st[a] - dv3(trace_stress);
             // viscoplastic/Constitutive.c:189 reads strain[1][0], strain[2][0] and stress[2][0]
             // (the pointer, not the tensor, is indexed); those entries are always zero.
             const double lower = 0.0;
@@ -276,9 +277,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
             double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
             if (eps_p >= pl1 && eps_p <= pl2) {
-                const double tgf = (f1 - f0) / (pl2 - pl1);
-                const double tgd = (M.dil[i + 1] - M.dil[i]) / (pl2 - pl1);
-                const double tgc = (c1 - c0) / (pl2 - pl1);
+                const double dpl = pl2 - pl1, zpl = recip(dpl);
+                const double tgf = dvz(f1 - f0, dpl, zpl);
+                const double tgd = dvz(M.dil[i + 1] - M.dil[i], dpl, zpl);
+                const double tgc = dvz(c1 - c0, dpl, zpl);
                 fa = f0 + tgf * (eps_p - pl1);
                 da = M.dil[i] + tgd * (eps_p - pl1);
                 co = c0 + tgc * (eps_p - pl1);
@@ -317,7 +319,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         if (phi_ok) {
             st_own = M.ten_off;
             if (frictionAngle > 0.0) {
-                double tmp = cohesion / tan_fric(M, frictionAngle);
+                double tmp = dv(cohesion, tan_fric(M, frictionAngle));
                 if (tmp < st_own) st_own = tmp;
             }
         }
@@ -330,8 +332,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             report(F.sc, SNAC_GPU_EPHYSICS, s.e);  // plastic/Constitutive.c:175 abort()
         double sphi = sin_fric(M, frictionAngle);
         double spsi = sin_dil(M, dilationAngle);
-        double anphi = (1.0f + sphi) / (1.0f - sphi);
-        double anpsi = (1.0f + spsi) / (1.0f - spsi);
+        double anphi = dv(1.0f + sphi, 1.0f - sphi);
+        double anpsi = dv(1.0f + spsi, 1.0f - spsi);
         const double a1 = M.lambda + 2.0f * M.mu;
         const double a2 = M.lambda;
         // The reference always computes the principal stresses; they only
@@ -344,11 +346,11 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     }
 
     // trace averaging over the 10 tets, Stress.c:87-137
-    double traceS = (st[0] + st[1] + st[2]) / 3.0f;
+    double traceS = dv3(st[0] + st[1] + st[2]);
     double partialS = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) partialS += grp(traceS, s.base, u) * grp(g.V, s.base, u);
-    const double avgTrace = partialS / elemVolume;
+    const double avgTrace = dv(partialS, elemVolume);
     double cs2 = -1.0f * traceS + avgTrace;
     st[0] += cs2;
     st[1] += cs2;
@@ -356,11 +358,11 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 
     if (cfg.has_density) {
         // Stress.c:125-170: pressure = mean tet trace/3, density update
-        double ptet = (st[0] + st[1] + st[2]) / 3.0f;
+        double ptet = dv3(st[0] + st[1] + st[2]);
         double pressure = 0.0f;
 #pragma unroll
         for (int u = 0; u < NT; u++) pressure += grp(ptet, s.base, u);
-        pressure /= NT;
+        pressure = dv10(pressure);
         double avgT = 0.0;
         if (cfg.temperature) {
             // UpdateAverageTemp_LoopElements (Heat.c:143-172) ran before the
@@ -384,15 +386,15 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             const V3& nr = g.n[f];
             const double A = g.A[f];
             double* o = F.fterm + s.q * 12 + f * 3;
-            o[0] = (st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A / 6.0f;
-            o[1] = (st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A / 6.0f;
-            o[2] = (st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A / 6.0f;
+            o[0] = dv6((st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A);
+            o[1] = dv6((st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A);
+            o[2] = dv6((st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A);
         }
         F.fgrav[s.q] = cfg.gravity * rho * g.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
             const double sos = F.sc->speed_of_sound;
-            const double inertialDensity = (M.lambda + 2.0f * M.mu) / (sos * sos);
+            const double inertialDensity = dv(M.lambda + 2.0f * M.mu, sos * sos);
             F.fmass[s.q] = factor4 * inertialDensity * g.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
@@ -407,7 +409,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
                 if (temp > area_sum) area_sum = temp;
                 temp = (nr.z * A) * (nr.z * A);
                 if (temp > area_sum) area_sum = temp;
-                F.fmass[s.q * 4 + f] = alpha1 * area_sum / (9.0f * g.V) * (dt * dt);
+                F.fmass[s.q * 4 + f] = dv(alpha1 * area_sum, 9.0f * g.V) * (dt * dt);
             }
         } else {
             F.fmass[s.q] = factor4 * rho * g.V;
@@ -503,7 +505,7 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elem
     for (int f = 0; f < 4; f++) {
         double l = g.A[f];
         if (l) {
-            l = fabs(g.V / l);
+            l = fabs(dv(g.V, l));
             if (ls > l) ls = l;
         }
     }
@@ -519,35 +521,43 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elem
 // tet, min_f RN(V/A_f) = RN(V / max_f A_f) because correctly rounded
 // division is monotonic, and max_f A_f = RN(sqrt(max_f s_f))/2 for the same
 // reason; faces with A = 0 are skipped as in the reference.
-__global__ void __launch_bounds__(256) k_min_length_scale(Mesh m, Fields F) {
-    long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
+    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double ls = 1.0e+27f;
-    if (q < m.ne * NT) {
-        long long e = q / NT;
-        int t = (int)(q - e * NT), i, j, k;
+    if (e < m.ne) {
+        int i, j, k;
         elem_ijk(m, e, i, j, k);
-        V3 c[4];
+        V3 corner[8];
 #pragma unroll
-        for (int qn = 0; qn < 4; qn++) {
-            double4 p = F.pos[corner_node(m, i, j, k, tet_node_rt(t, qn))];
-            c[qn] = {p.x, p.y, p.z};
+        for (int cc = 0; cc < 8; cc++) {
+            double4 p = F.pos[corner_node(m, i, j, k, cc)];
+            corner[cc] = {p.x, p.y, p.z};
         }
-        double V = tet_volume(c[0], c[1], c[2], c[3]);
-        double smax = 0.0;
 #pragma unroll
-        for (int f = 0; f < 4; f++) {
-            const V3 &c1 = c[face_node(f, 0)], &c2 = c[face_node(f, 1)], &c3 = c[face_node(f, 2)];
-            double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
-            double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
-            double a = y2 * z3 - z2 * y3;
-            double b = z2 * x3 - x2 * z3;
-            double cc = x2 * y3 - y2 * x3;
-            double sq = a * a + b * b + cc * cc;
-            if (sq > smax) smax = sq;
+        for (int t = 0; t < NT; t++) {
+            V3 c[4];
+#pragma unroll
+            for (int qn = 0; qn < 4; qn++) c[qn] = corner[tet_node(t, qn)];
+            double V = tet_volume(c[0], c[1], c[2], c[3]);
+            double smax = 0.0;
+#pragma unroll
+            for (int f = 0; f < 4; f++) {
+                const V3 &c1 = c[face_node(f, 0)], &c2 = c[face_node(f, 1)], &c3 = c[face_node(f, 2)];
+                double x2 = c2.x - c1.x, y2 = c2.y - c1.y, z2 = c2.z - c1.z;
+                double x3 = c3.x - c1.x, y3 = c3.y - c1.y, z3 = c3.z - c1.z;
+                double a = y2 * z3 - z2 * y3;
+                double b = z2 * x3 - x2 * z3;
+                double cc = x2 * y3 - y2 * x3;
+                double sq = a * a + b * b + cc * cc;
+                if (sq > smax) smax = sq;
+            }
+            double A = sqrt(smax) / 2.0;
+            if (A) {
+                double l = fabs(dv(V, A));
+                if (ls > l) ls = l;
+            }
+            if (V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, e);
         }
-        double A = sqrt(smax) / 2.0;
-        if (A) ls = fabs(V / A);
-        if (V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, e);
     }
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
@@ -596,9 +606,10 @@ __global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg
         fx -= demf * sgn(w.x) * fabs(fx);
         fy -= demf * sgn(w.y) * fabs(fy);
         fz -= demf * sgn(w.z) * fabs(fz);
-        w.x += dt * fx / imass;
-        w.y += dt * fy / imass;
-        w.z += dt * fz / imass;
+        const double zm = recip(imass);
+        w.x += dvz(dt * fx, imass, zm);
+        w.y += dvz(dt * fy, imass, zm);
+        w.z += dvz(dt * fz, imass, zm);
         uchar4 b = F.bc[n];
         if (b.x != 255) w.x = F.vbc_val[b.x * 3 + 0];
         if (b.y != 255) w.y = F.vbc_val[b.y * 3 + 1];
@@ -627,13 +638,14 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
                                               const double T[4], const double T0[4], const TetGeom& g) {
     const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
     double q[3], tsr = 0.0;
+    const double zV = recip(g.V);
     for (int d = 0; d < 3; d++)
-        q[d] = 1.0f * M.thermal_conduct *
-               (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
-                T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0]) /
-               3.0f / g.V;
+        q[d] = dvz(dv3(1.0f * M.thermal_conduct *
+                       (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
+                        T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0])),
+                   g.V, zV);
     if (cfg.thermal_stress) {
-        const double bulkm = M.lambda + 2.0f * M.mu / 3.0f;
+        const double bulkm = M.lambda + dv3(2.0f * M.mu);
         double temp = 0.25f * (T[0] + T[1] + T[2] + T[3]);
         double temp0 = 0.25f * (T0[0] + T0[1] + T0[2] + T0[3]);
         tsr = -1.0f * M.alpha * bulkm * (temp - temp0);
@@ -670,20 +682,31 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
             for (int d = 0; d < 3; d++) normal[d] = nrm[3][d];
         double gd[3];
         for (int d = 0; d < 3; d++)
-            gd[d] = -1.0f *
-                    (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
-                     T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0]) /
-                    3.0f / g.V;
+            gd[d] = dvz(dv3(-1.0f * (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
+                                     T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0])),
+                        g.V, zV);
         double Fn = 0.0f;
         for (int d = 0; d < 3; d++) Fn += gd[d] * normal[d];
         for (int d = 0; d < 3; d++) q[d] -= Fn * normal[d];
     }
+    // Per-tet terms of Snac_Heat (temperature/Heat.c:88-126) for the node
+    // gather: (q . n) A / 6 of each face, the lumped heat capacity
+    // Cp rho V / 8, and the thermal stress for the visco-plastic hook.
     if (s.active) {
-        double* h = F.hflux + s.q * 4;
-        h[0] = q[0];
-        h[1] = q[1];
-        h[2] = q[2];
-        if (cfg.thermal_stress) h[3] = tsr;
+        double* h = F.hflux + s.q * HF_STRIDE;
+#pragma unroll
+        for (int f = 0; f < 4; f++) h[f] = dv6((q[0] * g.n[f].x + q[1] * g.n[f].y + q[2] * g.n[f].z) * g.A[f]);
+        // tetra density is set from TimeStepZero on, so the reference's
+        // "density == 0" fallback (Heat.c:120-125) is never taken
+        const double rho = cfg.has_density ? F.density[s.q] : M.density;
+        h[4] = M.heat_capacity * ((rho)*g.V) / 8.0f;
+        if (cfg.thermal_stress) h[5] = tsr;
+        if (s.t == 0) {
+            // Heat.c:127-135, once per element
+            double dt_thermal_to_mech = sqrt((M.lambda + 2.0f * M.mu) / M.density) * F.sc->min_length_scale /
+                                        (M.thermal_conduct / (M.heat_capacity * M.density));
+            if (!(dt_thermal_to_mech > 1.0)) report(F.sc, SNAC_GPU_EPHYSICS, s.e);
+        }
     }
 }
 
@@ -725,50 +748,28 @@ __global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.nn) return;
     const double dt = F.sc->dt;
-    const double minLS = F.sc->min_length_scale;
     int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
-    double energy = 0.0f, source = 0.0f, lumpVolume = 0.0f;
-    const double sourceterm = 0.0;
+    double energy = 0.0f, lumpVolume = 0.0f;
+    // the volumetric source of Snac_Heat is called with sourceterm = 0
+    // (Heat.c:59), which adds +0 to the energy
+    const double source = 0.0f;
 #pragma unroll
     for (int ne = 0; ne < 8; ne++) {
         int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
         if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
         long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
-        const DevMaterial& M = F.mats[phase_of(F, e)];
-        V3 corner[8];
-#pragma unroll
-        for (int cc = 0; cc < 8; cc++) {
-            double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
-            corner[cc] = {p.x, p.y, p.z};
-        }
 #pragma unroll
         for (int idx = 0; idx < 5; idx++) {
-            const int t = node_tet(ne, idx);
-            const int f = node_face(ne, idx);
-            V3 tc[4];
-#pragma unroll
-            for (int qn = 0; qn < 4; qn++) tc[qn] = corner[tet_node(t, qn)];
-            double V = tet_volume(tc[0], tc[1], tc[2], tc[3]);
-            double A;
-            V3 nr;
-            tet_face(tc[face_node(f, 0)], tc[face_node(f, 1)], tc[face_node(f, 2)], A, nr);
-            const long long q = e * NT + t;
-            const double* h = F.hflux + q * 4;
-            energy += (h[0] * nr.x + h[1] * nr.y + h[2] * nr.z) * A / 6.0f;
-            source += sourceterm * V / 4.0f;
-            // tetra density is set from TimeStepZero on, so the reference's
-            // "density == 0" fallback (Heat.c:120-125) is never taken
-            double rho = cfg.has_density ? F.density[q] : M.density;
-            lumpVolume += M.heat_capacity * ((rho)*V) / 8.0f;
+            const long long q = e * NT + node_tet(ne, idx);
+            const double* h = F.hflux + q * HF_STRIDE;
+            energy += h[node_face(ne, idx)];
+            lumpVolume += h[4];
         }
-        double dt_thermal_to_mech = sqrt((M.lambda + 2.0f * M.mu) / M.density) * minLS /
-                                    (M.thermal_conduct / (M.heat_capacity * M.density));
-        if (!(dt_thermal_to_mech > 1.0)) report(F.sc, SNAC_GPU_EPHYSICS, n);
     }
     // only the w slots are written: other threads read this node's x, y, z
     double* pw = reinterpret_cast<double*>(const_cast<double4*>(F.pos) + n) + 3;
     double Told = *pw;
-    double Tnew = Told + (energy + source) * -1.0f * dt / lumpVolume;
+    double Tnew = Told + dv((energy + source) * -1.0f * dt, lumpVolume);
     if (F.tpre) F.tpre[n] = Tnew;
     uchar4 b = F.bc[n];
     if (b.w != 255) Tnew = F.tbc_val[b.w];
@@ -816,6 +817,34 @@ __global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
     for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
     if ((threadIdx.x & 31) == 0 && vcand > 0.0)
         atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
+}
+
+// ---- self-test of the straight-line division against the IEEE quotient -------------------
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long& x) {
+    unsigned long long z = (x += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+}
+__device__ __forceinline__ bool same_bits(double a, double b) {
+    return __double_as_longlong(a) == __double_as_longlong(b) || (a != a && b != b);
+}
+__global__ void k_selftest_division(long long n, unsigned long long seed, unsigned long long* bad) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned long long st = seed ^ (0x632be59bd9b4e019ull * (unsigned long long)(i + 1));
+    unsigned long long local = 0;
+    for (; i < n; i += (long long)gridDim.x * blockDim.x) {
+        unsigned long long a = splitmix64(st), b = splitmix64(st), c = splitmix64(st);
+        // random significands, exponents spread over +-300 (x) and +-130 (y), random signs
+        double x = __longlong_as_double((long long)((a & 0x800fffffffffffffull) | ((unsigned long long)(1023 + (int)(c % 601) - 300) << 52)));
+        double y = __longlong_as_double((long long)((b & 0x800fffffffffffffull) | ((unsigned long long)(1023 + (int)((c >> 20) % 261) - 130) << 52)));
+        if ((c >> 40) % 5 == 0) x = rint(x * 1e-3) * y;         // quotients that are exact or near ties
+        if ((c >> 44) % 97 == 0) x = ((c >> 50) & 1) ? 0.0 : -0.0;
+        local += !same_bits(dv(x, y), x / y);
+        local += !same_bits(dv3(x), x / 3.0) + !same_bits(dv6(x), x / 6.0);
+        local += !same_bits(dv9(x), x / 9.0) + !same_bits(dv10(x), x / 10.0);
+    }
+    if (local) atomicAdd(bad, local);
 }
 
 // _AbstractContext_Execute_Hook: timeStep++ and dt = dtFactor * dt (AbstractContext.c:874-890)

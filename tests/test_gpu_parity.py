@@ -244,3 +244,14 @@ def test_full_size_c3_bit_reproducible_and_hooks_match():
     for f in ("velocity", "stress", "plastic_strain", "viscosity", "temperature"):
         assert np.array_equal(getattr(runs[0], f), getattr(runs[1], f)), f
         assert np.array_equal(getattr(runs[0], f), getattr(runs[2], f)), f
+
+
+def test_straight_line_division_matches_ieee_on_gpu():
+    """the kernels' branch-free division returns the bits of the GPU's IEEE
+    '/' (2^28 random operand pairs x 5 divisors per pair)"""
+    import ctypes as C
+    from snac_b200.context import load_library
+    lib = load_library()
+    bad = C.c_longlong(-1)
+    assert lib.snac_gpu_selftest_division(1 << 28, 12345, C.byref(bad)) == 0
+    assert bad.value == 0
