@@ -106,13 +106,13 @@ struct TetSlot {
     int i, j, k;
 };
 
-__device__ __forceinline__ TetSlot tet_slot(const Mesh& m) {
+__device__ __forceinline__ TetSlot tet_slot(const Mesh& m, int lb) {
     TetSlot s;
     s.lane = threadIdx.x & 31;
     int g = s.lane / 10;
     s.base = g * 10;
     s.t = s.lane - s.base;
-    long long warp = (long long)blockIdx.x * ELEM_WARPS + (threadIdx.x >> 5);
+    long long warp = (long long)lb * ELEM_WARPS + (threadIdx.x >> 5);
     s.e = warp * 3 + g;
     s.active = (g < 3) && (s.e < m.ne);
     if (g >= 3) {  // lanes 30, 31 mirror lane 0-9 group 0 slots so shuffles stay in range
@@ -430,8 +430,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 }
 
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stresses(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
+__device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    TetSlot s = tet_slot(m, lb);
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -443,6 +443,11 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stress
         for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
     }
     stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+}
+
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stresses(Mesh m, Fields F, Config cfg) {
+    k_calc_stresses_body<PLUGIN>(m, F, cfg, blockIdx.x);
 }
 
 // UpdateElement.c:84-91 volume bookkeeping (Maxwell reads V/V_old) and the
@@ -467,9 +472,9 @@ __device__ __forceinline__ void element_update_tet(const Fields& F, const Config
 // same geometry and velocities): one geometry evaluation, one stress
 // read-modify-write.  Used when no energy hook sits between the two.
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
-    if (blockIdx.x == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+__device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    TetSlot s = tet_slot(m, lb);
+    if (lb == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -480,14 +485,19 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(
     stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
 
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
+    k_fused_step_body<PLUGIN>(m, F, cfg, blockIdx.x);
+}
+
 // ======================================================================================
 // Snac_EP_LoopElementsMomentum: UpdateElement.c:54-269 and the minLengthScale
 // reduction of _Snac_Context_LoopElements (Context.c:1156-1184)
 // ======================================================================================
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elements(Mesh m, Fields F, Config cfg,
-                                                                                     int pending) {
-    TetSlot s = tet_slot(m);
+__device__ __forceinline__ void k_update_elements_body(const Mesh& m, const Fields& F, const Config& cfg,
+                                                                                     int pending, int lb) {
+    TetSlot s = tet_slot(m, lb);
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -516,13 +526,19 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elem
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
 
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elements(Mesh m, Fields F, Config cfg,
+                                                                                     int pending) {
+    k_update_elements_body<PLUGIN>(m, F, cfg, pending, blockIdx.x);
+}
+
 // The minimum over all tets and faces of |V/A| (UpdateElement.c:109-139) for
 // the current coordinates, without the rest of the element update.  For a
 // tet, min_f RN(V/A_f) = RN(V / max_f A_f) because correctly rounded
 // division is monotonic, and max_f A_f = RN(sqrt(max_f s_f))/2 for the same
 // reason; faces with A = 0 are skipped as in the reference.
-__global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
-    long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fields& F, int lb) {
+    long long e = (long long)lb * blockDim.x + threadIdx.x;
     double ls = 1.0e+27f;
     if (e < m.ne) {
         int i, j, k;
@@ -563,6 +579,10 @@ __global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
 
+__global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
+    k_min_length_scale_body(m, F, blockIdx.x);
+}
+
 // ======================================================================================
 // Snac_EP_LoopNodesMomentum: Snac_Force (Force.c:53-188), then
 // Snac_UpdateNodeMomentum_PreProcess (UpdateNode.c:74-158) and
@@ -571,8 +591,8 @@ __global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
 // geometry, as in the reference where all forces are summed before any node moves.
 // ======================================================================================
 template <int DTTYPE>
-__global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    long long n = (long long)lb * blockDim.x + threadIdx.x;
     bool active = n < m.nn;
     double vcand = 0.0;
     if (active) {
@@ -628,6 +648,11 @@ __global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg
     for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
     if ((threadIdx.x & 31) == 0 && vcand > 0.0)
         atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
+}
+
+template <int DTTYPE>
+__global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg) {
+    k_loop_nodes_body<DTTYPE>(m, F, cfg, blockIdx.x);
 }
 
 // ======================================================================================
@@ -710,8 +735,8 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
     }
 }
 
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
+__device__ __forceinline__ void k_heat_flux_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    TetSlot s = tet_slot(m, lb);
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -720,12 +745,16 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(M
     heat_flux_tet(m, F, cfg, s, T, T0, g);
 }
 
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg) {
+    k_heat_flux_body(m, F, cfg, blockIdx.x);
+}
+
 // End of step n (element update) fused with the heat flux of step n+1: both
 // need the geometry of the same coordinates.
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(Mesh m, Fields F, Config cfg) {
-    TetSlot s = tet_slot(m);
-    if (blockIdx.x == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+__device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    TetSlot s = tet_slot(m, lb);
+    if (lb == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -740,12 +769,17 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(
     heat_flux_tet(m, F, cfg, s, T, T0, g);
 }
 
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(Mesh m, Fields F, Config cfg) {
+    k_fused_heat_body<PLUGIN>(m, F, cfg, blockIdx.x);
+}
+
 // ======================================================================================
 // Snac_EP_LoopNodesEnergy: Snac_Heat for every node (temperature/Heat.c:64-140),
 // the tet mean temperatures and the temperature BCs (Heat.c:47-62)
 // ======================================================================================
-__global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_heat_nodes_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+    long long n = (long long)lb * blockDim.x + threadIdx.x;
     if (n >= m.nn) return;
     const double dt = F.sc->dt;
     int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
@@ -778,11 +812,14 @@ __global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg
     if (!isfinite(Tnew)) report(F.sc, SNAC_GPU_ENAN, n);
 }
 
+__global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg) {
+    k_heat_nodes_body(m, F, cfg, blockIdx.x);
+}
+
 // ======================================================================================
 // AbstractContext_EP_Sync: _Snac_Context_Sync (Context.c:1208-1268), one thread
 // ======================================================================================
-__global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, double wave_speed) {
     double vmax = __longlong_as_double((long long)sc->vmax_bits);
     const double vlb = 3.0e-11f;
     if (vmax < vlb) vmax = vlb;
@@ -802,10 +839,15 @@ __global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {
     sc->minls_bits = 0x7ff0000000000000ull;  // +inf
 }
 
+__global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    sync_one(cfg, sc, wave_speed);
+}
+
 // max |v| over the velocity-BC nodes from the current velocities, for a
 // Sync that does not follow the node loop (step zero, hook-by-hook callers)
-__global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
-    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void k_vmax_body(const Mesh& m, const Fields& F, int lb) {
+    long long n = (long long)lb * blockDim.x + threadIdx.x;
     double vcand = 0.0;
     if (n < m.nn) {
         uchar4 b = F.bc[n];
@@ -817,6 +859,10 @@ __global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
     for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
     if ((threadIdx.x & 31) == 0 && vcand > 0.0)
         atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
+}
+
+__global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
+    k_vmax_body(m, F, blockIdx.x);
 }
 
 // ---- self-test of the straight-line division against the IEEE quotient -------------------
