@@ -4,8 +4,8 @@
     python bench.py --impl reference ...      # the reference's CPU code on the host cores
 
 A "step" is one _AbstractContext_Step of the model (Solve + Sync) over the
-whole mesh.  The default workload is configs[1]: 64 x 32(y) x 64 hex
-Mohr-Coulomb strain-softening (131,072 hex, 1.31 M tets), synthetic seeded
+whole mesh.  The default workload is the Mohr-Coulomb strain-softening
+plastic model of 64 x 32(y) x 64 hex (131,072 hex, 1.31 M tets), synthetic seeded
 inputs (snac_b200/workloads.py).  Its state (~0.1 GB) fits in the 126 MB L2,
 so a 512 MiB buffer is written between timed steps to flush L2.
 
@@ -37,6 +37,12 @@ UNIT = "element-steps/s"
 # 6 x 8 B x 2 = 96 B per node (nodes per hex below); plastic strain
 # 10 x 8 B x 2 = 160 B; per-element parameter 8 B; node temperature 8 B read.
 NODES_PER_HEX = {"c1": 2601 / 2048, "c2": 139425 / 131072, "c3": 1081665 / 1048576}
+
+
+# DRAM bytes (read + write) of one launch of the dominant kernel, from one
+# ncu capture of that kernel on the same workload
+# (profiles/k_fused_step_plastic_64x32x64.md); None where none was taken.
+NCU_TRAFFIC = {("c2", "k_fused_step"): 83.451392e6 + 173.069056e6}
 
 
 def algorithmic_bytes(workload: str) -> float:
@@ -203,9 +209,9 @@ def run_reference(args, ws, rank):
 
 
 def workload_name(w):
-    return {"c1": "configs[0] elastic 16x8(y)x16 hex over 100x30x100 km",
-            "c2": "configs[1] Mohr-Coulomb strain-softening 64x32(y)x64 hex over 200x40x200 km, lithostatic IC",
-            "c3": "configs[2] Maxwell visco-plastic + temperature 128x64(y)x128 hex over 400x100x400 km"}[w]
+    return {"c1": "elastic 16x8(y)x16 hex over 100x30x100 km",
+            "c2": "Mohr-Coulomb strain-softening 64x32(y)x64 hex over 200x40x200 km, lithostatic IC",
+            "c3": "Maxwell visco-plastic + temperature 128x64(y)x128 hex over 400x100x400 km"}[w]
 
 
 # ---------------------------------------------------------------------------------------------
@@ -320,7 +326,8 @@ def run_ours(args, ws, rank, local):
                        "parallelism": "replicas" if ws > 1 else "single model",
                        "arithmetic": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle"},
             "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
-                         "frac": achieved_kernel / peak, "traffic": None, "kernel": top,
+                         "frac": achieved_kernel / peak, "traffic": NCU_TRAFFIC.get((args.workload, top)),
+                         "kernel": top,
                          "kernel_ms": kern_ms[top], "algorithmic_bytes_per_hex": kb,
                          "peak_source": peak_kind,
                          "step": {"achieved": achieved_step, "frac": achieved_step / peak,

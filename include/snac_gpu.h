@@ -235,6 +235,52 @@ int  snac_gpu_device_count(void);
  * IEEE quotient of the GPU; *mismatches receives the count (expected 0). */
 int  snac_gpu_selftest_division(long long n, unsigned long long seed, long long* mismatches);
 
+/* ---- batched ensembles ------------------------------------------------------
+ * No counterpart in the reference, which runs one model per process (one
+ * Snac_Context per MPI job).  A batch holds n independent models, each built
+ * from its own descriptor exactly as snac_gpu_create builds it (uneven mesh
+ * sizes, rheologies and materials allowed), and advances all of them with ONE
+ * launch per kernel type per step: each launch walks a list of work tiles
+ * (model, block) over every model, and the step loop runs from CUDA graphs.
+ * Per-model results are bit-identical to stepping each model on its own.
+ * The models share one CUDA stream; snac_gpu_batch_model() returns a model's
+ * handle, through which state is downloaded or uploaded and scalars read
+ * (those calls are stream-ordered with the batch's steps). */
+typedef struct snac_gpu_batch snac_gpu_batch;
+
+typedef struct snac_batch_tuning {
+    int node_threads;       /* threads per node tile (64, 128, 256): nodes per tile        */
+    int minls_threads;      /* threads per min-length-scale tile (64, 128, 256)            */
+    int elem_blocks_per_sm; /* element launches: 0 = one block per tile, k > 0 = a
+                               persistent grid of k x SMs blocks striding over the tiles */
+    int node_blocks_per_sm; /* the same for the node launches                                */
+    int steps_per_graph;    /* steps captured in one CUDA graph (1..256)                     */
+    int order;              /* tile order: 0 = largest model first, 1 = model order          */
+} snac_batch_tuning;
+
+int  snac_gpu_batch_create(const snac_gpu_desc* descs, int n_models, snac_gpu_batch** out);
+void snac_gpu_batch_destroy(snac_gpu_batch* b);
+/* Snac_Context_TimeStepZero of every model. */
+int  snac_gpu_batch_time_step_zero(snac_gpu_batch* b);
+/* nsteps steps of every model, one launch per kernel type per step. */
+int  snac_gpu_batch_step(snac_gpu_batch* b, int nsteps);
+/* The same nsteps steps, model after model, each model's step with its own
+ * launches (its snac_gpu_step graph) on the shared stream: the
+ * one-launch-per-model baseline the batched form is measured against. */
+int  snac_gpu_batch_step_each(snac_gpu_batch* b, int nsteps);
+snac_gpu* snac_gpu_batch_model(snac_gpu_batch* b, int i);
+int  snac_gpu_batch_size(const snac_gpu_batch* b);
+int  snac_gpu_batch_get_tuning(const snac_gpu_batch* b, snac_batch_tuning* out);
+/* Applies a launch shape (validated; SNAC_GPU_EINVAL if out of range). */
+int  snac_gpu_batch_set_tuning(snac_gpu_batch* b, const snac_batch_tuning* t);
+/* Runs nsteps batched steps and returns their device time in *ms (CUDA
+ * events on the batch stream around the launches): the autotuner's probe. */
+int  snac_gpu_batch_time_steps(snac_gpu_batch* b, int nsteps, int each, double* ms);
+const char* snac_gpu_batch_last_error(const snac_gpu_batch* b);
+int  snac_gpu_batch_error_model(const snac_gpu_batch* b);  /* model of the last error, -1 if none */
+long long snac_gpu_batch_launch_count(const snac_gpu_batch* b);
+void* snac_gpu_batch_stream(snac_gpu_batch* b);
+
 #ifdef __cplusplus
 }
 #endif

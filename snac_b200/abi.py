@@ -118,6 +118,21 @@ class KernelTime(C.Structure):
     _fields_ = [("name", C.c_char * 40), ("ms", C.c_double)]
 
 
+class BatchTuning(C.Structure):
+    _fields_ = [("node_threads", C.c_int), ("minls_threads", C.c_int), ("elem_blocks_per_sm", C.c_int),
+                ("node_blocks_per_sm", C.c_int), ("steps_per_graph", C.c_int), ("order", C.c_int)]
+
+    def as_dict(self) -> Dict[str, int]:
+        return {k: int(getattr(self, k)) for k, _ in self._fields_}
+
+    @classmethod
+    def from_dict(cls, d: Dict[str, int]) -> "BatchTuning":
+        t = cls()
+        for k, _ in cls._fields_:
+            setattr(t, k, int(d[k]))
+        return t
+
+
 class Scalars(C.Structure):
     _fields_ = [("dt", C.c_double), ("min_length_scale", C.c_double), ("vmax", C.c_double),
                 ("speed_of_sound", C.c_double), ("time_step", C.c_longlong)]

@@ -14,7 +14,7 @@ import ctypes as C
 import os
 from typing import Optional
 
-from .abi import NT, STATUS_NAMES, Desc, KernelTime, Scalars, SnacConfig, State, StateView
+from .abi import NT, STATUS_NAMES, BatchTuning, Desc, KernelTime, Scalars, SnacConfig, State, StateView
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libsnac_b200.so")
@@ -74,12 +74,56 @@ def load_library(path: str = LIB_PATH):
     lib.snac_gpu_selftest_division.restype = C.c_int
     lib.snac_gpu_device_count.argtypes = []
     lib.snac_gpu_device_count.restype = C.c_int
+    # batched ensembles
+    lib.snac_gpu_batch_create.argtypes = [C.POINTER(Desc), C.c_int, C.POINTER(vp)]
+    lib.snac_gpu_batch_create.restype = C.c_int
+    lib.snac_gpu_batch_destroy.argtypes = [vp]
+    lib.snac_gpu_batch_destroy.restype = None
+    lib.snac_gpu_batch_time_step_zero.argtypes = [vp]
+    lib.snac_gpu_batch_time_step_zero.restype = C.c_int
+    for n in ("step", "step_each"):
+        f = getattr(lib, "snac_gpu_batch_" + n)
+        f.argtypes = [vp, C.c_int]
+        f.restype = C.c_int
+    lib.snac_gpu_batch_model.argtypes = [vp, C.c_int]
+    lib.snac_gpu_batch_model.restype = vp
+    lib.snac_gpu_batch_size.argtypes = [vp]
+    lib.snac_gpu_batch_size.restype = C.c_int
+    lib.snac_gpu_batch_get_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    lib.snac_gpu_batch_get_tuning.restype = C.c_int
+    lib.snac_gpu_batch_set_tuning.argtypes = [vp, C.POINTER(BatchTuning)]
+    lib.snac_gpu_batch_set_tuning.restype = C.c_int
+    lib.snac_gpu_batch_time_steps.argtypes = [vp, C.c_int, C.c_int, C.POINTER(C.c_double)]
+    lib.snac_gpu_batch_time_steps.restype = C.c_int
+    lib.snac_gpu_batch_last_error.argtypes = [vp]
+    lib.snac_gpu_batch_last_error.restype = C.c_char_p
+    lib.snac_gpu_batch_error_model.argtypes = [vp]
+    lib.snac_gpu_batch_error_model.restype = C.c_int
+    lib.snac_gpu_batch_launch_count.argtypes = [vp]
+    lib.snac_gpu_batch_launch_count.restype = C.c_longlong
+    lib.snac_gpu_batch_stream.argtypes = [vp]
+    lib.snac_gpu_batch_stream.restype = vp
     _LIB = lib
     return lib
 
 
 class SnacContext:
     """One model on the GPU (one snac_gpu handle)."""
+
+    owned = True
+
+    @classmethod
+    def borrowed(cls, cfg: SnacConfig, handle: int, owner) -> "SnacContext":
+        """A view of a model whose handle belongs to `owner` (a batch): same
+        methods, but closing it does not destroy the model."""
+        self = cls.__new__(cls)
+        self.lib = load_library()
+        self.cfg = cfg
+        self.h = C.c_void_p(handle)
+        self.ne, self.nn = cfg.n_elements, cfg.n_nodes
+        self.owned = False
+        self._owner = owner
+        return self
 
     def __init__(self, cfg: SnacConfig):
         self.lib = load_library()
@@ -98,7 +142,8 @@ class SnacContext:
     # -- lifetime ---------------------------------------------------------------------
     def close(self):
         if self.h:
-            self.lib.snac_gpu_destroy(self.h)
+            if self.owned:
+                self.lib.snac_gpu_destroy(self.h)
             self.h = C.c_void_p()
 
     def __del__(self):

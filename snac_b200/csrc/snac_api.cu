@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "snac_gpu.h"
+#include "snac_batch.cuh"
 #include "snac_kernels.cuh"
 
 using namespace snac;
@@ -29,6 +30,7 @@ struct snac_gpu {
     int n_phases = 0;
     double wave_speed = 0.0;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;  // false for the models of a batch, which share the batch's stream
     // device buffers
     double4* pos[2] = {nullptr, nullptr};
     double4* vel = nullptr;
@@ -52,6 +54,7 @@ struct snac_gpu {
     double* fric_scale = nullptr;
     double* visc_scale = nullptr;
     DevScalars* sc = nullptr;
+    double* stage = nullptr;  // host-transfer staging, 3 doubles per node (first upload/download)
     // host mirror of the step bookkeeping
     int parity = 0;
     long long time_step = 0;
@@ -153,10 +156,10 @@ DevMaterial to_dev(const snac_material& s, bool fric_scaled) {
     return d;
 }
 
-Fields fields(snac_gpu* h) {
+Fields fields_at(const snac_gpu* h, int parity) {
     Fields F;
-    F.pos = h->pos[h->parity];
-    F.pos_next = h->pos[h->parity ^ 1];
+    F.pos = h->pos[parity];
+    F.pos_next = h->pos[parity ^ 1];
     F.vel = h->vel;
     F.force = h->force;
     F.stress = h->stress;
@@ -180,6 +183,8 @@ Fields fields(snac_gpu* h) {
     F.sc = h->sc;
     return F;
 }
+
+Fields fields(const snac_gpu* h) { return fields_at(h, h->parity); }
 
 unsigned elem_blocks(const Mesh& m) { return (unsigned)((m.ne + ELEM_PER_BLOCK - 1) / ELEM_PER_BLOCK); }
 unsigned node_blocks(const Mesh& m) { return (unsigned)((m.nn + 127) / 128); }
@@ -362,6 +367,62 @@ int read_status(snac_gpu* h) {
     return 0;
 }
 
+// one step from the handle's CUDA graph for its (pending, parity) state,
+// captured on first use; no status read
+int launch_step(snac_gpu* h) {
+    int p = h->parity, f = h->pending ? 1 : 0;
+    if (!h->graph[f][p]) {
+        cudaGraph_t g;
+        long long l0 = h->launches, ts0 = h->time_step;
+        CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        int rc = record_step(h, f == 1);
+        cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+        if (rc) return rc;
+        if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "graph capture: %s", cudaGetErrorString(e));
+        CK(cudaGraphInstantiate(&h->graph[f][p], g, 0));
+        cudaGraphDestroy(g);
+        h->steps_kernels[f] = (int)(h->launches - l0);
+        h->launches = l0;  // counted again below, when the graph actually runs
+        h->time_step = ts0;
+        h->parity = p;
+    }
+    CK(cudaGraphLaunch(h->graph[f][p], h->stream));
+    h->launches += h->steps_kernels[f];
+    h->time_step++;
+    h->parity ^= 1;
+    h->pending = true;
+    return 0;
+}
+
+// node-field transfers through a device staging buffer of 3 doubles per
+// node (allocated on first use), repacked by a kernel on the handle's stream
+int ensure_stage(snac_gpu* h) {
+    if (h->stage) return 0;
+    return dalloc(h, &h->stage, (size_t)h->mesh.nn * 3);
+}
+
+int node_in(snac_gpu* h, double4* dst, const double* src, int what) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long nn = h->mesh.nn;
+    CK(cudaMemcpyAsync(h->stage, src, nn * (what == 0 ? 3 : 1) * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    k_unpack_nodes<<<(unsigned)((nn + 255) / 256), 256, 0, h->stream>>>(dst, h->stage, nn, what);
+    h->launches++;
+    return launch_check_named(h, "k_unpack_nodes");
+}
+
+int node_out(snac_gpu* h, const double4* src, double* dst, int what) {
+    int rc = ensure_stage(h);
+    if (rc) return rc;
+    const long long nn = h->mesh.nn;
+    k_pack_nodes<<<(unsigned)((nn + 255) / 256), 256, 0, h->stream>>>(src, h->stage, nn, what);
+    h->launches++;
+    if ((rc = launch_check_named(h, "k_pack_nodes"))) return rc;
+    CK(cudaMemcpyAsync(dst, h->stage, nn * (what == 0 ? 3 : 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    // the next transfer reuses the staging buffer only after this copy (same stream)
+    return 0;
+}
+
 // hydroStaticIC/VariableConditions.c:43-152 on one rank: lithostatic
 // pressure integrated down each element column; densities are the phase
 // densities (tet densities are still zero at this point of the reference's IC).
@@ -423,7 +484,8 @@ int snac_gpu_device_count(void) {
     return n;
 }
 
-int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
+// Builds a model; with shared != null the model uses that stream (batches)
+static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t shared) {
     if (!out) return SNAC_GPU_EINVAL;
     *out = nullptr;
     if (!d || d->abi_version != SNAC_GPU_ABI_VERSION) return SNAC_GPU_EINVAL;
@@ -475,7 +537,12 @@ int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
     c.gravity = d->gravity;
     c.demf = d->demf;
     c.strain_inert = d->strain_inert;
-    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    if (shared) {
+        h->stream = shared;
+        h->own_stream = false;
+    } else {
+        CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    }
 
     const long long ne = m.ne, nn = m.nn, nq = ne * NT;
     int rc = 0;
@@ -618,6 +685,8 @@ int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) {
     return 0;
 }
 
+int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) { return create_model(d, out, nullptr); }
+
 void snac_gpu_destroy(snac_gpu* h) {
     if (!h) return;
     if (h->stream) cudaStreamSynchronize(h->stream);
@@ -626,10 +695,10 @@ void snac_gpu_destroy(snac_gpu* h) {
             if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
-                    h->visc_scale, h->sc};
+                    h->visc_scale, h->sc, h->stage};
     for (void* b : bufs)
         if (b) cudaFree(b);
-    if (h->stream) cudaStreamDestroy(h->stream);
+    if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
     delete h;
 }
 
@@ -661,27 +730,8 @@ int snac_gpu_step(snac_gpu* h, int nsteps) {
     if (!h || nsteps < 0) return SNAC_GPU_EINVAL;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
     for (int s = 0; s < nsteps; s++) {
-        int p = h->parity, f = h->pending ? 1 : 0;
-        if (!h->graph[f][p]) {
-            cudaGraph_t g;
-            long long l0 = h->launches, ts0 = h->time_step;
-            CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-            int rc = record_step(h, f == 1);
-            cudaError_t e = cudaStreamEndCapture(h->stream, &g);
-            if (rc) return rc;
-            if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "graph capture: %s", cudaGetErrorString(e));
-            CK(cudaGraphInstantiate(&h->graph[f][p], g, 0));
-            cudaGraphDestroy(g);
-            h->steps_kernels[f] = (int)(h->launches - l0);
-            h->launches = l0;  // counted again below, when the graph actually runs
-            h->time_step = ts0;
-            h->parity = p;
-        }
-        CK(cudaGraphLaunch(h->graph[f][p], h->stream));
-        h->launches += h->steps_kernels[f];
-        h->time_step++;
-        h->parity ^= 1;
-        h->pending = true;
+        int rc = launch_step(h);
+        if (rc) return rc;
     }
     return read_status(h);
 }
@@ -731,67 +781,39 @@ int snac_gpu_upload(snac_gpu* h, const snac_state_view* v) {
     if (!h || !v) return SNAC_GPU_EINVAL;
     if (int rc = flush_pending(h)) return rc;
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
-    if (v->coord || v->velocity || v->temperature) {
-        std::vector<double4> p(nn), w(nn);
-        CK(cudaMemcpy(p.data(), h->pos[h->parity], nn * sizeof(double4), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(w.data(), h->vel, nn * sizeof(double4), cudaMemcpyDeviceToHost));
-        for (long long n = 0; n < nn; n++) {
-            if (v->coord) p[n] = make_double4(v->coord[n * 3], v->coord[n * 3 + 1], v->coord[n * 3 + 2], p[n].w);
-            if (v->velocity) w[n] = make_double4(v->velocity[n * 3], v->velocity[n * 3 + 1], v->velocity[n * 3 + 2], w[n].w);
-            if (v->temperature) p[n].w = v->temperature[n];
-        }
-        CK(cudaMemcpy(h->pos[h->parity], p.data(), nn * sizeof(double4), cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(h->vel, w.data(), nn * sizeof(double4), cudaMemcpyHostToDevice));
-    }
-    if (v->stress) CK(cudaMemcpy(h->stress, v->stress, nq * 6 * sizeof(double), cudaMemcpyHostToDevice));
-    if (v->plastic_strain && h->eps_p) CK(cudaMemcpy(h->eps_p, v->plastic_strain, nq * sizeof(double), cudaMemcpyHostToDevice));
-    if (v->viscosity && h->visc) CK(cudaMemcpy(h->visc, v->viscosity, nq * sizeof(double), cudaMemcpyHostToDevice));
+    int rc;
+    // every copy and repacking kernel is ordered on the handle's stream
+    if (v->coord && (rc = node_in(h, h->pos[h->parity], v->coord, 0))) return rc;
+    if (v->velocity && (rc = node_in(h, h->vel, v->velocity, 0))) return rc;
+    if (v->temperature && (rc = node_in(h, h->pos[h->parity], v->temperature, 1))) return rc;
+    if (v->stress) CK(cudaMemcpyAsync(h->stress, v->stress, nq * 6 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (v->plastic_strain && h->eps_p)
+        CK(cudaMemcpyAsync(h->eps_p, v->plastic_strain, nq * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (v->viscosity && h->visc)
+        CK(cudaMemcpyAsync(h->visc, v->viscosity, nq * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    CK(cudaStreamSynchronize(h->stream));  // the caller may reuse its buffers on return
+    (void)nn;
     return 0;
 }
 
 int snac_gpu_download(snac_gpu* h, const snac_state_view* v) {
     if (!h || !v) return SNAC_GPU_EINVAL;
     if (int rc = flush_pending(h)) return rc;
+    const long long nq = h->mesh.ne * NT;
+    int rc;
+    if (v->coord && (rc = node_out(h, h->pos[h->parity], v->coord, 0))) return rc;
+    if (v->velocity && (rc = node_out(h, h->vel, v->velocity, 0))) return rc;
+    if (v->temperature && (rc = node_out(h, h->pos[h->parity], v->temperature, 1))) return rc;
+    if (v->force && (rc = node_out(h, h->force, v->force, 0))) return rc;
+    if (v->inertial_mass && (rc = node_out(h, h->force, v->inertial_mass, 1))) return rc;
+    if (v->stress) CK(cudaMemcpyAsync(v->stress, h->stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (v->plastic_strain && h->eps_p)
+        CK(cudaMemcpyAsync(v->plastic_strain, h->eps_p, nq * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    if (v->viscosity && h->visc)
+        CK(cudaMemcpyAsync(v->viscosity, h->visc, nq * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
-    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
-    if (v->coord || v->velocity || v->temperature || v->force || v->inertial_mass) {
-        std::vector<double4> p(nn), w(nn), f(nn);
-        CK(cudaMemcpy(p.data(), h->pos[h->parity], nn * sizeof(double4), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(w.data(), h->vel, nn * sizeof(double4), cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(f.data(), h->force, nn * sizeof(double4), cudaMemcpyDeviceToHost));
-        for (long long n = 0; n < nn; n++) {
-            if (v->coord) {
-                v->coord[n * 3] = p[n].x;
-                v->coord[n * 3 + 1] = p[n].y;
-                v->coord[n * 3 + 2] = p[n].z;
-            }
-            if (v->velocity) {
-                v->velocity[n * 3] = w[n].x;
-                v->velocity[n * 3 + 1] = w[n].y;
-                v->velocity[n * 3 + 2] = w[n].z;
-            }
-            if (v->temperature) v->temperature[n] = p[n].w;
-            if (v->force) {
-                v->force[n * 3] = f[n].x;
-                v->force[n * 3 + 1] = f[n].y;
-                v->force[n * 3 + 2] = f[n].z;
-            }
-            if (v->inertial_mass) v->inertial_mass[n] = f[n].w;
-        }
-    }
-    if (v->stress) CK(cudaMemcpy(v->stress, h->stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToHost));
-    if (v->plastic_strain) {
-        if (h->eps_p)
-            CK(cudaMemcpy(v->plastic_strain, h->eps_p, nq * sizeof(double), cudaMemcpyDeviceToHost));
-        else
-            memset(v->plastic_strain, 0, nq * sizeof(double));
-    }
-    if (v->viscosity) {
-        if (h->visc)
-            CK(cudaMemcpy(v->viscosity, h->visc, nq * sizeof(double), cudaMemcpyDeviceToHost));
-        else
-            memset(v->viscosity, 0, nq * sizeof(double));
-    }
+    if (v->plastic_strain && !h->eps_p) memset(v->plastic_strain, 0, nq * sizeof(double));
+    if (v->viscosity && !h->visc) memset(v->viscosity, 0, nq * sizeof(double));
     return 0;
 }
 
@@ -852,5 +874,396 @@ int snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max) {
     return rc ? rc : h->prof_n;
 }
 void* snac_gpu_stream(snac_gpu* h) { return h ? (void*)h->stream : nullptr; }
+
+}  // extern "C"
+
+// ======================================================================================
+// Batched ensembles: every model keeps its own buffers; the batch adds per-model
+// descriptors (one table per coordinate parity) and tile lists, and launches
+// each kernel type once per step over all models.
+// ======================================================================================
+struct snac_gpu_batch {
+    std::vector<snac_gpu*> models;
+    cudaStream_t stream = nullptr;
+    int n = 0;
+    int n_sm = 148;
+    ModelDesc* desc[2] = {nullptr, nullptr};  // [parity]
+    int2* tiles = nullptr;
+    size_t tiles_cap = 0;
+    struct List {
+        long long off = 0;
+        int n = 0;
+    };
+    List elem_all, elem_temp, node_all, node_temp, minls_all;
+    bool any_temp = false;
+    snac_batch_tuning tune{128, 128, 0, 0, 8, 0};
+    bool tiles_dirty = true;
+    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [multi-step chunk][start parity]
+    int graph_kernels[2] = {0, 0};
+    ModelStatus* d_status = nullptr;
+    std::vector<ModelStatus> h_status;
+    int parity = 0;
+    long long launches = 0;
+    cudaEvent_t ev[2] = {nullptr, nullptr};
+    char err[512] = {0};
+    int err_model = -1;
+};
+
+namespace {
+
+int bset_err(snac_gpu_batch* b, int code, int model, const char* fmt, ...) {
+    if (!b) return code;
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(b->err, sizeof b->err, fmt, ap);
+    va_end(ap);
+    b->err_model = model;
+    return code;
+}
+
+#define BCK(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) return bset_err(b, SNAC_GPU_ECUDA, -1, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+void drop_graphs(snac_gpu_batch* b) {
+    for (auto& gc : b->graph)
+        for (auto& g : gc)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+}
+
+int build_desc(snac_gpu_batch* b) {
+    std::vector<ModelDesc> d(b->n);
+    for (int p = 0; p < 2; p++) {
+        for (int i = 0; i < b->n; i++) {
+            const snac_gpu* h = b->models[i];
+            d[i].m = h->mesh;
+            d[i].F = fields_at(h, p);
+            d[i].cfg = h->cfg;
+            d[i].cfg.time_step_zero = 0;
+            d[i].wave_speed = h->wave_speed;
+        }
+        BCK(cudaMemcpyAsync(b->desc[p], d.data(), b->n * sizeof(ModelDesc), cudaMemcpyHostToDevice, b->stream));
+        BCK(cudaStreamSynchronize(b->stream));
+    }
+    return 0;
+}
+
+// Tile lists for the current launch shape.  Order 0 puts the largest models
+// first (longest-processing-time first), so the last wave of a launch holds
+// the small tiles.
+int build_tiles(snac_gpu_batch* b) {
+    std::vector<int> order(b->n);
+    for (int i = 0; i < b->n; i++) order[i] = i;
+    if (b->tune.order == 0)
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int x, int y) { return b->models[x]->mesh.ne > b->models[y]->mesh.ne; });
+    std::vector<int2> t;
+    auto add = [&](snac_gpu_batch::List& L, bool temp_only, int kind) {
+        L.off = (long long)t.size();
+        for (int i : order) {
+            const snac_gpu* h = b->models[i];
+            if (temp_only && !h->temperature) continue;
+            long long nb = kind == 0   ? (long long)elem_blocks(h->mesh)
+                           : kind == 1 ? (h->mesh.nn + b->tune.node_threads - 1) / b->tune.node_threads
+                                       : (h->mesh.ne + b->tune.minls_threads - 1) / b->tune.minls_threads;
+            for (long long k = 0; k < nb; k++) t.push_back(make_int2(i, (int)k));
+        }
+        L.n = (int)((long long)t.size() - L.off);
+    };
+    add(b->elem_all, false, 0);
+    add(b->elem_temp, true, 0);
+    add(b->node_all, false, 1);
+    add(b->node_temp, true, 1);
+    add(b->minls_all, false, 2);
+    if (t.size() > (size_t)0x7fffffff) return bset_err(b, SNAC_GPU_EINVAL, -1, "too many tiles in one batch");
+    if (t.size() > b->tiles_cap) {
+        if (b->tiles) cudaFree(b->tiles);
+        b->tiles = nullptr;
+        b->tiles_cap = 0;
+        cudaError_t e = cudaMalloc((void**)&b->tiles, t.size() * sizeof(int2));
+        if (e != cudaSuccess) return bset_err(b, SNAC_GPU_ENOMEM, -1, "cudaMalloc(tiles): %s", cudaGetErrorString(e));
+        b->tiles_cap = t.size();
+    }
+    BCK(cudaMemcpyAsync(b->tiles, t.data(), t.size() * sizeof(int2), cudaMemcpyHostToDevice, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    drop_graphs(b);
+    b->tiles_dirty = false;
+    return 0;
+}
+
+unsigned tile_grid(const snac_gpu_batch* b, int ntiles, int per_sm) {
+    long long g = ntiles;
+    if (per_sm > 0) g = std::min<long long>(g, (long long)per_sm * b->n_sm);
+    return (unsigned)std::max<long long>(g, 1);
+}
+
+int bcheck_launch(snac_gpu_batch* b, const char* name) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return bset_err(b, SNAC_GPU_ECUDA, -1, "%s launch: %s", name, cudaGetErrorString(e));
+    b->launches++;
+    return 0;
+}
+
+template <int OP>
+int blaunch_elem(snac_gpu_batch* b, const ModelDesc* D, const snac_gpu_batch::List& L) {
+    if (L.n == 0) return 0;
+    kb_elements<OP><<<tile_grid(b, L.n, b->tune.elem_blocks_per_sm), ELEM_WARPS * 32, 0, b->stream>>>(D, b->tiles + L.off, L.n);
+    return bcheck_launch(b, "kb_elements");
+}
+
+template <int OP>
+int blaunch_nodes(snac_gpu_batch* b, const ModelDesc* D, const snac_gpu_batch::List& L, int threads) {
+    if (L.n == 0) return 0;
+    kb_nodes<OP><<<tile_grid(b, L.n, b->tune.node_blocks_per_sm), threads, 0, b->stream>>>(D, b->tiles + L.off, L.n);
+    return bcheck_launch(b, "kb_nodes");
+}
+
+// one step of every model, in the order of record_step
+int record_batch_step(snac_gpu_batch* b, bool fused, int parity) {
+    const ModelDesc* D = b->desc[parity];
+    const unsigned mb = (unsigned)((b->n + 127) / 128);
+    int rc;
+    if (fused) {
+        if ((rc = blaunch_elem<BOP_FUSED>(b, D, b->elem_all))) return rc;
+    } else {
+        kb_begin_step<<<mb, 128, 0, b->stream>>>(D, b->n);
+        if ((rc = bcheck_launch(b, "kb_begin_step"))) return rc;
+        if ((rc = blaunch_elem<BOP_HEAT_FLUX>(b, D, b->elem_temp))) return rc;
+    }
+    if ((rc = blaunch_nodes<BOP_HEAT_NODES>(b, D, b->node_temp, b->tune.node_threads))) return rc;
+    if ((rc = blaunch_elem<BOP_STRESS>(b, D, fused ? b->elem_temp : b->elem_all))) return rc;
+    if ((rc = blaunch_nodes<BOP_LOOP_NODES>(b, D, b->node_all, b->tune.node_threads))) return rc;
+    // the node loop wrote the new coordinates into the other buffer
+    const ModelDesc* Dn = b->desc[parity ^ 1];
+    if ((rc = blaunch_nodes<BOP_MINLS>(b, Dn, b->minls_all, b->tune.minls_threads))) return rc;
+    kb_sync<<<mb, 128, 0, b->stream>>>(D, b->n);
+    return bcheck_launch(b, "kb_sync");
+}
+
+// models of a batch step together: same parity, all past step zero, and
+// either all or none with a deferred element update (a model whose state was
+// downloaded on its own has had its update applied; the others are flushed too)
+int batch_prepare(snac_gpu_batch* b, bool* fused) {
+    int npending = 0;
+    for (int i = 0; i < b->n; i++) {
+        snac_gpu* h = b->models[i];
+        if (!h->zero_done) return bset_err(b, SNAC_GPU_ESTATE, i, "model %d: time step zero must come first", i);
+        if (h->parity != b->models[0]->parity)
+            return bset_err(b, SNAC_GPU_ESTATE, i, "model %d was stepped on its own: the models are out of step", i);
+        npending += h->pending ? 1 : 0;
+    }
+    if (npending != 0 && npending != b->n) {
+        for (int i = 0; i < b->n; i++) {
+            int rc = flush_pending(b->models[i]);
+            if (rc) return bset_err(b, rc, i, "model %d: %s", i, b->models[i]->err);
+        }
+        npending = 0;
+    }
+    *fused = npending == b->n;
+    b->parity = b->models[0]->parity;
+    if (b->tiles_dirty) return build_tiles(b);
+    return 0;
+}
+
+// launches nsteps batched steps (no status read)
+int batch_run(snac_gpu_batch* b, int nsteps) {
+    bool fused;
+    int rc;
+    if ((rc = batch_prepare(b, &fused))) return rc;
+    int s = 0;
+    if (!fused && nsteps > 0) {
+        if ((rc = record_batch_step(b, false, b->parity))) return rc;
+        b->parity ^= 1;
+        s = 1;
+    }
+    const int S = b->tune.steps_per_graph;
+    while (s < nsteps) {
+        const int chunk = (S > 1 && nsteps - s >= S) ? 1 : 0;
+        const int k = chunk ? S : 1;
+        cudaGraphExec_t& ge = b->graph[chunk][b->parity];
+        if (!ge) {
+            cudaGraph_t g;
+            long long l0 = b->launches;
+            BCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+            int rc2 = 0;
+            for (int j = 0; j < k && !rc2; j++) rc2 = record_batch_step(b, true, b->parity ^ (j & 1));
+            cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+            if (rc2) return rc2;
+            if (e != cudaSuccess) return bset_err(b, SNAC_GPU_ECUDA, -1, "graph capture: %s", cudaGetErrorString(e));
+            e = cudaGraphInstantiate(&ge, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return bset_err(b, SNAC_GPU_ECUDA, -1, "graph instantiate: %s", cudaGetErrorString(e));
+            b->graph_kernels[chunk] = (int)(b->launches - l0);
+            b->launches = l0;
+        }
+        BCK(cudaGraphLaunch(ge, b->stream));
+        b->launches += b->graph_kernels[chunk];
+        s += k;
+        b->parity ^= (k & 1);
+    }
+    for (snac_gpu* h : b->models) {
+        h->time_step += nsteps;
+        h->parity = b->parity;
+        if (nsteps > 0) h->pending = true;
+    }
+    return 0;
+}
+
+// the same steps model by model, each with its own step graph
+int batch_run_each(snac_gpu_batch* b, int nsteps) {
+    bool fused;
+    int rc;
+    if ((rc = batch_prepare(b, &fused))) return rc;
+    for (int s = 0; s < nsteps; s++)
+        for (int i = 0; i < b->n; i++) {
+            snac_gpu* h = b->models[i];
+            long long l0 = h->launches;
+            if ((rc = launch_step(h))) return bset_err(b, rc, i, "model %d: %s", i, h->err);
+            b->launches += h->launches - l0;
+        }
+    b->parity = b->models[0]->parity;
+    return 0;
+}
+
+int batch_status(snac_gpu_batch* b) {
+    kb_status<<<(unsigned)((b->n + 127) / 128), 128, 0, b->stream>>>(b->desc[0], b->n, b->d_status);
+    BCK(cudaGetLastError());
+    BCK(cudaMemcpyAsync(b->h_status.data(), b->d_status, b->n * sizeof(ModelStatus), cudaMemcpyDeviceToHost, b->stream));
+    BCK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < b->n; i++) {
+        if (b->h_status[i].status) {
+            int rc = read_status(b->models[i]);  // the model's own message
+            return bset_err(b, rc ? rc : b->h_status[i].status, i, "model %d: %s", i, b->models[i]->err);
+        }
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int snac_gpu_batch_create(const snac_gpu_desc* descs, int n_models, snac_gpu_batch** out) {
+    if (!out) return SNAC_GPU_EINVAL;
+    *out = nullptr;
+    if (!descs || n_models < 1) return SNAC_GPU_EINVAL;
+    snac_gpu_batch* b = new (std::nothrow) snac_gpu_batch();
+    if (!b) return SNAC_GPU_ENOMEM;
+    *out = b;
+    int dev = 0;
+    BCK(cudaGetDevice(&dev));
+    BCK(cudaDeviceGetAttribute(&b->n_sm, cudaDevAttrMultiProcessorCount, dev));
+    BCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BCK(cudaEventCreate(&b->ev[0]));
+    BCK(cudaEventCreate(&b->ev[1]));
+    b->n = n_models;
+    b->models.assign(n_models, nullptr);
+    for (int i = 0; i < n_models; i++) {
+        int rc = create_model(&descs[i], &b->models[i], b->stream);
+        if (rc) {
+            const char* msg = b->models[i] ? b->models[i]->err : "invalid descriptor";
+            return bset_err(b, rc, i, "model %d: %s", i, msg[0] ? msg : "invalid descriptor");
+        }
+        b->any_temp = b->any_temp || b->models[i]->temperature;
+    }
+    cudaError_t e = cudaMalloc((void**)&b->desc[0], n_models * sizeof(ModelDesc));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->desc[1], n_models * sizeof(ModelDesc));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&b->d_status, n_models * sizeof(ModelStatus));
+    if (e != cudaSuccess) return bset_err(b, SNAC_GPU_ENOMEM, -1, "cudaMalloc: %s", cudaGetErrorString(e));
+    b->h_status.resize(n_models);
+    return build_desc(b);
+}
+
+void snac_gpu_batch_destroy(snac_gpu_batch* b) {
+    if (!b) return;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graphs(b);
+    for (snac_gpu* h : b->models)
+        if (h) snac_gpu_destroy(h);
+    void* bufs[] = {b->desc[0], b->desc[1], b->tiles, b->d_status};
+    for (void* p : bufs)
+        if (p) cudaFree(p);
+    for (cudaEvent_t ev : b->ev)
+        if (ev) cudaEventDestroy(ev);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int snac_gpu_batch_time_step_zero(snac_gpu_batch* b) {
+    if (!b) return SNAC_GPU_EINVAL;
+    for (int i = 0; i < b->n; i++) {
+        int rc = snac_gpu_time_step_zero(b->models[i]);
+        if (rc) return bset_err(b, rc, i, "model %d: %s", i, b->models[i]->err);
+    }
+    return 0;
+}
+
+int snac_gpu_batch_step(snac_gpu_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return SNAC_GPU_EINVAL;
+    int rc = batch_run(b, nsteps);
+    return rc ? rc : batch_status(b);
+}
+
+int snac_gpu_batch_step_each(snac_gpu_batch* b, int nsteps) {
+    if (!b || nsteps < 0) return SNAC_GPU_EINVAL;
+    int rc = batch_run_each(b, nsteps);
+    return rc ? rc : batch_status(b);
+}
+
+int snac_gpu_batch_time_steps(snac_gpu_batch* b, int nsteps, int each, double* ms) {
+    if (!b || nsteps < 0 || !ms) return SNAC_GPU_EINVAL;
+    bool fused;
+    int rc = batch_prepare(b, &fused);  // tile lists and flushes outside the timed region
+    if (rc) return rc;
+    BCK(cudaEventRecord(b->ev[0], b->stream));
+    rc = each ? batch_run_each(b, nsteps) : batch_run(b, nsteps);
+    if (rc) return rc;
+    BCK(cudaEventRecord(b->ev[1], b->stream));
+    if ((rc = batch_status(b))) return rc;
+    float t = 0.0f;
+    BCK(cudaEventElapsedTime(&t, b->ev[0], b->ev[1]));
+    *ms = t;
+    return 0;
+}
+
+snac_gpu* snac_gpu_batch_model(snac_gpu_batch* b, int i) {
+    if (!b || i < 0 || i >= b->n) return nullptr;
+    return b->models[i];
+}
+
+int snac_gpu_batch_size(const snac_gpu_batch* b) { return b ? b->n : 0; }
+
+int snac_gpu_batch_get_tuning(const snac_gpu_batch* b, snac_batch_tuning* out) {
+    if (!b || !out) return SNAC_GPU_EINVAL;
+    *out = b->tune;
+    return 0;
+}
+
+int snac_gpu_batch_set_tuning(snac_gpu_batch* b, const snac_batch_tuning* t) {
+    if (!b || !t) return SNAC_GPU_EINVAL;
+    auto threads_ok = [](int x) { return x >= 32 && x <= 256 && x % 32 == 0; };
+    if (!threads_ok(t->node_threads) || !threads_ok(t->minls_threads) || t->elem_blocks_per_sm < 0 ||
+        t->elem_blocks_per_sm > 32 || t->node_blocks_per_sm < 0 || t->node_blocks_per_sm > 32 ||
+        t->steps_per_graph < 1 || t->steps_per_graph > 256 || (t->order != 0 && t->order != 1))
+        return bset_err(b, SNAC_GPU_EINVAL, -1, "launch shape out of range");
+    const snac_batch_tuning o = b->tune;
+    b->tune = *t;
+    if (o.node_threads != t->node_threads || o.minls_threads != t->minls_threads || o.order != t->order)
+        b->tiles_dirty = true;
+    else if (o.elem_blocks_per_sm != t->elem_blocks_per_sm || o.node_blocks_per_sm != t->node_blocks_per_sm ||
+             o.steps_per_graph != t->steps_per_graph)
+        drop_graphs(b);
+    return 0;
+}
+
+const char* snac_gpu_batch_last_error(const snac_gpu_batch* b) { return b ? b->err : "null batch"; }
+int snac_gpu_batch_error_model(const snac_gpu_batch* b) { return b ? b->err_model : -1; }
+long long snac_gpu_batch_launch_count(const snac_gpu_batch* b) { return b ? b->launches : 0; }
+void* snac_gpu_batch_stream(snac_gpu_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"

@@ -1,0 +1,139 @@
+// snac_batch.cuh — one launch per kernel type for a whole ensemble of models.
+//
+// Every model of a batch keeps its own device buffers (the same layout as a
+// single-model handle).  A batch adds a table of per-model descriptors
+// (mesh, field pointers, configuration) and, for each kind of launch, a list
+// of work tiles: (model, block index within that model).  A tile is exactly
+// the work one block of the single-model kernel does, so the per-model
+// results are the single-model results bit for bit; only the launch
+// geometry changes.  A block copies its tile's descriptor to shared memory
+// and calls the same kernel body as the single-model kernel.  With a grid
+// smaller than the tile list, blocks stride over the list (a persistent
+// grid whose size the autotuner chooses).
+#pragma once
+
+#include "snac_kernels.cuh"
+
+namespace snac {
+
+struct ModelDesc {
+    Mesh m;
+    Fields F;
+    Config cfg;
+    double wave_speed;
+};
+static_assert(sizeof(ModelDesc) % 8 == 0, "descriptor is copied as 64-bit words");
+
+// per-model status gathered after a batch of steps
+struct ModelStatus {
+    int status;
+    int pad;
+    long long err_index;
+    long long time_step;
+};
+
+enum { BOP_FUSED = 0, BOP_HEAT_FLUX = 1, BOP_STRESS = 2, BOP_LOOP_NODES = 3, BOP_HEAT_NODES = 4, BOP_MINLS = 5 };
+
+__device__ __forceinline__ void load_desc(ModelDesc& dst, const ModelDesc* __restrict__ src) {
+    constexpr int W = sizeof(ModelDesc) / 8;
+    const long long* s = reinterpret_cast<const long long*>(src);
+    long long* d = reinterpret_cast<long long*>(&dst);
+    for (int i = threadIdx.x; i < W; i += blockDim.x) d[i] = s[i];
+}
+
+// Element-tile kernels: the fused end-of-step/next-stress kernel (or its
+// heat variant for models with temperature), the heat flux, the stress update.
+template <int OP>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
+    kb_elements(const ModelDesc* __restrict__ D, const int2* __restrict__ tiles, int ntiles) {
+    __shared__ ModelDesc md;
+    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+        const int2 t = tiles[i];
+        __syncthreads();  // the previous tile is done with md
+        load_desc(md, D + t.x);
+        __syncthreads();
+        const int P = md.cfg.constitutive;
+        if (OP == BOP_FUSED) {
+            if (md.cfg.temperature) {
+                if (P == SNAC_RHEOLOGY_MAXWELL)
+                    k_fused_heat_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y);
+                else
+                    k_fused_heat_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y);
+            } else {
+                switch (P) {
+                    case SNAC_RHEOLOGY_ELASTIC: k_fused_step_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y); break;
+                    case SNAC_RHEOLOGY_PLASTIC: k_fused_step_body<SNAC_RHEOLOGY_PLASTIC>(md.m, md.F, md.cfg, t.y); break;
+                    case SNAC_RHEOLOGY_VISCOPLASTIC:
+                        k_fused_step_body<SNAC_RHEOLOGY_VISCOPLASTIC>(md.m, md.F, md.cfg, t.y);
+                        break;
+                    default: k_fused_step_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y); break;
+                }
+            }
+        } else if (OP == BOP_STRESS) {
+            switch (P) {
+                case SNAC_RHEOLOGY_ELASTIC: k_calc_stresses_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_RHEOLOGY_PLASTIC: k_calc_stresses_body<SNAC_RHEOLOGY_PLASTIC>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_RHEOLOGY_VISCOPLASTIC:
+                    k_calc_stresses_body<SNAC_RHEOLOGY_VISCOPLASTIC>(md.m, md.F, md.cfg, t.y);
+                    break;
+                default: k_calc_stresses_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y); break;
+            }
+        } else {
+            k_heat_flux_body(md.m, md.F, md.cfg, t.y);
+        }
+    }
+}
+
+// Node-tile kernels (one thread per node, or per element for the minimum
+// length scale); the block size is the tile size the tile list was built for.
+template <int OP>
+__global__ void __launch_bounds__(256) kb_nodes(const ModelDesc* __restrict__ D, const int2* __restrict__ tiles, int ntiles) {
+    __shared__ ModelDesc md;
+    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+        const int2 t = tiles[i];
+        __syncthreads();
+        load_desc(md, D + t.x);
+        __syncthreads();
+        if (OP == BOP_LOOP_NODES) {
+            switch (md.cfg.dt_type) {
+                case SNAC_DT_CONSTANT: k_loop_nodes_body<SNAC_DT_CONSTANT>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_DT_DYNAMIC: k_loop_nodes_body<SNAC_DT_DYNAMIC>(md.m, md.F, md.cfg, t.y); break;
+                default: k_loop_nodes_body<SNAC_DT_WAVE>(md.m, md.F, md.cfg, t.y); break;
+            }
+        } else if (OP == BOP_HEAT_NODES) {
+            k_heat_nodes_body(md.m, md.F, md.cfg, t.y);
+        } else {
+            k_min_length_scale_body(md.m, md.F, t.y);
+        }
+    }
+}
+
+// _Snac_Context_Sync of every model: one thread per model
+__global__ void kb_sync(const ModelDesc* __restrict__ D, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) sync_one(D[i].cfg, D[i].F.sc, D[i].wave_speed);
+}
+
+// _AbstractContext_Execute_Hook of every model (a step that does not start
+// with the fused kernel): timeStep++ and dt = dtFactor * dt
+__global__ void kb_begin_step(const ModelDesc* __restrict__ D, int n) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        DevScalars* sc = D[i].F.sc;
+        sc->time_step += 1;
+        sc->dt = 1.0 * sc->dt;
+    }
+}
+
+__global__ void kb_status(const ModelDesc* __restrict__ D, int n, ModelStatus* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const DevScalars* sc = D[i].F.sc;
+        out[i].status = sc->status;
+        out[i].pad = 0;
+        out[i].err_index = sc->err_index;
+        out[i].time_step = sc->time_step;
+    }
+}
+
+}  // namespace snac

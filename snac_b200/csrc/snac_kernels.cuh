@@ -893,6 +893,35 @@ __global__ void k_selftest_division(long long n, unsigned long long seed, unsign
     if (local) atomicAdd(bad, local);
 }
 
+// ---- host transfers: node fields between the packed double4 layout and
+// the reference's interleaved (x, y, z) / scalar arrays -------------------------------------
+// what: 0 = x, y, z of each double4 <-> 3 doubles per node; 1 = w <-> 1 double per node
+__global__ void k_pack_nodes(const double4* __restrict__ src, double* __restrict__ dst, long long nn, int what) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    double4 a = src[n];
+    if (what == 0) {
+        dst[n * 3 + 0] = a.x;
+        dst[n * 3 + 1] = a.y;
+        dst[n * 3 + 2] = a.z;
+    } else {
+        dst[n] = a.w;
+    }
+}
+
+__global__ void k_unpack_nodes(double4* __restrict__ dst, const double* __restrict__ src, long long nn, int what) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    double* d = reinterpret_cast<double*>(dst + n);
+    if (what == 0) {
+        d[0] = src[n * 3 + 0];
+        d[1] = src[n * 3 + 1];
+        d[2] = src[n * 3 + 2];
+    } else {
+        d[3] = src[n];
+    }
+}
+
 // _AbstractContext_Execute_Hook: timeStep++ and dt = dtFactor * dt (AbstractContext.c:874-890)
 __global__ void k_begin_step(DevScalars* sc) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {

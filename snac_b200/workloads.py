@@ -141,8 +141,8 @@ def c5_adjoint(nx=32, ny=16, nz=32, seed=5, dt=None) -> SnacConfig:
     return cfg
 
 
-def ensemble_member(rng: np.random.Generator, plastic: bool) -> SnacConfig:
-    nx, ny, nz = int(rng.integers(8, 49)), int(rng.integers(4, 25)), int(rng.integers(8, 49))
+def ensemble_member(rng: np.random.Generator, plastic: bool, xz=(8, 48), y=(4, 24)) -> SnacConfig:
+    nx, ny, nz = int(rng.integers(xz[0], xz[1] + 1)), int(rng.integers(y[0], y[1] + 1)), int(rng.integers(xz[0], xz[1] + 1))
     coh = math.exp(rng.uniform(math.log(10.0e6), math.log(60.0e6)))
     phi = float(rng.uniform(15.0, 35.0))
     refvisc = math.exp(rng.uniform(math.log(1.0e20), math.log(1.0e23)))
@@ -161,9 +161,11 @@ def ensemble_member(rng: np.random.Generator, plastic: bool) -> SnacConfig:
     return cfg
 
 
-def c4_ensemble(n_models=256, seed=4) -> List[SnacConfig]:
+def c4_ensemble(n_models=256, seed=4, xz=(8, 48), y=(4, 24)) -> List[SnacConfig]:
+    """Batched ensemble: half Mohr-Coulomb plastic, half visco-plastic with a
+    geotherm; hex counts drawn per model in [8..48] x [4..24](y) x [8..48]."""
     rng = np.random.default_rng(seed)
-    return [ensemble_member(rng, plastic=(i % 2 == 0)) for i in range(n_models)]
+    return [ensemble_member(rng, plastic=(i % 2 == 0), xz=xz, y=y) for i in range(n_models)]
 
 
 # ---- the reference's own test fixtures ------------------------------------------------------

@@ -14,7 +14,7 @@ HEADER = os.path.join(ROOT, "include", "snac_gpu.h")
 
 def declared():
     text = open(HEADER).read()
-    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*|long long|void\*)\s+\**(snac_gpu_\w+)\s*\(", text, re.M)))
+    return sorted(set(re.findall(r"^\s*(?:int|void|const char\*|long long|void\*|snac_gpu\*)\s+\**(snac_gpu_\w+)\s*\(", text, re.M)))
 
 
 @pytest.fixture(scope="module")

@@ -78,7 +78,7 @@ def test_device_transcendentals_within_tolerance(case, tol):
 
 
 def test_elastic_c1_full_1000_steps():
-    """configs[0] in full: 16 x 8 x 16 hex, 1000 elastic steps."""
+    """The plain elastic workload in full: 16 x 8 x 16 hex, 1000 elastic steps."""
     g, c = run_both(W.c1_elastic(), 1000)
     sg, sc = g.state(), c.state()
     assert relerr(sg.velocity, sc.velocity) <= 1e-9
@@ -213,13 +213,13 @@ def test_step_before_step_zero_is_refused():
 # ---- full-size configurations: bounded CPU comparisons and size-free properties ------------
 
 def test_c2_full_size_first_steps_bitwise():
-    """configs[1] at full size (64 x 32 x 64): three steps against the oracle."""
+    """The Mohr-Coulomb plastic workload at full size (64 x 32 x 64): three steps against the oracle."""
     g, c = run_both(W.c2_plastic(), 3)
     assert_bitwise(g, c)
 
 
 def test_c3_full_size_first_step_within_tolerance():
-    """configs[2] at full size (128 x 64 x 128, ~1M hex): one step against the oracle."""
+    """The Maxwell visco-plastic workload at full size (128 x 64 x 128, ~1M hex): one step against the oracle."""
     g, c = run_both(W.c3_viscoplastic(), 1)
     sg, sc = g.state(), c.state()
     for f in ("velocity", "stress", "viscosity", "temperature"):
@@ -227,7 +227,7 @@ def test_c3_full_size_first_step_within_tolerance():
 
 
 def test_full_size_c3_bit_reproducible_and_hooks_match():
-    """configs[2] at full size: two graph runs agree to the bit, and the
+    """The visco-plastic workload at full size: two graph runs agree to the bit, and the
     hook-by-hook path gives the same bits as the graph path"""
     cfg = W.c3_viscoplastic()
     runs = []
