@@ -220,6 +220,26 @@ typedef struct snac_kernel_time {
 } snac_kernel_time;
 int  snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max);
 
+/* Node fields (coord[nn*3], velocity[nn*3], temperature[nn]; any may be
+ * NULL) copied to host arrays like snac_gpu_download, but without allocating
+ * anything: no cudaMalloc/cudaFree, no library allocator.  For callers that
+ * must not allocate device memory during a run, e.g. a dump hook of a
+ * process whose device memory is fully committed to its models, where the
+ * lazily allocated staging buffer of snac_gpu_download could fail or evict.
+ * No counterpart in the reference (its node arrays are host memory).
+ *   - Staging is a static device array of 262,144 nodes x 3 doubles
+ *     (6 MiB); models with more nodes get SNAC_GPU_EINVAL and a message.
+ *   - Nothing in the staging has to start at zero: each call writes every
+ *     staged value before copying it out.
+ *   - The first call on each device looks up the staging address
+ *     (cudaGetSymbolAddress) with that device current; make that first call
+ *     before any stream capture begins.  The handle's device must be current.
+ *   - One staging array per device: overlapping calls would race on it, so
+ *     the call holds a process-wide lock until its copies have finished
+ *     (calls from several threads run one after another).
+ * Applies a pending element update first, as snac_gpu_download does. */
+int  snac_gpu_download_nodes_noalloc(snac_gpu* h, double* coord, double* velocity, double* temperature);
+
 /* ---- errors / introspection ------------------------------------------------ */
 const char* snac_gpu_last_error(const snac_gpu* h);
 long long   snac_gpu_error_index(const snac_gpu* h);   /* element/node id, -1 if none */

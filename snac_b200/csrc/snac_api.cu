@@ -12,6 +12,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -1267,3 +1268,63 @@ long long snac_gpu_batch_launch_count(const snac_gpu_batch* b) { return b ? b->l
 void* snac_gpu_batch_stream(snac_gpu_batch* b) { return b ? (void*)b->stream : nullptr; }
 
 }  // extern "C"
+
+// ======================================================================================
+// Node-field download without any allocation: the staging lives in a
+// file-scope device array instead of the handle's lazily allocated buffer.
+// ======================================================================================
+namespace {
+
+constexpr long long NOALLOC_MAX_NODES = 262144;  // 262,144 nodes x 3 doubles = 6 MiB
+
+// every element the call copies out was written by k_pack_nodes earlier in
+// the same call, so no part of it has to start at zero
+__device__ __align__(256) double g_noalloc_stage[NOALLOC_MAX_NODES * 3];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+void* g_noalloc_addr[NOALLOC_MAX_DEVICES] = {nullptr};
+std::mutex g_noalloc_lock;  // held for a whole call: one staging array per device
+
+int noalloc_node_out(snac_gpu* h, double* stage, const double4* src, double* dst, int what) {
+    const long long nn = h->mesh.nn;
+    k_pack_nodes<<<(unsigned)((nn + 255) / 256), 256, 0, h->stream>>>(src, stage, nn, what);
+    h->launches++;
+    int rc = launch_check_named(h, "k_pack_nodes");
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(dst, stage, nn * (what == 0 ? 3 : 1) * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    return 0;
+}
+
+}  // namespace
+
+extern "C" int snac_gpu_download_nodes_noalloc(snac_gpu* h, double* coord, double* velocity, double* temperature) {
+    if (!h) return SNAC_GPU_EINVAL;
+    if (h->mesh.nn > NOALLOC_MAX_NODES)
+        return set_err(h, SNAC_GPU_EINVAL, -1,
+                       "snac_gpu_download_nodes_noalloc: the model has %lld nodes, the static staging holds at most %lld",
+                       h->mesh.nn, NOALLOC_MAX_NODES);
+    int dev = -1;
+    CK(cudaGetDevice(&dev));
+    cudaPointerAttributes pa;
+    CK(cudaPointerGetAttributes(&pa, h->vel));
+    if (pa.device != dev)
+        return set_err(h, SNAC_GPU_EINVAL, -1,
+                       "snac_gpu_download_nodes_noalloc: the handle lives on device %d, device %d is current", pa.device, dev);
+    if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return set_err(h, SNAC_GPU_EINVAL, -1, "device index %d out of range", dev);
+    std::lock_guard<std::mutex> guard(g_noalloc_lock);
+    if (!g_noalloc_addr[dev]) {  // once per device, with that device current
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_stage);
+        if (e != cudaSuccess || !p)
+            return set_err(h, SNAC_GPU_ECUDA, -1, "cudaGetSymbolAddress(staging): %s", cudaGetErrorString(e));
+        g_noalloc_addr[dev] = p;
+    }
+    double* stage = static_cast<double*>(g_noalloc_addr[dev]);
+    int rc;
+    if ((rc = flush_pending(h))) return rc;
+    if (coord && (rc = noalloc_node_out(h, stage, h->pos[h->parity], coord, 0))) return rc;
+    if (velocity && (rc = noalloc_node_out(h, stage, h->vel, velocity, 0))) return rc;
+    if (temperature && (rc = noalloc_node_out(h, stage, h->pos[h->parity], temperature, 1))) return rc;
+    CK(cudaStreamSynchronize(h->stream));  // the staging is free again, and the host arrays are filled
+    return 0;
+}
