@@ -290,13 +290,21 @@ def run_ours(args, ws, rank, local):
             pinned[f] = t
             setattr(host, f, t.numpy())
         h2d = sum(pinned[f].numel() * 8 for f in fields)
+        out = State.empty(ctx.ne, ctx.nn)       # the step's result, into pinned host buffers
+        keep = []
+        for f, _ in out.view()._fields_:
+            a = getattr(out, f, None)
+            if a is not None:
+                t = torch.from_numpy(a).pin_memory()
+                keep.append(t)
+                setattr(out, f, t.numpy())
         ke = max(3, min(args.steps, 10))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(ke):
             ctx.set_state(host, fields)          # host -> device, the step's inputs
             ctx.step(1)
-            out = ctx.state()                    # device -> host, the step's result
+            ctx.state(out)                       # device -> host, the step's result
         torch.cuda.synchronize()
         te = (time.perf_counter() - t0) / ke
         d2h = sum(getattr(out, f).nbytes for f in ("coord", "velocity", "stress", "plastic_strain", "viscosity",
@@ -354,13 +362,131 @@ KERNEL_BYTES = {
 }
 
 
+# ---------------------------------------------------------------------------------------------
+def run_ensemble(args, ws, rank, local):
+    """--workload ensemble: 256 independent plastic / visco-plastic models of
+    uneven size advanced together (one launch per kernel type per step),
+    against the same models stepped one launch each (each model's own
+    step graph, back to back on the same stream)."""
+    import torch
+    from snac_b200 import workloads as W
+    from snac_b200.abi import State
+    from snac_b200.batch import SnacBatch, autotune
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    cfgs = W.c4_ensemble()
+    b = SnacBatch(cfgs)
+    ne = b.n_elements
+    b.time_step_zero()
+    tuning = autotune(b, steps=8)
+    b.step(max(3, args.warmup, tuning["steps_per_graph"]))  # warm-up; captures the graphs
+    torch.cuda.synchronize()
+
+    # state of all models: ~7 GB, far above the 126 MB L2, so no flush is needed
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    l0 = b.launches
+    barrier(ws)
+    torch.cuda.synchronize()
+    ms = b.time_steps(args.steps)
+    launches = b.launches - l0
+    b.time_steps(2, each=True)  # captures the per-model graphs
+    ms_each = b.time_steps(max(3, args.steps // 4), each=True) * args.steps / max(3, args.steps // 4)
+    barrier(ws)
+    clocks = sampler.stop() if sampler else None
+    t_max = allmax(ws, ms / 1e3)
+    value = ws * ne * args.steps / t_max
+    value_each = ws * ne * args.steps / allmax(ws, ms_each / 1e3)
+
+    peak, peak_kind = load_peaks()
+    alg_total = 0.0
+    for c in cfgs:
+        nph = c.n_nodes / c.n_elements
+        alg_total += c.n_elements * (960.0 + 96.0 * nph + 160.0 + 8.0 + (8.0 * nph if c.temperature else 0.0))
+    achieved = alg_total / (ms / 1e3 / args.steps) / 1e9
+
+    # end to end: every model's state up from pinned host memory, one batched
+    # step, every model's state down, per step
+    e2e = None
+    if not args.no_e2e:
+        fields = ["coord", "velocity", "stress", "plastic_strain", "viscosity", "temperature"]
+        hosts = []
+        for m in b.models:
+            st = m.state()
+            h = State.empty(m.ne, m.nn)
+            for f in fields:
+                setattr(h, f, torch.from_numpy(getattr(st, f)).pin_memory().numpy())
+            hosts.append(h)
+        h2d = sum(getattr(h, f).nbytes for h in hosts for f in fields)
+        ke = 2
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(ke):
+            for m, h in zip(b.models, hosts):
+                m.set_state(h, fields)
+            b.step(1)
+            outs = [m.state() for m in b.models]
+        torch.cuda.synchronize()
+        te = (time.perf_counter() - t0) / ke
+        d2h = sum(getattr(o, f).nbytes for o in outs for f in ("coord", "velocity", "stress", "plastic_strain",
+                                                               "viscosity", "temperature", "force", "inertial_mass"))
+        e2e = {"value": ws * ne / allmax(ws, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
+               "d2h_bytes_per_step": int(d2h),
+               "note": "per step: snac_gpu_upload of every model's state from pinned host buffers, "
+                       "snac_gpu_batch_step(1), snac_gpu_download of every model's state"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle.pyoracle import Checker, available
+        kind = "reference" if available("reference") else "port"
+        sample = cfgs[:8]
+        t = 0.0
+        hexsteps = 0
+        for c in sample:
+            ck = Checker(c, kind)
+            ck.time_step_zero()
+            t0 = time.perf_counter()
+            ck.step(2)
+            t += time.perf_counter() - t0
+            hexsteps += 2 * c.n_elements
+        cpu = {"value": hexsteps / t, "unit": UNIT, "cores": 1, "kind": kind,
+               "sample": f"2 SNAC steps of each of the first 8 ensemble models ({hexsteps // 2} hex) on one host core, "
+                         f"{t:.1f} s"}
+    b.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded, snac_b200/workloads.py)",
+            "config": {"workload": "batched ensemble: 256 models, hex per model drawn in [8..48] x [4..24](y) x "
+                                   "[8..48], half Mohr-Coulomb plastic, half visco-plastic with a geotherm",
+                       "hex": ne, "models": len(cfgs), "tuning": tuning,
+                       "l2": "inputs larger than L2 (~7 GB of model state)",
+                       "parallelism": "replicas" if ws > 1 else "single GPU, one launch per kernel type per step"},
+            "one_launch_each": {"value": value_each, "ms_per_step": ms_each / args.steps,
+                                "speedup_of_batched": value / value_each},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "kernel": "whole batched step",
+                         "algorithmic_bytes_per_step": alg_total, "peak_source": peak_kind},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "ensemble"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -375,7 +501,7 @@ def main():
         return
     ws, rank, local = dist_setup()
     try:
-        run_ours(args, ws, rank, local)
+        (run_ensemble if args.workload == "ensemble" else run_ours)(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

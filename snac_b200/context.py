@@ -202,8 +202,9 @@ class SnacContext:
         self.sync()
 
     # -- state --------------------------------------------------------------------------
-    def state(self) -> State:
-        s = State.empty(self.ne, self.nn)
+    def state(self, out: Optional[State] = None) -> State:
+        """The state at the end of the last step (into `out` if given, e.g. pinned buffers)."""
+        s = out if out is not None else State.empty(self.ne, self.nn)
         v = s.view()
         self._check(self.lib.snac_gpu_download(self.h, C.byref(v)))
         return s
