@@ -480,13 +480,105 @@ def run_ensemble(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------------------------------------
+def run_adjoint(args, ws, rank, local):
+    """--workload adjoint: the visco-plastic adjoint workload (32 x 16(y) x 32
+    hex, constant dt, fixed uniform temperature), loss = top-surface v_y and
+    topography misfit after `--adj-steps` steps against a run with smooth
+    +-10 % cohesion and viscosity perturbations; gradients with respect to
+    the per-element cohesion, friction and viscosity scales, checkpoint
+    every 45 steps.  Reports the adjoint's cost in forward runs and its
+    agreement with central finite differences of GPU forward runs."""
+    import numpy as np
+    import torch
+    from snac_b200 import workloads as W
+    from snac_b200.adjoint import adjoint, forward_loss, top_surface
+    from snac_b200.context import SnacContext
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    nx, ny, nz, N, K = 32, 16, 32, args.adj_steps, 45
+    ne = nx * ny * nz
+
+    def make(c, f, v):
+        cfg = W.c5_adjoint(nx, ny, nz, t_uniform=300.0)
+        cfg.element_cohesion_scale, cfg.element_friction_scale, cfg.element_visc_scale = c, f, v
+        return cfg
+
+    ones = np.ones(ne)
+    with SnacContext(make(1.0 + W.smooth_field(nx, ny, nz, 7), ones, 1.0 + W.smooth_field(nx, ny, nz, 8))) as t:
+        t.time_step_zero()
+        t.step(N)
+        tv, ty = top_surface(t.cfg, t.state())
+    wv, wh = 1.0 / max(1e-30, float(np.mean(tv ** 2))), 1.0 / (20.0e3 ** 2)
+    p = (ones.copy(), ones.copy(), ones.copy())
+
+    # forward alone: N steps from step zero, device time
+    with SnacContext(make(*p)) as ctx:
+        ctx.time_step_zero()
+        stream = torch.cuda.ExternalStream(ctx.stream, device=dev)
+        ctx.step(3)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            a.record(stream)
+        ctx.step(N)
+        with torch.cuda.stream(stream):
+            b.record(stream)
+        torch.cuda.synchronize()
+        ms_fwd = a.elapsed_time(b)
+    sampler = ClockSampler(local) if rank == 0 else None
+    if sampler:
+        sampler.start()
+        time.sleep(0.5)
+    with SnacContext(make(*p)) as ctx:
+        ctx.time_step_zero()
+        l0 = ctx.launches
+        t0 = time.perf_counter()
+        r = adjoint(ctx, N, tv, ty, wv, wh, checkpoint_every=K)
+        wall = time.perf_counter() - t0
+        launches = ctx.launches - l0
+    clocks = sampler.stop() if sampler else None
+    ms_adj = r.ms_forward + r.ms_reverse
+    g = [r.grad["cohesion"], r.grad["friction"], r.grad["viscosity"]]
+    rng = np.random.default_rng(11)
+    checks = []
+    for _ in range(args.adj_fd):
+        d = [rng.standard_normal(ne) for _ in range(3)]
+        h = 1.0e-6
+        lp = forward_loss(make, *[x + h * dx for x, dx in zip(p, d)], N, tv, ty, wv, wh)
+        lm = forward_loss(make, *[x - h * dx for x, dx in zip(p, d)], N, tv, ty, wv, wh)
+        fd = (lp - lm) / (2 * h)
+        ad = sum(float(np.dot(x, y)) for x, y in zip(g, d))
+        checks.append(abs(ad - fd) / max(abs(fd), 1e-300))
+    if rank == 0:
+        value = ne * N / (ms_adj / 1e3)
+        line = {
+            "metric": METRIC, "value": value, "unit": "element-steps/s (forward + adjoint)", "n_gpus": ws,
+            "steps": N, "warmup": 3, "ms_per_step": ms_adj / N, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, snac_b200/workloads.py)",
+            "config": {"workload": "adjoint: visco-plastic 32x16(y)x32 hex, constant dt, fixed uniform temperature, "
+                                   "top-surface v_y + topography misfit, gradients w.r.t. per-element cohesion, "
+                                   "friction, viscosity scales", "hex": ne, "checkpoint_every": r.checkpoint_every,
+                       "checkpoints": r.checkpoints},
+            "adjoint": {"loss": r.loss, "ms_forward_alone": ms_fwd, "ms_adjoint_call": ms_adj,
+                        "ms_adjoint_forward_sweep": r.ms_forward, "ms_adjoint_reverse": r.ms_reverse,
+                        "cost_in_forward_runs": ms_adj / ms_fwd, "fd_directions": len(checks),
+                        "fd_max_rel_err": max(checks) if checks else None,
+                        "fd_rel_errs": checks},
+            "gpu_launches": int(launches), "wall_s": wall, "clocks": clocks, "e2e": None, "cpu_baseline": None,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "ensemble"])
+    ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "ensemble", "adjoint"])
+    ap.add_argument("--adj-steps", type=int, default=2000)
+    ap.add_argument("--adj-fd", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--cpu-steps", type=int, default=10)
@@ -501,7 +593,7 @@ def main():
         return
     ws, rank, local = dist_setup()
     try:
-        (run_ensemble if args.workload == "ensemble" else run_ours)(args, ws, rank, local)
+        {"ensemble": run_ensemble, "adjoint": run_adjoint}.get(args.workload, run_ours)(args, ws, rank, local)
     finally:
         if ws > 1:
             import torch.distributed as dist

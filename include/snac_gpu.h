@@ -255,6 +255,42 @@ int  snac_gpu_device_count(void);
  * IEEE quotient of the GPU; *mismatches receives the count (expected 0). */
 int  snac_gpu_selftest_division(long long n, unsigned long long seed, long long* mismatches);
 
+/* ---- adjoint ------------------------------------------------------------------
+ * No counterpart in the reference.  Loss on the top surface (node plane
+ * j = ny, node order i + k*(nx+1)) after nsteps steps from the current state:
+ *   L = sum w_v (v_y - target_vy)^2 + w_h (y - target_y)^2
+ * snac_gpu_adjoint runs the nsteps forward (keeping every checkpoint_every-th
+ * state; 0 = ceil(sqrt(nsteps))), then the hand-written reverse sweep
+ * segment by segment (each segment recomputed from its checkpoint), and
+ * returns L and dL/d(scale) for the per-element cohesion, friction-angle
+ * and viscosity scales (element_cohesion_scale / element_friction_scale /
+ * element_visc_scale; an absent array is a scale of 1).  On return the model
+ * holds the forward's final state, as after snac_gpu_step(h, nsteps).
+ * Differentiated physics: SnacPlastic and SnacViscoPlastic (Mohr-Coulomb
+ * return map along the branch the forward took), dtType constant, no density
+ * coupling or thermal stress, temperature held fixed (thermal_conduct = 0);
+ * otherwise SNAC_GPU_ENOTSUP. */
+typedef struct snac_adjoint_desc {
+    int nsteps;
+    int checkpoint_every;
+    const double* target_vy;   /* [(nx+1)*(nz+1)] */
+    const double* target_y;    /* [(nx+1)*(nz+1)] */
+    double w_v, w_h;
+} snac_adjoint_desc;
+
+typedef struct snac_adjoint_stats {
+    double ms_forward;   /* the first forward sweep (device time)                   */
+    double ms_reverse;   /* segment recomputation + reverse sweep (device time)     */
+    int checkpoint_every;
+    int checkpoints;
+} snac_adjoint_stats;
+
+int  snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, double* grad_cohesion,
+                      double* grad_friction, double* grad_viscosity, snac_adjoint_stats* stats);
+/* L of the current state (no stepping): the forward half of the above, for
+ * finite-difference checks. */
+int  snac_gpu_misfit(snac_gpu* h, const snac_adjoint_desc* a, double* loss);
+
 /* ---- batched ensembles ------------------------------------------------------
  * No counterpart in the reference, which runs one model per process (one
  * Snac_Context per MPI job).  A batch holds n independent models, each built

@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "snac_gpu.h"
+#include "snac_adjoint.cuh"
 #include "snac_batch.cuh"
 #include "snac_kernels.cuh"
 
@@ -1328,3 +1329,294 @@ extern "C" int snac_gpu_download_nodes_noalloc(snac_gpu* h, double* coord, doubl
     CK(cudaStreamSynchronize(h->stream));  // the staging is free again, and the host arrays are filled
     return 0;
 }
+
+// ======================================================================================
+// Adjoint: gradients of a top-surface misfit with respect to the per-element
+// cohesion, friction and viscosity scales, with checkpointing every K steps
+// and recomputation of each segment before its reverse sweep.
+// ======================================================================================
+namespace {
+
+struct Snap {
+    double4* pos = nullptr;
+    double4* vel = nullptr;
+    double4* force = nullptr;
+    double* stress = nullptr;
+    double* eps_p = nullptr;
+    DevScalars* sc = nullptr;
+    bool pending = false;
+    long long time_step = 0;
+};
+
+int snap_alloc(snac_gpu* h, Snap& z) {
+    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
+    int rc;
+    if ((rc = dalloc(h, &z.pos, nn)) || (rc = dalloc(h, &z.vel, nn)) || (rc = dalloc(h, &z.force, nn)) ||
+        (rc = dalloc(h, &z.stress, nq * 6)) || (rc = dalloc(h, &z.eps_p, nq)) || (rc = dalloc(h, &z.sc, 1)))
+        return rc;
+    return 0;
+}
+
+void snap_free(Snap& z) {
+    void* b[] = {z.pos, z.vel, z.force, z.stress, z.eps_p, z.sc};
+    for (void* p : b)
+        if (p) cudaFree(p);
+    z = Snap();
+}
+
+int snap_save(snac_gpu* h, Snap& z) {
+    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
+    CK(cudaMemcpyAsync(z.pos, h->pos[h->parity], nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(z.vel, h->vel, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(z.force, h->force, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(z.stress, h->stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(z.eps_p, h->eps_p, nq * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(z.sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream));
+    z.pending = h->pending;
+    z.time_step = h->time_step;
+    return 0;
+}
+
+int snap_restore(snac_gpu* h, const Snap& z) {
+    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
+    CK(cudaMemcpyAsync(h->pos[h->parity], z.pos, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->vel, z.vel, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->force, z.force, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->stress, z.stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->eps_p, z.eps_p, nq * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(h->sc, z.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream));
+    h->pending = z.pending;
+    h->time_step = z.time_step;
+    return 0;
+}
+
+AdjState adj_state(const Snap& z) { return AdjState{z.pos, z.vel, z.force, z.stress, z.eps_p}; }
+
+int adjoint_supported(snac_gpu* h) {
+    if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "adjoint: time step zero must come first");
+    if (h->constitutive != SNAC_RHEOLOGY_PLASTIC && h->constitutive != SNAC_RHEOLOGY_VISCOPLASTIC)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and visco-plastic hooks are differentiated");
+    if (h->cfg.dt_type != SNAC_DT_CONSTANT)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: dtType must be constant (dt may not depend on the state)");
+    if (h->has_density || h->cfg.thermal_stress)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: density coupling and thermal stress are not differentiated");
+    if (h->temperature) {
+        std::vector<DevMaterial> dm(MAX_PHASES);
+        CK(cudaMemcpy(dm.data(), h->mats, MAX_PHASES * sizeof(DevMaterial), cudaMemcpyDeviceToHost));
+        for (int p = 0; p < h->n_phases; p++)
+            if (dm[p].thermal_conduct != 0.0)
+                return set_err(h, SNAC_GPU_ENOTSUP, -1,
+                               "adjoint: the temperature is held fixed; phase %d has thermal_conduct != 0", p);
+    }
+    return 0;
+}
+
+int adj_tet_launch(snac_gpu* h, const AdjState& S, const AdjBufs& B, int rotate, int first_rev, double dt) {
+    const unsigned nb = elem_blocks(h->mesh);
+    if (h->constitutive == SNAC_RHEOLOGY_PLASTIC)
+        k_adj_tet<SNAC_RHEOLOGY_PLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg, S, B, rotate,
+                                                                              first_rev, dt);
+    else
+        k_adj_tet<SNAC_RHEOLOGY_VISCOPLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg, S, B,
+                                                                                   rotate, first_rev, dt);
+    h->launches++;
+    return launch_check_named(h, "k_adj_tet");
+}
+
+int adj_nodes_launch(snac_gpu* h, const AdjState& cur, const AdjState& prev, const AdjBufs& B, int gather, int update,
+                     double dt) {
+    k_adj_nodes<<<(unsigned)((h->mesh.nn + 127) / 128), 128, 0, h->stream>>>(h->mesh, fields(h), cur, prev, B, gather,
+                                                                           update, dt, h->cfg.demf);
+    h->launches++;
+    return launch_check_named(h, "k_adj_nodes");
+}
+
+int misfit(snac_gpu* h, const snac_adjoint_desc* a, const AdjBufs& B, double* terms_dev, double* loss) {
+    const long long nt = (long long)h->mesh.nnx * h->mesh.nnz;
+    double *tv = nullptr, *ty = nullptr;
+    int rc;
+    if ((rc = dalloc(h, &tv, nt)) || (rc = dalloc(h, &ty, nt))) {
+        if (tv) cudaFree(tv);
+        return rc;
+    }
+    cudaMemcpyAsync(tv, a->target_vy, nt * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    cudaMemcpyAsync(ty, a->target_y, nt * sizeof(double), cudaMemcpyHostToDevice, h->stream);
+    k_adj_loss<<<(unsigned)((h->mesh.nn + 127) / 128), 128, 0, h->stream>>>(h->mesh, h->pos[h->parity], h->vel, tv, ty,
+                                                                          a->w_v, a->w_h, terms_dev, B);
+    h->launches++;
+    rc = launch_check_named(h, "k_adj_loss");
+    std::vector<double> t(nt);
+    cudaError_t e = cudaMemcpyAsync(t.data(), terms_dev, nt * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tv);
+    cudaFree(ty);
+    if (rc) return rc;
+    if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "misfit: %s", cudaGetErrorString(e));
+    double L = 0.0;
+    for (long long i = 0; i < nt; i++) L += t[i];
+    *loss = L;
+    return 0;
+}
+
+struct AdjWork {
+    AdjBufs B{};
+    double* terms = nullptr;
+    double* grads = nullptr;  // [3][ne]
+    void release() {
+        void* b[] = {B.xbar, B.vbar, B.fbar, B.cbuf, B.sbar, B.epbar, B.pbar, terms, grads};
+        for (void* p : b)
+            if (p) cudaFree(p);
+        *this = AdjWork();
+    }
+};
+
+int adj_work_alloc(snac_gpu* h, AdjWork& w) {
+    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT, nt = (long long)h->mesh.nnx * h->mesh.nnz;
+    int rc;
+    if ((rc = dalloc(h, &w.B.xbar, nn)) || (rc = dalloc(h, &w.B.vbar, nn)) || (rc = dalloc(h, &w.B.fbar, nn)) ||
+        (rc = dalloc(h, &w.B.cbuf, nq * 24)) || (rc = dalloc(h, &w.B.sbar, nq * 6)) || (rc = dalloc(h, &w.B.epbar, nq)) ||
+        (rc = dalloc(h, &w.B.pbar, nq * 3)) || (rc = dalloc(h, &w.terms, nt)) || (rc = dalloc(h, &w.grads, 3 * h->mesh.ne)))
+        return rc;
+    return 0;
+}
+
+int adj_status(snac_gpu* h) {
+    DevScalars sc;
+    CK(cudaMemcpyAsync(&sc, h->sc, sizeof sc, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (sc.status == SNAC_GPU_ENOTSUP)
+        return set_err(h, SNAC_GPU_ENOTSUP, sc.err_index,
+                       "adjoint: element %lld left the softening table or has a friction angle <= 0", sc.err_index);
+    return read_status(h);
+}
+
+}  // namespace
+
+extern "C" {
+
+int snac_gpu_misfit(snac_gpu* h, const snac_adjoint_desc* a, double* loss) {
+    if (!h || !a || !loss || !a->target_vy || !a->target_y) return SNAC_GPU_EINVAL;
+    AdjWork w;
+    int rc = 0;
+    const long long nn = h->mesh.nn, nt = (long long)h->mesh.nnx * h->mesh.nnz;
+    if ((rc = dalloc(h, &w.B.xbar, nn)) || (rc = dalloc(h, &w.B.vbar, nn)) || (rc = dalloc(h, &w.B.fbar, nn)) ||
+        (rc = dalloc(h, &w.terms, nt))) {
+        w.release();
+        return rc;
+    }
+    rc = misfit(h, a, w.B, w.terms, loss);
+    w.release();
+    return rc;
+}
+
+int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, double* grad_cohesion,
+                     double* grad_friction, double* grad_viscosity, snac_adjoint_stats* stats) {
+    if (!h || !a || !loss || !a->target_vy || !a->target_y || a->nsteps < 1) return SNAC_GPU_EINVAL;
+    int rc = adjoint_supported(h);
+    if (rc) return rc;
+    const int N = a->nsteps;
+    int K = a->checkpoint_every > 0 ? a->checkpoint_every : (int)std::ceil(std::sqrt((double)N));
+    if (K > N) K = N;
+    const int ncp = (N + K - 1) / K;  // checkpoints at steps 0, K, 2K, ...
+    const double dt = [&] {
+        DevScalars sc;
+        cudaMemcpy(&sc, h->sc, sizeof sc, cudaMemcpyDeviceToHost);
+        return sc.dt;
+    }();
+    if ((rc = flush_pending(h))) return rc;
+
+    std::vector<Snap> cp(ncp), seg(K + 1);
+    Snap fin;
+    AdjWork w;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    auto cleanup = [&]() {
+        cudaStreamSynchronize(h->stream);
+        for (auto& z : cp) snap_free(z);
+        for (auto& z : seg) snap_free(z);
+        snap_free(fin);
+        w.release();
+        for (auto& e : ev)
+            if (e) cudaEventDestroy(e);
+    };
+#define ACK(x)              \
+    do {                    \
+        int rc_ = (x);      \
+        if (rc_) {          \
+            cleanup();      \
+            return rc_;     \
+        }                   \
+    } while (0)
+    for (auto& z : cp) ACK(snap_alloc(h, z));
+    for (auto& z : seg) ACK(snap_alloc(h, z));
+    ACK(snap_alloc(h, fin));
+    ACK(adj_work_alloc(h, w));
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) ACK(set_err(h, SNAC_GPU_ECUDA, -1, "cudaEventCreate"));
+
+    // forward sweep, keeping every K-th state
+    cudaEventRecord(ev[0], h->stream);
+    ACK(snap_save(h, cp[0]));
+    for (int k = 1; k <= N; k++) {
+        ACK(launch_step(h));
+        if (k % K == 0 && k / K < ncp) ACK(snap_save(h, cp[k / K]));
+    }
+    ACK(snap_save(h, fin));
+    cudaEventRecord(ev[1], h->stream);
+    ACK(read_status(h));
+    ACK(misfit(h, a, w.B, w.terms, loss));  // also seeds the node adjoints
+
+    // reverse sweep, segment by segment from the last
+    const long long nq = h->mesh.ne * NT;
+    cudaMemsetAsync(w.B.sbar, 0, nq * 6 * sizeof(double), h->stream);
+    cudaMemsetAsync(w.B.epbar, 0, nq * sizeof(double), h->stream);
+    cudaMemsetAsync(w.B.pbar, 0, nq * 3 * sizeof(double), h->stream);
+    cudaEventRecord(ev[2], h->stream);
+    for (int j = ncp - 1; j >= 0; j--) {
+        const int a0 = j * K, b0 = std::min(a0 + K, N);
+        ACK(snap_restore(h, cp[j]));
+        ACK(snap_save(h, seg[0]));
+        for (int k = a0 + 1; k <= b0; k++) {
+            ACK(launch_step(h));
+            ACK(snap_save(h, seg[k - a0]));
+        }
+        // reverse of the node update of step b0-1
+        ACK(adj_nodes_launch(h, adj_state(seg[b0 - a0]), adj_state(seg[b0 - 1 - a0]), w.B, 0, 1, dt));
+        for (int n = b0 - 1; n >= a0; n--) {
+            ACK(adj_tet_launch(h, adj_state(seg[n - a0]), w.B, n >= 1, n == N - 1, dt));
+            if (n > a0)
+                ACK(adj_nodes_launch(h, adj_state(seg[n - a0]), adj_state(seg[n - 1 - a0]), w.B, 1, 1, dt));
+            else
+                ACK(adj_nodes_launch(h, adj_state(seg[0]), adj_state(seg[0]), w.B, 1, 0, dt));
+        }
+    }
+    const long long ne = h->mesh.ne;
+    k_adj_reduce<<<(unsigned)((ne + 127) / 128), 128, 0, h->stream>>>(ne, w.B.pbar, w.grads, w.grads + ne,
+                                                                    w.grads + 2 * ne);
+    h->launches++;
+    ACK(launch_check_named(h, "k_adj_reduce"));
+    cudaEventRecord(ev[3], h->stream);
+    ACK(adj_status(h));
+    if (grad_cohesion)
+        cudaMemcpyAsync(grad_cohesion, w.grads, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (grad_friction)
+        cudaMemcpyAsync(grad_friction, w.grads + ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (grad_viscosity)
+        cudaMemcpyAsync(grad_viscosity, w.grads + 2 * ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    // leave the model at the forward's final state
+    ACK(snap_restore(h, fin));
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess) ACK(set_err(h, SNAC_GPU_ECUDA, -1, "adjoint: sync"));
+    if (stats) {
+        float f = 0, r = 0;
+        cudaEventElapsedTime(&f, ev[0], ev[1]);
+        cudaEventElapsedTime(&r, ev[2], ev[3]);
+        stats->ms_forward = f;
+        stats->ms_reverse = r;
+        stats->checkpoint_every = K;
+        stats->checkpoints = ncp;
+    }
+    cleanup();
+#undef ACK
+    return 0;
+}
+
+}  // extern "C"

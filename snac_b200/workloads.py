@@ -130,15 +130,42 @@ def c3_viscoplastic(nx=128, ny=64, nz=128, seed=3, v=0.5 * CM_PER_YR,
     return cfg
 
 
-def c5_adjoint(nx=32, ny=16, nz=32, seed=5, dt=None) -> SnacConfig:
-    """C2 physics with viscosity (the visco-plastic hook), constant dt."""
-    cfg = c3_viscoplastic(nx, ny, nz, seed=seed, extent=(100.0e3, 20.0e3, 100.0e3), sigma=5.0e3)
-    rng = np.random.default_rng(seed)
+def c5_adjoint(nx=32, ny=16, nz=32, seed=5, dt=2.0e7, v=0.5 * CM_PER_YR, t_uniform=600.0,
+               extent=(100.0e3, 20.0e3, 100.0e3), cohesion=(44.0e6, 4.0e6)) -> SnacConfig:
+    """Adjoint workload: the plastic workload's physics (Mohr-Coulomb
+    strain softening, lithostatic IC, gravity, extension) through the
+    visco-plastic hook so that a viscosity field exists, with a constant dt
+    and a uniform, fixed temperature (zero conductivity).  Per-element
+    cohesion, friction and viscosity scales start at 1."""
+    cfg = c3_viscoplastic(nx, ny, nz, seed=seed, v=v, extent=extent)
+    m = vp_phase(thermal_conduct=0.0)
+    m.update(mc_phase(c0=cohesion[0], c1=cohesion[1], flat_tail=1.0e3))
+    m.update({k: val for k, val in vp_phase(thermal_conduct=0.0).items() if k not in m})
+    cfg.materials = [m]
+    cfg.temperatureBCs = [{"wall": "top", "T": t_uniform}, {"wall": "bottom", "T": t_uniform}]
+    cfg.init_temperature = np.full(cfg.n_nodes, t_uniform)
     ne = nx * ny * nz
-    cfg.element_cohesion_scale = 1.0 + rng.uniform(-0.05, 0.05, ne)
+    cfg.element_cohesion_scale = np.ones(ne)
+    cfg.element_friction_scale = np.ones(ne)
+    cfg.element_visc_scale = np.ones(ne)
     cfg.dtType = "constant"
-    cfg.timeStep = dt if dt is not None else 2.0e7
+    cfg.timeStep = dt
     return cfg
+
+
+def smooth_field(nx, ny, nz, seed, amplitude=0.1) -> np.ndarray:
+    """Seeded smooth perturbation in [-amplitude, amplitude] per element (a
+    few low-wavenumber sine modes), for targets of the adjoint workload."""
+    rng = np.random.default_rng(seed)
+    k, j, i = np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij")
+    f = np.zeros((nz, ny, nx))
+    for _ in range(4):
+        a, b, c = rng.integers(1, 3, 3)
+        ph = rng.uniform(0, 2 * math.pi, 3)
+        f += np.sin(math.pi * a * (i + 0.5) / nx + ph[0]) * np.sin(math.pi * b * (j + 0.5) / ny + ph[1]) * \
+            np.sin(math.pi * c * (k + 0.5) / nz + ph[2])
+    f /= max(1e-30, np.max(np.abs(f)))
+    return amplitude * f.reshape(-1)
 
 
 def ensemble_member(rng: np.random.Generator, plastic: bool, xz=(8, 48), y=(4, 24)) -> SnacConfig:
