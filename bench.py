@@ -120,7 +120,9 @@ class ClockSampler:
         return out
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun env).  The CPU tests run the same
+    replica logic with backend="gloo"."""
     import torch
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -128,8 +130,9 @@ def dist_setup():
     if ws > 1:
         import datetime
         import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return ws, rank, local
 
 
@@ -140,13 +143,21 @@ def barrier(ws):
 
 
 def allmax(ws, x: float) -> float:
+    """Max over ranks (every timing is the slowest rank's)."""
     if ws == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_throughput(ws: int, units_per_rank: float, seconds_this_rank: float) -> float:
+    """Whole-job throughput of ws independent replicas (weak scaling): all
+    ranks' units over the slowest rank's time."""
+    return ws * units_per_rank / allmax(ws, seconds_this_rank)
 
 
 # ---------------------------------------------------------------------------------------------
@@ -257,8 +268,7 @@ def run_ours(args, ws, rank, local):
     clocks = sampler.stop() if sampler else None
     step_ms = [a.elapsed_time(b) for a, b in ev]
     t_dev = sum(step_ms) / 1e3
-    t_max = allmax(ws, t_dev)
-    value = ws * ne * args.steps / t_max
+    value = replica_throughput(ws, ne * args.steps, t_dev)
 
     # ---- per-kernel breakdown: one step kernel by kernel, events on the library stream -----
     kern = {}
@@ -397,8 +407,7 @@ def run_ensemble(args, ws, rank, local):
     ms_each = b.time_steps(max(3, args.steps // 4), each=True) * args.steps / max(3, args.steps // 4)
     barrier(ws)
     clocks = sampler.stop() if sampler else None
-    t_max = allmax(ws, ms / 1e3)
-    value = ws * ne * args.steps / t_max
+    value = replica_throughput(ws, ne * args.steps, ms / 1e3)
     value_each = ws * ne * args.steps / allmax(ws, ms_each / 1e3)
 
     peak, peak_kind = load_peaks()
