@@ -287,11 +287,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         double avgTemp = 0.0;
         for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
         const double refvisc = M.refvisc * vsc;
-        const double Rg = 8.31448;
-        R.eta_base = M.refvisc * pow((dv(J, M.refsrate)), (dv(1., M.srexponent) - 1.)) *
-                     exp(dv(M.H, Rg) * (dv(1., avgTemp + 273.15) - dv(1., M.reftemp + 273.15)));
-        double eta = arrhenius_viscosity(refvisc, J, M.refsrate, M.srexponent, M.H, avgTemp, M.reftemp, M.vis_min,
-                                         M.vis_max);
+        // unclipped viscosity without the element's scale: d eta / d scale
+        R.eta_base = M.refvisc * pow(dvz(J, M.refsrate, M.vp_zrs), M.vp_expo) *
+                     exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+        double eta = arrhenius_viscosity(M, refvisc, J, avgTemp);
         R.eta_free = (eta > M.vis_min && eta < M.vis_max);
         R.eta = eta;
         R.tmp = dv(M.mu, 2.0f * (eta)) * dt;

@@ -142,6 +142,10 @@ DevMaterial to_dev(const snac_material& s, bool fric_scaled) {
     d.srexponent = s.srexponent;
     d.thermal_conduct = s.thermal_conduct;
     d.heat_capacity = s.heat_capacity;
+    d.vp_expo = (1. / s.srexponent) - 1.;
+    d.vp_hr = s.activation_e / 8.31448;
+    d.vp_irt = 1. / (s.reftemp + 273.15);
+    d.vp_zrs = 1. / s.refsrate;
     const double degrad = 3.14159265358979323846 / 180.0f;
     bool fc = !fric_scaled, dc = true;
     for (int i = 1; i <= s.nsegments; i++) {

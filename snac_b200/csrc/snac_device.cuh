@@ -76,6 +76,9 @@ struct DevMaterial {
     double ten_off;
     double vis_min, vis_max, refvisc, refsrate, reftemp, H, srexponent;
     double thermal_conduct, heat_capacity;
+    // constant factors of the Arrhenius viscosity, evaluated on the host with
+    // the same IEEE operations: 1/srexponent - 1, H/R, 1/(reftemp + 273.15), RN(1/refsrate)
+    double vp_expo, vp_hr, vp_irt, vp_zrs;
     // host-evaluated transcendentals (valid when the *_const flag is set)
     int fric_const, dil_const;
     double fric0, sin_fric0, tan_fric0;
@@ -103,94 +106,87 @@ __device__ __forceinline__ void report(DevScalars* sc, int code, long long index
     if (atomicCAS(&sc->status, 0, code) == 0) sc->err_index = index;
 }
 
-#ifndef SNAC_FAST_DIV
-#define SNAC_FAST_DIV 0  // measured slower than the hardware IEEE division on B200; kept switchable
+#ifndef SNAC_MARKSTEIN_DIV
+#define SNAC_MARKSTEIN_DIV 2
 #endif
 
-// ---- correctly rounded division without the slow-path branch -----------------
-// dv(x, y) returns the same bits as the IEEE quotient x / y (round to
-// nearest even) for operands in the normal range, as a straight-line
-// sequence the compiler can interleave with other work:
-//   1. a reciprocal seed z0 ~ 1/y from the single-precision approximate
-//      reciprocal (relative error < 2^-22 after the conversions),
-//   2. two Newton-Raphson steps z <- z + z (1 - y z), each fused, which leave
-//      |1 - y z| ~ 2^-52,
-//   3. q = x z corrected once with the exact remainder, q <- q + (x - q y) z;
-//      q is then within one ulp of x / y (faithful),
-//   4. the rounding decision from the exact remainder r = x - q y (one FMA,
-//      exact because q is faithful): the correctly rounded quotient is q or
-//      its neighbour qn towards x / y, whichever is nearer; nearer is decided
-//      by comparing 2|r| with |qn - q| |y| (both exact: |qn - q| is a power of
-//      two), ties to the even significand.
-// This is the Newton-Raphson division with Markstein's remainder-based
-// correction: P. Markstein, "Computation of elementary functions on the IBM
-// RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; J.-M. Muller
-// et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018, ch. 4.
-// Divisors outside [2^-120, 2^120], non-finite operands and quotients
-// outside [2^-800, 2^800] (other than zero) take the IEEE division instead.
-// The device self-test (snac_gpu_selftest_division) compares it with the
-// hardware-rounded '/' on random operands.
-__host__ __device__ __forceinline__ double approx_recip(double y) {
-#ifdef __CUDA_ARCH__
-    float r, yf = (float)y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(yf));
-    return (double)r;
-#else
-    return (double)(1.0f / (float)y);
-#endif
-}
+// ---- correctly rounded division by a known reciprocal --------------------------------
+// With z = RN(1/y) (the correctly rounded reciprocal) and q0 = RN(x z),
+// which is within one ulp of x / y, the remainder r = x - q0 y is exact in
+// one FMA and RN(q0 + r z) is the correctly rounded quotient RN(x / y):
+// Markstein's theorem (P. Markstein, "Computation of elementary functions on
+// the IBM RISC System/6000 processor", IBM J. Res. Dev. 34(1), 1990; J.-M.
+// Muller et al., Handbook of Floating-Point Arithmetic, 2nd ed., 2018,
+// ch. 4).  So a division by a constant (z a literal) or several divisions by
+// one divisor (z computed once) cost a multiply and two FMAs each instead of
+// a full division.  The theorem needs the quotient and divisor in the normal
+// range without overflow or underflow: zeros keep the sign of x z, and
+// operands outside a safe exponent window (checked with integer operations
+// on the exponent field) take the IEEE division.  SNAC_MARKSTEIN_DIV = 1
+// uses it for the constant divisors only, 2 also for shared divisors.  The device self-test
+// (snac_gpu_selftest_division) compares every helper with the hardware '/'
+// on random operands, near-ties included.
 
-// ~1/y, |1 - y z| ~ 2^-52 (only meaningful when 2^-120 <= |y| <= 2^120)
+// RN(1/y)
 __host__ __device__ __forceinline__ double recip(double y) {
-    double z = approx_recip(y);
-    double e = fma(-y, z, 1.0);
-    z = fma(z, e, z);
-    e = fma(-y, z, 1.0);
-    return fma(z, e, z);
+#ifdef __CUDA_ARCH__
+    return __drcp_rn(y);
+#else
+    return 1.0 / y;
+#endif
 }
 
-__host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
-#if SNAC_FAST_DIV
-    const double q0 = x * z;  // for x = +-0 this is already the IEEE zero with the right sign
-    double r = fma(-q0, y, x);
-    double q = fma(r, z, q0);
-    r = fma(-q, y, x);
-    const bool up = (r > 0.0) == (y > 0.0);  // x / y lies above q
-#ifdef __CUDA_ARCH__
-    long long b = __double_as_longlong(q);
-    double qn = __longlong_as_double(b + (((q > 0.0) == up) ? 1 : -1));
+// biased exponent of x (0 for zeros and subnormals, 2047 for Inf/NaN)
+__host__ __device__ __forceinline__ unsigned biased_exp(double x) {
+    unsigned long long b;
+    memcpy(&b, &x, 8);
+    return (unsigned)(b >> 52) & 0x7ffu;
+}
+__host__ __device__ __forceinline__ bool is_zero(double x) {
+    unsigned long long b;
+    memcpy(&b, &x, 8);
+    return (b << 1) == 0ull;
+}
+// |x| in [2^lo, 2^(hi+1)) by integer tests (keeps the checks off the FP64 pipe)
+template <int LO, int HI>
+__host__ __device__ __forceinline__ bool exp_within(double x) {
+    return biased_exp(x) - (unsigned)(1023 + LO) <= (unsigned)(HI - LO);
+}
+
+// RN(x / c) for a constant c with z = RN(1/c) and 1 <= c <= 16
+__host__ __device__ __forceinline__ double dvk(double x, double c, double z) {
+#if SNAC_MARKSTEIN_DIV >= 1
+    const double q0 = x * z;
+    const double q = fma(fma(-q0, c, x), z, q0);
+    if (is_zero(x)) return q0;
+    if (!exp_within<-900, 900>(x)) return x / c;
+    return q;
 #else
-    long long b;
-    memcpy(&b, &q, 8);
-    long long bn = b + (((q > 0.0) == up) ? 1 : -1);
-    double qn;
-    memcpy(&qn, &bn, 8);
+    (void)z;
+    return x / c;
 #endif
-    const double tr = 2.0 * fabs(r);
-    const double h = fabs(qn - q) * fabs(y);
-    double res = (tr < h) ? q : (tr > h ? qn : ((b & 1) ? qn : q));
-    if (r == 0.0) res = q;
-    if (x == 0.0) res = q0;
-    const double ay = fabs(y), aq = fabs(q);
-    const bool ok = ay >= 0x1p-120 && ay <= 0x1p120 && (x == 0.0 || (aq >= 0x1p-800 && aq <= 0x1p800));
-    return ok ? res : x / y;
+}
+
+// RN(x / y) given z = RN(1/y)
+__host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
+#if SNAC_MARKSTEIN_DIV >= 2
+    const double q0 = x * z;
+    const double q = fma(fma(-q0, y, x), z, q0);
+    if (is_zero(x)) return q0;
+    if (!(exp_within<-450, 450>(x) && exp_within<-450, 450>(y))) return x / y;
+    return q;
 #else
     (void)z;
     return x / y;
 #endif
 }
-__host__ __device__ __forceinline__ double dv(double x, double y) {
-#if SNAC_FAST_DIV
-    return dvz(x, y, recip(y));
-#else
-    return x / y;
-#endif
-}
+
+__host__ __device__ __forceinline__ double dv(double x, double y) { return x / y; }
 // division by the constants the reference uses; the reciprocal is RN(1/c)
-__host__ __device__ __forceinline__ double dv3(double x) { return dvz(x, 3.0, 0x1.5555555555555p-2); }
-__host__ __device__ __forceinline__ double dv6(double x) { return dvz(x, 6.0, 0x1.5555555555555p-3); }
-__host__ __device__ __forceinline__ double dv9(double x) { return dvz(x, 9.0, 0x1.c71c71c71c71cp-4); }
-__host__ __device__ __forceinline__ double dv10(double x) { return dvz(x, 10.0, 0x1.999999999999ap-4); }
+__host__ __device__ __forceinline__ double dv3(double x) { return dvk(x, 3.0, 0x1.5555555555555p-2); }
+__host__ __device__ __forceinline__ double dv6(double x) { return dvk(x, 6.0, 0x1.5555555555555p-3); }
+__host__ __device__ __forceinline__ double dv9(double x) { return dvk(x, 9.0, 0x1.c71c71c71c71cp-4); }
+__host__ __device__ __forceinline__ double dv10(double x) { return dvk(x, 10.0, 0x1.999999999999ap-4); }
 
 struct V3 {
     double x, y, z;
@@ -223,12 +219,14 @@ __device__ __forceinline__ void tet_face(const V3& c1, const V3& c2, const V3& c
 
 struct TetGeom {
     double V;
+    double zV;  // RN(1/V), shared by every division by V
     double A[4];
     V3 n[4];
 };
 
 __device__ __forceinline__ void tet_geometry(const V3 c[4], TetGeom& g) {
     g.V = tet_volume(c[0], c[1], c[2], c[3]);
+    g.zV = recip(g.V);
 #pragma unroll
     for (int f = 0; f < 4; f++)
         tet_face(c[face_node(f, 0)], c[face_node(f, 1)], c[face_node(f, 2)], g.A[f], g.n[f]);
@@ -262,7 +260,7 @@ __device__ __forceinline__ double shear_sum(const V3 v[4], const TetGeom& g, int
 // StrainRate.c:65-184, before the mixed-discretisation correction;
 // sr = (xx, yy, zz, xy, xz, yz)
 __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g, double sr[6]) {
-    const double zV = recip(g.V);
+    const double zV = g.zV;
     sr[0] = dvz(dv3(-1.0f * (face_sum(v, 0, g, 0))), g.V, zV);
     sr[1] = dvz(dv3(-1.0f * (face_sum(v, 1, g, 1))), g.V, zV);
     sr[2] = dvz(dv3(-1.0f * (face_sum(v, 2, g, 2))), g.V, zV);
@@ -274,7 +272,8 @@ __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g,
 // Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
 // zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
-    const double hV = dv(0.5, g.V);
+    // RN(0.5 / V) = 0.5 RN(1 / V) exactly while 1 / V is a normal number
+    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : dv(0.5, g.V);
     double r01 = dv3(-(hV) * (spin_sum(v, g, 0, 1)));
     double r02 = dv3(-(hV) * (spin_sum(v, g, 0, 2)));
     double r12 = dv3(-(hV) * (spin_sum(v, g, 1, 2)));
@@ -487,14 +486,12 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
 
 // Power-law / Arrhenius viscosity, viscoplastic/Constitutive.c:186-210 and
 // maxwell/Constitutive.c:122-142, clipped to [vis_min, vis_max].
-__device__ __forceinline__ double arrhenius_viscosity(double refvisc, double srJ2, double rstrainrate,
-                                                      double srexponent, double H, double avgTemp, double rTemp,
-                                                      double vis_min, double vis_max) {
-    const double R = 8.31448;
-    double eta = refvisc * pow((dv(srJ2, rstrainrate)), (dv(1., srexponent) - 1.)) *
-                 exp(dv(H, R) * (dv(1., avgTemp + 273.15) - dv(1., rTemp + 273.15)));
-    if (eta < vis_min) eta = vis_min;
-    if (eta > vis_max) eta = vis_max;
+__device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, double refvisc, double srJ2,
+                                                      double avgTemp) {
+    double eta = refvisc * pow(dvz(srJ2, M.refsrate, M.vp_zrs), M.vp_expo) *
+                 exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+    if (eta < M.vis_min) eta = M.vis_min;
+    if (eta > M.vis_max) eta = M.vis_max;
     return eta;
 }
 

@@ -169,7 +169,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     double partial = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) partial += grp(trace, s.base, u) * grp(g.V, s.base, u);
-    double corr = -1.0f * trace + dv(partial, elemVolume);
+    const double zE = recip(elemVolume);
+    double corr = -1.0f * trace + dvz(partial, elemVolume, zE);
     sr[0] += corr;
     sr[1] += corr;
     sr[2] += corr;
@@ -217,13 +218,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         if (srJ2 == 0.0f) srJ2 = M.refsrate;
         double avgTemp = 0.0;
         for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
-        eta = arrhenius_viscosity(M.refvisc, srJ2, M.refsrate, M.srexponent, M.H, avgTemp, M.reftemp, M.vis_min,
-                                  M.vis_max);
+        eta = arrhenius_viscosity(M, M.refvisc, srJ2, avgTemp);
         if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
         if (ph == 0) maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
     } else {
-        const double a1 = M.lambda + 2.0f * M.mu;
-        const double a2 = M.lambda;
         if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) {
             // elastic trial, plastic/Constitutive.c:114-121
             double tr = e[0] + e[1] + e[2];
@@ -259,8 +257,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
             double refvisc = M.refvisc;
             if (F.visc_scale && s.active) refvisc = M.refvisc * F.visc_scale[s.e];
-            eta = arrhenius_viscosity(refvisc, srJ2, M.refsrate, M.srexponent, M.H, avgTemp, M.reftemp, M.vis_min,
-                                      M.vis_max);
+            eta = arrhenius_viscosity(M, refvisc, srJ2, avgTemp);
             if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
             maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
         }
@@ -350,7 +347,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     double partialS = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) partialS += grp(traceS, s.base, u) * grp(g.V, s.base, u);
-    const double avgTrace = dv(partialS, elemVolume);
+    const double avgTrace = dvz(partialS, elemVolume, zE);
     double cs2 = -1.0f * traceS + avgTrace;
     st[0] += cs2;
     st[1] += cs2;
@@ -398,6 +395,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             F.fmass[s.q] = factor4 * inertialDensity * g.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
+            const double nineV = 9.0f * g.V, z9V = recip(nineV);
 #pragma unroll
             for (int f = 0; f < 4; f++) {
                 const V3& nr = g.n[f];
@@ -409,7 +407,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
                 if (temp > area_sum) area_sum = temp;
                 temp = (nr.z * A) * (nr.z * A);
                 if (temp > area_sum) area_sum = temp;
-                F.fmass[s.q * 4 + f] = dv(alpha1 * area_sum, 9.0f * g.V) * (dt * dt);
+                F.fmass[s.q * 4 + f] = dvz(alpha1 * area_sum, nineV, z9V) * (dt * dt);
             }
         } else {
             F.fmass[s.q] = factor4 * rho * g.V;
@@ -663,7 +661,7 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
                                               const double T[4], const double T0[4], const TetGeom& g) {
     const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
     double q[3], tsr = 0.0;
-    const double zV = recip(g.V);
+    const double zV = g.zV;
     for (int d = 0; d < 3; d++)
         q[d] = dvz(dv3(1.0f * M.thermal_conduct *
                        (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
@@ -887,6 +885,7 @@ __global__ void k_selftest_division(long long n, unsigned long long seed, unsign
         if ((c >> 40) % 5 == 0) x = rint(x * 1e-3) * y;         // quotients that are exact or near ties
         if ((c >> 44) % 97 == 0) x = ((c >> 50) & 1) ? 0.0 : -0.0;
         local += !same_bits(dv(x, y), x / y);
+        local += !same_bits(dvz(x, y, recip(y)), x / y);
         local += !same_bits(dv3(x), x / 3.0) + !same_bits(dv6(x), x / 6.0);
         local += !same_bits(dv9(x), x / 9.0) + !same_bits(dv10(x), x / 10.0);
     }
