@@ -385,7 +385,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     R.tension = false;
     R.alam = 0.0;
     R.inc = 0.0;
-    if (!surely_elastic(st, R.co, R.anphi, R.stc)) {
+    if (!surely_elastic(st, R.co, R.anphi, sqrt(R.anphi), R.stc)) {
         principal_stresses(st, R.sp, R.cn);
         double sp[3] = {R.sp[0], R.sp[1], R.sp[2]};
         double fs = sp[0] - sp[2] * R.anphi + 2 * R.co * sqrt(R.anphi);

@@ -159,6 +159,12 @@ DevMaterial to_dev(const snac_material& s, bool fric_scaled) {
     d.tan_fric0 = tan(d.fric0 * degrad);
     d.dil0 = s.dilation_angle[0];
     d.sin_dil0 = sin(d.dil0 * degrad);
+    d.anphi0 = (1.0f + d.sin_fric0) / (1.0f - d.sin_fric0);
+    d.anpsi0 = (1.0f + d.sin_dil0) / (1.0f - d.sin_dil0);
+    d.sq_anphi0 = sqrt(d.anphi0);
+    d.ztan_fric0 = 1.0 / d.tan_fric0;
+    for (int i = 0; i < SNAC_MAX_SEGMENTS; i++)
+        d.zpl[i] = i < s.nsegments ? 1.0 / (s.plstrain[i + 1] - s.plstrain[i]) : 0.0;
     return d;
 }
 

@@ -79,6 +79,11 @@ struct DevMaterial {
     // constant factors of the Arrhenius viscosity, evaluated on the host with
     // the same IEEE operations: 1/srexponent - 1, H/R, 1/(reftemp + 273.15), RN(1/refsrate)
     double vp_expo, vp_hr, vp_irt, vp_zrs;
+    // host-evaluated per-segment 1/(plstrain[i+1] - plstrain[i]) and, for a
+    // constant angle, (1 + sin)/(1 - sin) of friction and dilation,
+    // sqrt of the former and RN(1 / tan(friction))
+    double zpl[SNAC_MAX_SEGMENTS];
+    double anphi0, anpsi0, sq_anphi0, ztan_fric0;
     // host-evaluated transcendentals (valid when the *_const flag is set)
     int fric_const, dil_const;
     double fric0, sin_fric0, tan_fric0;
@@ -410,14 +415,15 @@ __host__ __device__ void principal_stresses(const double st[6], double sp[3], do
 // exact eigenvalues lie in the Gershgorin interval [lo, hi], the Jacobi
 // values are within ~1e-15 of the stress scale of them, and the margin asked
 // for is 1e-9 of that scale.  Skipping the eigen-solve then changes no bit.
-__host__ __device__ __forceinline__ bool surely_elastic(const double st[6], double cohesion, double anphi, double stc) {
+__host__ __device__ __forceinline__ bool surely_elastic(const double st[6], double cohesion, double anphi,
+                                                       double sqrt_anphi, double stc) {
     double r0 = fabs(st[3]) + fabs(st[4]);
     double r1 = fabs(st[3]) + fabs(st[5]);
     double r2 = fabs(st[4]) + fabs(st[5]);
     double hi = fmax(st[0] + r0, fmax(st[1] + r1, st[2] + r2));
     double lo = fmin(st[0] - r0, fmin(st[1] - r1, st[2] - r2));
     double scale = fabs(st[0]) + fabs(st[1]) + fabs(st[2]) + 2.0 * (r0 + r1 + r2);
-    double cterm = 2.0 * cohesion * sqrt(anphi);
+    double cterm = 2.0 * cohesion * sqrt_anphi;
     double tol_t = 1e-9 * (scale + fabs(stc)) + 1e-300;
     double tol_s = 1e-9 * (scale * (1.0 + anphi) + fabs(cterm)) + 1e-300;
     bool no_tension = hi - stc < -tol_t;

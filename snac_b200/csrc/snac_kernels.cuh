@@ -274,7 +274,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
             double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
             if (eps_p >= pl1 && eps_p <= pl2) {
-                const double dpl = pl2 - pl1, zpl = recip(dpl);
+                const double dpl = pl2 - pl1, zpl = M.zpl[i];  // = RN(1 / dpl)
                 const double tgf = dvz(f1 - f0, dpl, zpl);
                 const double tgd = dvz(M.dil[i + 1] - M.dil[i], dpl, zpl);
                 const double tgc = dvz(c1 - c0, dpl, zpl);
@@ -299,44 +299,52 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         // The reference keeps the table values (and the tension cutoff) in
         // variables that outlive the tet loop: a tet whose lookup matched no
         // segment reuses the previous tet's values, 0 before the first match.
-        unsigned mb = __ballot_sync(FULL, matched && s.active);
-        unsigned mine = (mb >> s.base) & ((1u << (s.t + 1)) - 1u);
-        int src = mine ? (31 - __clz(mine)) : -1;
-        double src_fa = __shfl_sync(FULL, fa, s.base + (src < 0 ? 0 : src));
-        double src_da = __shfl_sync(FULL, da, s.base + (src < 0 ? 0 : src));
-        double src_co = __shfl_sync(FULL, co, s.base + (src < 0 ? 0 : src));
-        double src_hd = __shfl_sync(FULL, hd, s.base + (src < 0 ? 0 : src));
-        double frictionAngle = src < 0 ? 0.0f : src_fa;
-        double dilationAngle = src < 0 ? 0.0f : src_da;
-        double cohesion = src < 0 ? 0.0f : src_co;
-        double hardening = src < 0 ? 0.0f : src_hd;
+        double frictionAngle = fa, dilationAngle = da, cohesion = co, hardening = hd;
+        // warp-uniform test: when every tet of the warp matched, each uses its own values
+        if (__ballot_sync(FULL, s.active && !matched) != 0u) {
+            unsigned mb = __ballot_sync(FULL, matched && s.active);
+            unsigned mine = (mb >> s.base) & ((1u << (s.t + 1)) - 1u);
+            int src = mine ? (31 - __clz(mine)) : -1;
+            double src_fa = __shfl_sync(FULL, fa, s.base + (src < 0 ? 0 : src));
+            double src_da = __shfl_sync(FULL, da, s.base + (src < 0 ? 0 : src));
+            double src_co = __shfl_sync(FULL, co, s.base + (src < 0 ? 0 : src));
+            double src_hd = __shfl_sync(FULL, hd, s.base + (src < 0 ? 0 : src));
+            frictionAngle = src < 0 ? 0.0f : src_fa;
+            dilationAngle = src < 0 ? 0.0f : src_da;
+            cohesion = src < 0 ? 0.0f : src_co;
+            hardening = src < 0 ? 0.0f : src_hd;
+        }
         // tension cutoff st = min(ten_off, c / tan(phi)) when phi > 0, else carried over
+        const bool fconst = M.fric_const && frictionAngle == M.fric0;
         bool phi_ok = (PLUGIN == SNAC_RHEOLOGY_PLASTIC) ? (frictionAngle >= 0.0f) : (frictionAngle > 0.0f);
         double st_own = 0.0;
         if (phi_ok) {
             st_own = M.ten_off;
             if (frictionAngle > 0.0) {
-                double tmp = dv(cohesion, tan_fric(M, frictionAngle));
+                double tmp = fconst ? dvz(cohesion, M.tan_fric0, M.ztan_fric0) : dv(cohesion, tan_fric(M, frictionAngle));
                 if (tmp < st_own) st_own = tmp;
             }
         }
-        unsigned pb = __ballot_sync(FULL, phi_ok && s.active);
-        unsigned pm = (pb >> s.base) & ((1u << (s.t + 1)) - 1u);
-        int psrc = pm ? (31 - __clz(pm)) : -1;
-        double st_c = __shfl_sync(FULL, st_own, s.base + (psrc < 0 ? 0 : psrc));
-        double stc = psrc < 0 ? 0.0 : st_c;
+        double stc = st_own;
+        if (__ballot_sync(FULL, s.active && !phi_ok) != 0u) {
+            unsigned pb = __ballot_sync(FULL, phi_ok && s.active);
+            unsigned pm = (pb >> s.base) & ((1u << (s.t + 1)) - 1u);
+            int psrc = pm ? (31 - __clz(pm)) : -1;
+            double st_c = __shfl_sync(FULL, st_own, s.base + (psrc < 0 ? 0 : psrc));
+            stc = psrc < 0 ? 0.0 : st_c;
+        }
         if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && s.active && frictionAngle < 0.0f)
             report(F.sc, SNAC_GPU_EPHYSICS, s.e);  // plastic/Constitutive.c:175 abort()
         double sphi = sin_fric(M, frictionAngle);
         double spsi = sin_dil(M, dilationAngle);
-        double anphi = dv(1.0f + sphi, 1.0f - sphi);
-        double anpsi = dv(1.0f + spsi, 1.0f - spsi);
+        double anphi = fconst ? M.anphi0 : dv(1.0f + sphi, 1.0f - sphi);
+        double anpsi = (M.dil_const && dilationAngle == M.dil0) ? M.anpsi0 : dv(1.0f + spsi, 1.0f - spsi);
         const double a1 = M.lambda + 2.0f * M.mu;
         const double a2 = M.lambda;
         // The reference always computes the principal stresses; they only
         // matter when the tet yields.  A tet that provably stays inside the
         // yield surface keeps its trial stress without the eigen-solve.
-        if (!surely_elastic(st, cohesion, anphi, stc)) {
+        if (!surely_elastic(st, cohesion, anphi, fconst ? M.sq_anphi0 : sqrt(anphi), stc)) {
             principal_stresses(st, sp, cn);
             mc_return_map(sp, cn, st, eps_p, cohesion, hardening, anphi, anpsi, stc, a1, a2);
         }
