@@ -42,7 +42,7 @@ NODES_PER_HEX = {"c1": 2601 / 2048, "c2": 139425 / 131072, "c3": 1081665 / 10485
 # DRAM bytes (read + write) of one launch of the dominant kernel, from one
 # ncu capture of that kernel on the same workload
 # (profiles/k_fused_step_plastic_64x32x64.md); None where none was taken.
-NCU_TRAFFIC = {("c2", "k_fused_step"): 83.451392e6 + 173.069056e6}
+NCU_TRAFFIC = {("c2", "k_fused_step"): 83.461888e6 + 170.524416e6}
 
 
 def algorithmic_bytes(workload: str) -> float:
@@ -580,7 +580,7 @@ def run_adjoint(args, ws, rank, local):
     clocks = sampler.stop() if sampler else None
     ms_adj = r.ms_forward + r.ms_reverse
     gnorm = float(max(np.abs(r.grad[k]).max() for k in r.grad))
-    fd_long = fd_check(maker(0.0), N, 1.0e-4, args.adj_fd, 11) if args.adj_fd else []
+    fd_long = fd_check(maker(0.0), N, 1.0e-5, args.adj_fd, 11) if args.adj_fd else []
     fd_short = fd_check(make, 24, 1.0e-6, args.adj_fd, 12) if args.adj_fd else []
     if rank == 0:
         value = ne * N / (ms_adj / 1e3)
@@ -595,7 +595,7 @@ def run_adjoint(args, ws, rank, local):
             "adjoint": {"loss": r.loss, "ms_forward_alone": ms_fwd, "ms_adjoint_call": ms_adj,
                         "ms_adjoint_forward_sweep": r.ms_forward, "ms_adjoint_reverse": r.ms_reverse,
                         "cost_in_forward_runs": ms_adj / ms_fwd, "max_abs_gradient": gnorm,
-                        "fd_full_horizon_demf0": {"steps": N, "h": 1.0e-4, "rel_errs": fd_long,
+                        "fd_full_horizon_demf0": {"steps": N, "h": 1.0e-5, "rel_errs": fd_long,
                                                   "max": max(fd_long) if fd_long else None},
                         "fd_24_steps_demf08": {"steps": 24, "h": 1.0e-6, "rel_errs": fd_short,
                                                "max": max(fd_short) if fd_short else None}},

@@ -49,6 +49,8 @@ struct Fields {
     const double* tbc_val;   // [n_tc]
     const unsigned char* mat;        // [ne] phase, NULL = 0
     const DevMaterial* mats;         // phase table of this model
+    double* escal;                   // [ne][4] element strain rate, stress, hydroPressure, aps
+                                     // (written on steps with sc->want_scalars; NULL = never)
     const double* coh_scale;         // [ne] or NULL
     const double* fric_scale;        // [ne] or NULL
     const double* visc_scale;        // [ne] or NULL
@@ -174,6 +176,16 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     sr[0] += corr;
     sr[1] += corr;
     sr[2] += corr;
+    // scalar element outputs for the dump writers, on the steps that need them
+    const bool want = F.escal != nullptr && F.sc->want_scalars;
+    if (want) {
+        // StrainRate.c:284-304
+        double srVolAvg = grp_sum(sr[1] * sr[2] + sr[2] * sr[0] + sr[0] * sr[1], s.base);
+        double srOtherAvg = grp_sum(sr[3] * sr[3] + sr[5] * sr[5] + sr[4] * sr[4], s.base);
+        srVolAvg = dv10(srVolAvg);
+        srOtherAvg = dv10(srOtherAvg);
+        if (s.active && s.t == 0) F.escal[s.e * 4 + 0] = 0.5f * sqrt(0.5f * fabs(-1.0f * srVolAvg + srOtherAvg));
+    }
 
     // strain, Stress.c:71-82
     double e[6];
@@ -360,6 +372,26 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     st[0] += cs2;
     st[1] += cs2;
     st[2] += cs2;
+    if (want) {
+        // Stress.c:130-156: the element's scalar stress and hydrostatic pressure
+        double sVolAvg = grp_sum((st[1] - avgTrace) * (st[2] - avgTrace) + (st[2] - avgTrace) * (st[0] - avgTrace) +
+                                     (st[0] - avgTrace) * (st[1] - avgTrace),
+                                 s.base);
+        double sOtherAvg = grp_sum(st[3] * st[3] + st[5] * st[5] + st[4] * st[4], s.base);
+        double pressure = grp_sum(dv3(st[0] + st[1] + st[2]), s.base);
+        sVolAvg = dv10(sVolAvg);
+        sOtherAvg = dv10(sOtherAvg);
+        pressure = dv10(pressure);
+        // plastic/Constitutive.c:239-244, viscoplastic/Constitutive.c:519-523: aps
+        double aps = 0.0;
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
+            aps = dv(grp_sum(eps_p * g.V, s.base), vsum);
+        if (s.active && s.t == 0) {
+            F.escal[s.e * 4 + 1] = 0.5f * sqrt(0.5f * fabs(-1.0f * sVolAvg + sOtherAvg));
+            F.escal[s.e * 4 + 2] = -1.0 * pressure;
+            F.escal[s.e * 4 + 3] = aps;
+        }
+    }
 
     if (cfg.has_density) {
         // Stress.c:125-170: pressure = mean tet trace/3, density update
