@@ -161,6 +161,7 @@ typedef struct snac_scalars {
     double vmax;             /* max |v| over velocity-BC nodes (floored at 3e-11f) */
     double speed_of_sound;
     long long time_step;     /* steps completed after step zero      */
+    double current_time;     /* sum of the steps' dt (AbstractContext currentTime) */
 } snac_scalars;
 
 typedef struct snac_gpu snac_gpu;
@@ -207,6 +208,30 @@ int  snac_gpu_upload(snac_gpu* h, const snac_state_view* v);
 int  snac_gpu_download(snac_gpu* h, const snac_state_view* v);
 int  snac_gpu_scalars(snac_gpu* h, snac_scalars* out);
 int  snac_gpu_set_dt(snac_gpu* h, double dt);   /* _Snac_Context_SetDt, Context.c:1047-1053 */
+
+/* ---- dump and checkpoint files --------------------------------------------------
+ * The reference's output files (Snac/libSnac/src/Context.c:1311-1531 with
+ * StGermain's VariableDumpStream, the plastic / visco-plastic / temperature
+ * plugins' Output.c): raw float32 records (int32 phase indices) appended per
+ * dump or checkpoint step to <output_path>/<name>.<rank>:
+ *   dump:       strainRate, stress, hydroPressure (element scalars), phaseIndex,
+ *               coord, vel, force (3 per node), stressTensor (6 per element,
+ *               volume-weighted in float), plStrain (aps), viscosity (log10 of
+ *               the mean), temperature
+ *   checkpoint: phaseIndexCP, coordCP, velCP, stressTensorCP (6 per tet),
+ *               plStrainCP, viscosityCP (log10 per tet), temperatureCP
+ *   rank 0:     sim.0, and timeStep.0 / checkpointTimeStep.0 lines
+ *               "%16u %16g %16g" (timeStep, currentTime, dt).
+ * Open before stepping: the steps whose end is a dump (isTimeToDump:
+ * timeStep 1 and every dump_every) then also store the element scalars.
+ * snac_gpu_write_output is _Snac_Context_WriteOutput + the loop-info writers
+ * for the current timeStep; it packs the records on the device, copies them
+ * into pinned memory and returns, and a writer thread appends them to the
+ * files (the next write or close waits for it). */
+int  snac_gpu_output_open(snac_gpu* h, const char* output_path, unsigned rank, unsigned dump_every,
+                          unsigned checkpoint_every, unsigned max_time_steps);
+int  snac_gpu_write_output(snac_gpu* h);
+int  snac_gpu_output_close(snac_gpu* h);
 
 /* ---- profiling ---------------------------------------------------------------- */
 /* One step launched kernel by kernel (no graph), with CUDA events recorded

@@ -78,6 +78,7 @@ typedef struct ref_ctx {
     SnacTemperature_Element* te;
     SnacTemperature_Node* tn;
     double vmax;
+    double currentTime; /* AbstractContext.c:871, 891 */
     double (*mass_store);
     double (*balance_store)[3];
     long timeStep_total;
@@ -546,6 +547,7 @@ int ref_time_step_zero(ref_ctx* r) {
 int ref_begin_step(ref_ctx* r) {
     r->ctx.timeStep++;
     r->ctx.dt = 1.0 * r->ctx.dt;
+    r->currentTime += r->ctx.dt;
     return status_of();
 }
 
@@ -632,6 +634,7 @@ void ref_scalars(ref_ctx* r, snac_scalars* o) {
     o->vmax = r->vmax;
     o->speed_of_sound = r->ctx.speedOfSound;
     o->time_step = r->ctx.timeStep;
+    o->current_time = r->currentTime;
 }
 
 void ref_set_dt(ref_ctx* r, double dt) { r->ctx.dt = dt; }

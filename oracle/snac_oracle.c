@@ -68,6 +68,7 @@ struct so_ctx {
     double dt, strain_inert, gravity, demf;
     double speedOfSound, minLengthScale, initMinLengthScale, vmax;
     long timeStep;
+    double currentTime; /* AbstractContext.c:871, 891 */
     int nmat;
     snac_material* mat;
     unsigned* rheology;         /* per phase */
@@ -1050,6 +1051,7 @@ int so_time_step_zero(so_ctx* s) {
 int so_begin_step(so_ctx* s) {
     s->timeStep++;
     s->dt = 1.0 * s->dt; /* dtFactor * AbstractContext_Dt */
+    s->currentTime += s->dt;
     return s->status;
 }
 
@@ -1376,6 +1378,7 @@ void so_scalars(so_ctx* s, snac_scalars* o) {
     o->vmax = s->vmax;
     o->speed_of_sound = s->speedOfSound;
     o->time_step = s->timeStep;
+    o->current_time = s->currentTime;
 }
 
 void so_set_dt(so_ctx* s, double dt) { s->dt = dt; }

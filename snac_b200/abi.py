@@ -135,7 +135,7 @@ class BatchTuning(C.Structure):
 
 class Scalars(C.Structure):
     _fields_ = [("dt", C.c_double), ("min_length_scale", C.c_double), ("vmax", C.c_double),
-                ("speed_of_sound", C.c_double), ("time_step", C.c_longlong)]
+                ("speed_of_sound", C.c_double), ("time_step", C.c_longlong), ("current_time", C.c_double)]
 
 
 def _dptr(a: Optional[np.ndarray]):

@@ -74,6 +74,12 @@ def load_library(path: str = LIB_PATH):
     lib.snac_gpu_selftest_division.restype = C.c_int
     lib.snac_gpu_device_count.argtypes = []
     lib.snac_gpu_device_count.restype = C.c_int
+    lib.snac_gpu_output_open.argtypes = [vp, C.c_char_p, C.c_uint, C.c_uint, C.c_uint, C.c_uint]
+    lib.snac_gpu_output_open.restype = C.c_int
+    lib.snac_gpu_write_output.argtypes = [vp]
+    lib.snac_gpu_write_output.restype = C.c_int
+    lib.snac_gpu_output_close.argtypes = [vp]
+    lib.snac_gpu_output_close.restype = C.c_int
     # batched ensembles
     lib.snac_gpu_batch_create.argtypes = [C.POINTER(Desc), C.c_int, C.POINTER(vp)]
     lib.snac_gpu_batch_create.restype = C.c_int
@@ -220,6 +226,20 @@ class SnacContext:
 
     def set_dt(self, dt: float):
         self._check(self.lib.snac_gpu_set_dt(self.h, C.c_double(dt)))
+
+    # -- output files in the reference's format ---------------------------------------
+    def output_open(self, path: str, rank: int = 0, dump_every: int = 1, checkpoint_every: int = 0,
+                    max_time_steps: int = 0):
+        """Context.c _Snac_Context_InitDump / InitCheckpoint: open the dump files."""
+        return self._check(self.lib.snac_gpu_output_open(self.h, path.encode(), rank, dump_every,
+                                                          checkpoint_every, max_time_steps))
+
+    def write_output(self):
+        """_Snac_Context_WriteOutput for the current timeStep (asynchronous file writes)."""
+        return self._check(self.lib.snac_gpu_write_output(self.h))
+
+    def output_close(self):
+        return self._check(self.lib.snac_gpu_output_close(self.h))
 
     def profile_step(self):
         """One step kernel by kernel with CUDA events: [(kernel name, ms)]."""

@@ -798,6 +798,22 @@ __global__ void k_adj_loss(Mesh m, const double4* pos, const double4* vel, const
     B.fbar[n] = make_double4(0, 0, 0, 0);
 }
 
+// up to 6 array copies in one launch (checkpoint save / restore), 64-bit words
+struct CopyJob {
+    unsigned long long* dst[6];
+    const unsigned long long* src[6];
+    long long n[6];
+    int count;
+};
+__global__ void __launch_bounds__(256) k_copy_many(CopyJob J) {
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (int a = 0; a < J.count; a++) {
+        unsigned long long* d = J.dst[a];
+        const unsigned long long* s = J.src[a];
+        for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < J.n[a]; i += stride) d[i] = s[i];
+    }
+}
+
 // per-element gradients: sum of the element's 10 tets in tet order
 __global__ void k_adj_reduce(long long ne, const double* pbar, double* gc, double* gf, double* gv) {
     long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -14,14 +14,43 @@
 #include <cstring>
 #include <mutex>
 #include <new>
+#include <string>
+#include <thread>
 #include <vector>
 
 #include "snac_gpu.h"
 #include "snac_adjoint.cuh"
 #include "snac_batch.cuh"
+#include "snac_output.cuh"
 #include "snac_kernels.cuh"
 
 using namespace snac;
+
+// Dump / checkpoint files in the reference's format (see snac_gpu_output_open)
+struct OutputState {
+    enum {
+        D_SR, D_ST, D_HP, D_PH, D_CO, D_VE, D_FO, D_TEN, D_PL, D_VI, D_TE,
+        C_PH, C_CO, C_VE, C_TEN, C_PL, C_VI, C_TE, T_STEP, T_CP, T_SIM, NF
+    };
+    std::string dir;
+    unsigned rank = 0, dump_every = 1, checkpoint_every = 0, max_steps = 0;
+    FILE* f[NF] = {};
+    char* dstage = nullptr;   // device staging
+    char* pinned = nullptr;   // pinned host copy
+    size_t cap = 0;
+    cudaEvent_t ready = nullptr;
+    std::thread writer;
+    struct Piece {
+        int file;
+        size_t off, bytes;
+    };
+    std::vector<Piece> pieces;
+    std::string lines[2];     // timeStep / checkpointTimeStep records of the pending write
+    size_t scal_off = 0;      // where the step scalars sit in the pinned copy
+    bool dump = false, cp = false;
+    int err = 0;
+    int want = 0;             // the last element-scalar request sent to the device
+};
 
 struct snac_gpu {
     Mesh mesh{};
@@ -57,6 +86,8 @@ struct snac_gpu {
     double* visc_scale = nullptr;
     DevScalars* sc = nullptr;
     double* stage = nullptr;  // host-transfer staging, 3 doubles per node (first upload/download)
+    double* escal = nullptr;  // [ne][4] element scalars for the dump files (allocated by snac_gpu_output_open)
+    OutputState* out = nullptr;
     // host mirror of the step bookkeeping
     int parity = 0;
     long long time_step = 0;
@@ -189,6 +220,7 @@ Fields fields_at(const snac_gpu* h, int parity) {
     F.tbc_val = h->tbc_val;
     F.mat = h->mat;
     F.mats = h->mats;
+    F.escal = h->escal;
     F.coh_scale = h->coh_scale;
     F.fric_scale = h->fric_scale;
     F.visc_scale = h->visc_scale;
@@ -379,9 +411,31 @@ int read_status(snac_gpu* h) {
     return 0;
 }
 
+// _Snac_Context's isTimeToDump / isTimeToCheckpoint (Context.c:1505-1531)
+bool time_to_dump(const OutputState* o, long long ts) {
+    return ts == 1 || (ts > 1 && o->dump_every && ts % o->dump_every == 0);
+}
+bool time_to_checkpoint(const OutputState* o, long long ts) {
+    if (ts == (long long)o->max_steps) return true;
+    if (ts == 0 || o->checkpoint_every == 0) return false;
+    return ts % o->checkpoint_every == 0;
+}
+
+// Before step ts runs: ask its stress update to store the element scalars
+// when a dump follows it.  A plain stream operation outside any graph.
+int request_scalars(snac_gpu* h, long long ts) {
+    if (!h->out) return 0;
+    const int want = time_to_dump(h->out, ts) ? 1 : 0;
+    if (want == h->out->want) return 0;
+    CK(cudaMemsetAsync(&h->sc->want_scalars, want, sizeof(int), h->stream));  // any nonzero byte pattern is true
+    h->out->want = want;
+    return 0;
+}
+
 // one step from the handle's CUDA graph for its (pending, parity) state,
 // captured on first use; no status read
 int launch_step(snac_gpu* h) {
+    if (int rc = request_scalars(h, h->time_step + 1)) return rc;
     int p = h->parity, f = h->pending ? 1 : 0;
     if (!h->graph[f][p]) {
         cudaGraph_t g;
@@ -699,15 +753,18 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
 
 int snac_gpu_create(const snac_gpu_desc* d, snac_gpu** out) { return create_model(d, out, nullptr); }
 
+int snac_gpu_output_close(snac_gpu* h);
+
 void snac_gpu_destroy(snac_gpu* h) {
     if (!h) return;
+    snac_gpu_output_close(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (auto& gf : h->graph)
         for (auto& g : gf)
             if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
-                    h->visc_scale, h->sc, h->stage};
+                    h->visc_scale, h->sc, h->stage, h->escal};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
@@ -750,6 +807,7 @@ int snac_gpu_step(snac_gpu* h, int nsteps) {
 
 int snac_gpu_begin_step(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    if (int rc = request_scalars(h, h->time_step + 1)) return rc;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
     int rc = flush_pending(h);
     return rc ? rc : op_begin(h);
@@ -839,6 +897,7 @@ int snac_gpu_scalars(snac_gpu* h, snac_scalars* out) {
     out->vmax = s.vmax;
     out->speed_of_sound = s.speed_of_sound;
     out->time_step = s.time_step;
+    out->current_time = s.current_time;
     return 0;
 }
 
@@ -1374,31 +1433,37 @@ void snap_free(Snap& z) {
     z = Snap();
 }
 
-int snap_save(snac_gpu* h, Snap& z) {
+// one launch copying the six arrays of a state (sizes in 64-bit words)
+int snap_copy(snac_gpu* h, bool save, Snap& z) {
+    static_assert(sizeof(DevScalars) % 8 == 0, "scalars are copied as 64-bit words");
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
-    CK(cudaMemcpyAsync(z.pos, h->pos[h->parity], nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(z.vel, h->vel, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(z.force, h->force, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(z.stress, h->stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(z.eps_p, h->eps_p, nq * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(z.sc, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream));
-    z.pending = h->pending;
-    z.time_step = h->time_step;
+    using U = unsigned long long;
+    U* hp[6] = {(U*)h->pos[h->parity], (U*)h->vel, (U*)h->force, (U*)h->stress, (U*)h->eps_p, (U*)h->sc};
+    U* zp[6] = {(U*)z.pos, (U*)z.vel, (U*)z.force, (U*)z.stress, (U*)z.eps_p, (U*)z.sc};
+    const long long n[6] = {nn * 4, nn * 4, nn * 4, nq * 6, nq, (long long)(sizeof(DevScalars) / 8)};
+    CopyJob J;
+    J.count = 6;
+    for (int a = 0; a < 6; a++) {
+        J.dst[a] = save ? zp[a] : hp[a];
+        J.src[a] = save ? hp[a] : zp[a];
+        J.n[a] = n[a];
+    }
+    k_copy_many<<<148 * 8, 256, 0, h->stream>>>(J);
+    h->launches++;
+    int rc = launch_check_named(h, "k_copy_many");
+    if (rc) return rc;
+    if (save) {
+        z.pending = h->pending;
+        z.time_step = h->time_step;
+    } else {
+        h->pending = z.pending;
+        h->time_step = z.time_step;
+    }
     return 0;
 }
 
-int snap_restore(snac_gpu* h, const Snap& z) {
-    const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
-    CK(cudaMemcpyAsync(h->pos[h->parity], z.pos, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->vel, z.vel, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->force, z.force, nn * sizeof(double4), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->stress, z.stress, nq * 6 * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->eps_p, z.eps_p, nq * sizeof(double), cudaMemcpyDeviceToDevice, h->stream));
-    CK(cudaMemcpyAsync(h->sc, z.sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream));
-    h->pending = z.pending;
-    h->time_step = z.time_step;
-    return 0;
-}
+int snap_save(snac_gpu* h, Snap& z) { return snap_copy(h, true, z); }
+int snap_restore(snac_gpu* h, const Snap& z) { return snap_copy(h, false, const_cast<Snap&>(z)); }
 
 AdjState adj_state(const Snap& z) { return AdjState{z.pos, z.vel, z.force, z.stress, z.eps_p}; }
 
@@ -1584,7 +1649,7 @@ int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, doub
     for (int j = ncp - 1; j >= 0; j--) {
         const int a0 = j * K, b0 = std::min(a0 + K, N);
         ACK(snap_restore(h, cp[j]));
-        ACK(snap_save(h, seg[0]));
+        std::swap(seg[0], cp[j]);  // the checkpoint is the segment's first state
         for (int k = a0 + 1; k <= b0; k++) {
             ACK(launch_step(h));
             ACK(snap_save(h, seg[k - a0]));
@@ -1627,6 +1692,193 @@ int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, doub
     cleanup();
 #undef ACK
     return 0;
+}
+
+}  // extern "C"
+
+// ======================================================================================
+// Dump and checkpoint files in the reference's format
+// ======================================================================================
+namespace {
+
+const char* const kOutName[OutputState::NF] = {
+    "strainRate", "stress", "hydroPressure", "phaseIndex", "coord", "vel", "force", "stressTensor", "plStrain",
+    "viscosity", "temperature", "phaseIndexCP", "coordCP", "velCP", "stressTensorCP", "plStrainCP", "viscosityCP",
+    "temperatureCP", "timeStep", "checkpointTimeStep", "sim"};
+
+void output_join(OutputState* o) {
+    if (o->writer.joinable()) o->writer.join();
+}
+
+// runs on the writer thread once the device records are in pinned memory
+void output_write(OutputState* o) {
+    if (cudaEventSynchronize(o->ready) != cudaSuccess) {
+        o->err = SNAC_GPU_ECUDA;
+        return;
+    }
+    for (const auto& p : o->pieces)
+        if (o->f[p.file] && fwrite(o->pinned + p.off, 1, p.bytes, o->f[p.file]) != p.bytes) o->err = SNAC_GPU_EINVAL;
+    DevScalars sc;
+    memcpy(&sc, o->pinned + o->scal_off, sizeof sc);
+    // Context.c:1286-1298 (rank 0 only): timeStep, currentTime, dt after Sync
+    char line[128];
+    snprintf(line, sizeof line, "%16u %16g %16g\n", (unsigned)sc.time_step, sc.current_time, sc.dt);
+    if (o->dump && o->f[OutputState::T_STEP]) fputs(line, o->f[OutputState::T_STEP]);
+    if (o->cp && o->f[OutputState::T_CP]) fputs(line, o->f[OutputState::T_CP]);
+    for (FILE* f : o->f)
+        if (f) fflush(f);
+}
+
+}  // namespace
+
+extern "C" {
+
+int snac_gpu_output_open(snac_gpu* h, const char* output_path, unsigned rank, unsigned dump_every,
+                         unsigned checkpoint_every, unsigned max_time_steps) {
+    if (!h || !output_path || dump_every == 0) return SNAC_GPU_EINVAL;
+    if (h->out) return set_err(h, SNAC_GPU_ESTATE, -1, "output files are already open");
+    OutputState* o = new (std::nothrow) OutputState();
+    if (!o) return SNAC_GPU_ENOMEM;
+    o->dir = output_path;
+    o->rank = rank;
+    o->dump_every = dump_every;
+    o->checkpoint_every = checkpoint_every;
+    o->max_steps = max_time_steps;
+    const bool plastic = h->constitutive == SNAC_RHEOLOGY_PLASTIC || h->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC;
+    const bool visc = h->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC;
+    for (int i = 0; i < OutputState::NF; i++) {
+        if ((i == OutputState::D_PL || i == OutputState::C_PL) && !plastic) continue;
+        if ((i == OutputState::D_VI || i == OutputState::C_VI) && !visc) continue;
+        if ((i == OutputState::D_TE || i == OutputState::C_TE) && !h->temperature) continue;
+        if (i >= OutputState::T_STEP && rank != 0) continue;  // rank 0 only, Context.c:429-463
+        std::string fn = o->dir + "/" + kOutName[i] + "." + std::to_string(rank);
+        o->f[i] = fopen(fn.c_str(), "w+");
+        if (!o->f[i]) {
+            for (FILE* f : o->f)
+                if (f) fclose(f);
+            delete o;
+            return set_err(h, SNAC_GPU_EINVAL, -1, "cannot open %s for writing", fn.c_str());
+        }
+    }
+    if (o->f[OutputState::T_SIM]) {  // Context.c:431-446, one rank: the local counts are the global ones
+        fprintf(o->f[OutputState::T_SIM],
+                "%u %u %u %u %u %u %u %u %u\n(global element numbers)[3]=(proc numbers)[3]*(local element numbers)[3]\n",
+                h->mesh.nx, h->mesh.ny, h->mesh.nz, 1u, 1u, 1u, h->mesh.nx, h->mesh.ny, h->mesh.nz);
+        fflush(o->f[OutputState::T_SIM]);
+    }
+    // staging: the largest write is a dump plus a checkpoint at the same step
+    const long long ne = h->mesh.ne, nn = h->mesh.nn;
+    const size_t need = (size_t)(ne * (4 + 1 + 6 + 1 + 1) + nn * (3 * 3 + 1) + ne * (1 + 60 + 10 + 10) + nn * (3 * 2 + 1)) * 4 +
+                        sizeof(DevScalars) + 256 * 24;
+    cudaError_t e = cudaMalloc((void**)&o->dstage, need);
+    if (e == cudaSuccess) e = cudaMallocHost((void**)&o->pinned, need);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o->ready, cudaEventDisableTiming);
+    if (e == cudaSuccess && !h->escal) {
+        e = cudaMalloc((void**)&h->escal, ne * 4 * sizeof(double));
+        if (e == cudaSuccess) e = cudaMemsetAsync(h->escal, 0, ne * 4 * sizeof(double), h->stream);
+    }
+    o->cap = need;
+    h->out = o;
+    if (e != cudaSuccess) {
+        snac_gpu_output_close(h);
+        return set_err(h, SNAC_GPU_ENOMEM, -1, "output staging: %s", cudaGetErrorString(e));
+    }
+    // the graphs hold the field pointers: re-capture them with the element-scalar buffer
+    for (auto& gf : h->graph)
+        for (auto& g : gf)
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+    return 0;
+}
+
+int snac_gpu_write_output(snac_gpu* h) {
+    if (!h) return SNAC_GPU_EINVAL;
+    OutputState* o = h->out;
+    if (!o) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_output_open must come first");
+    const long long ts = h->time_step;
+    const bool dump = time_to_dump(o, ts), cp = time_to_checkpoint(o, ts);
+    if (!dump && !cp) return 0;
+    output_join(o);  // the previous write has left the pinned buffer
+    if (o->err) return set_err(h, o->err, -1, "writing the output files failed");
+    int rc = flush_pending(h);  // the files hold the end-of-step state
+    if (rc) return rc;
+    o->dump = dump;
+    o->cp = cp;
+    o->pieces.clear();
+    size_t off = 0;
+    auto take = [&](int file, size_t bytes) -> char* {
+        if (!o->f[file]) return nullptr;
+        char* p = o->dstage + off;
+        o->pieces.push_back({file, off, bytes});
+        off = (off + bytes + 255) & ~(size_t)255;
+        return p;
+    };
+    const long long ne = h->mesh.ne, nn = h->mesh.nn;
+    using S = OutputState;
+    float *co = nullptr, *ve = nullptr, *fo = nullptr, *te = nullptr, *cco = nullptr, *cve = nullptr, *cte = nullptr;
+    ElemOut E{};
+    if (dump) {
+        E.strain_rate = (float*)take(S::D_SR, ne * 4);
+        E.stress = (float*)take(S::D_ST, ne * 4);
+        E.hydro_pressure = (float*)take(S::D_HP, ne * 4);
+        E.tensor = (float*)take(S::D_TEN, ne * 24);
+        co = (float*)take(S::D_CO, nn * 12);
+        ve = (float*)take(S::D_VE, nn * 12);
+        fo = (float*)take(S::D_FO, nn * 12);
+        E.phase = (int*)take(S::D_PH, ne * 4);
+        E.aps = (float*)take(S::D_PL, ne * 4);
+        E.log_visc = (float*)take(S::D_VI, ne * 4);
+        te = (float*)take(S::D_TE, nn * 4);
+    }
+    if (cp) {
+        E.tensor_cp = (float*)take(S::C_TEN, ne * 240);
+        cco = (float*)take(S::C_CO, nn * 12);
+        cve = (float*)take(S::C_VE, nn * 12);
+        E.phase_cp = (int*)take(S::C_PH, ne * 4);
+        E.eps_cp = (float*)take(S::C_PL, ne * 40);
+        E.log_visc_cp = (float*)take(S::C_VI, ne * 40);
+        cte = (float*)take(S::C_TE, nn * 4);
+    }
+    o->scal_off = off;
+    off += sizeof(DevScalars);
+    if (off > o->cap) return set_err(h, SNAC_GPU_EINVAL, -1, "output staging too small");
+    const Fields F = fields(h);
+    const unsigned nb = (unsigned)((nn + 255) / 256), eb = (unsigned)((ne + 127) / 128);
+    if (co || ve || fo || te) {
+        k_out_nodes<<<nb, 256, 0, h->stream>>>(F.pos, F.vel, F.force, nn, co, ve, fo, te);
+        h->launches++;
+        if ((rc = launch_check_named(h, "k_out_nodes"))) return rc;
+    }
+    if (cco || cve || cte) {
+        k_out_nodes<<<nb, 256, 0, h->stream>>>(F.pos, F.vel, F.force, nn, cco, cve, nullptr, cte);
+        h->launches++;
+        if ((rc = launch_check_named(h, "k_out_nodes"))) return rc;
+    }
+    k_out_elements<<<eb, 128, 0, h->stream>>>(h->mesh, F, E);
+    h->launches++;
+    if ((rc = launch_check_named(h, "k_out_elements"))) return rc;
+    CK(cudaMemcpyAsync(o->dstage + o->scal_off, h->sc, sizeof(DevScalars), cudaMemcpyDeviceToDevice, h->stream));
+    CK(cudaMemcpyAsync(o->pinned, o->dstage, off, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaEventRecord(o->ready, h->stream));
+    o->writer = std::thread(output_write, o);
+    return 0;
+}
+
+int snac_gpu_output_close(snac_gpu* h) {
+    if (!h || !h->out) return h ? 0 : SNAC_GPU_EINVAL;
+    OutputState* o = h->out;
+    output_join(o);
+    const int err = o->err;
+    for (FILE* f : o->f)
+        if (f) fclose(f);
+    if (o->dstage) cudaFree(o->dstage);
+    if (o->pinned) cudaFreeHost(o->pinned);
+    if (o->ready) cudaEventDestroy(o->ready);
+    delete o;
+    h->out = nullptr;
+    return err ? set_err(h, err, -1, "writing the output files failed") : 0;
 }
 
 }  // extern "C"

@@ -122,6 +122,7 @@ __global__ void kb_begin_step(const ModelDesc* __restrict__ D, int n) {
         DevScalars* sc = D[i].F.sc;
         sc->time_step += 1;
         sc->dt = 1.0 * sc->dt;
+        sc->current_time += sc->dt;
     }
 }
 

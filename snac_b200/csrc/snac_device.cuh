@@ -101,6 +101,7 @@ struct DevScalars {
     unsigned long long minls_bits;   // running min of |V/A| (non-negative doubles order as integers)
     unsigned long long vmax_bits;    // running max of |v| over velocity-BC nodes
     long long time_step;
+    double current_time;             // AbstractContext currentTime: the sum of the steps' dt
     int pos_parity;                  // which of the two coordinate buffers is current
     int want_scalars;                // the next step stores the element scalars (a dump follows it)
     int status;                      // first error (SNAC_GPU_E*), 0 if none

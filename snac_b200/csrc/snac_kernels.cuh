@@ -512,7 +512,10 @@ __device__ __forceinline__ void element_update_tet(const Fields& F, const Config
 template <int PLUGIN>
 __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
-    if (lb == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+    if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
+        F.sc->time_step += 1;
+        F.sc->current_time += F.sc->dt;
+    }
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -792,7 +795,10 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(M
 template <int PLUGIN>
 __device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
-    if (lb == 0 && threadIdx.x == 0) F.sc->time_step += 1;  // _AbstractContext_Execute_Hook: timeStep++
+    if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
+        F.sc->time_step += 1;
+        F.sc->current_time += F.sc->dt;
+    }
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -966,6 +972,7 @@ __global__ void k_begin_step(DevScalars* sc) {
     if (threadIdx.x == 0 && blockIdx.x == 0) {
         sc->time_step += 1;
         sc->dt = 1.0 * sc->dt;
+        sc->current_time += sc->dt;
     }
 }
 

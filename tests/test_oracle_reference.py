@@ -45,6 +45,11 @@ def test_restatement_is_bitwise_equal_to_reference(case):
             assert np.array_equal(x, y), (case, f, np.max(np.abs(x - y)))
         assert a.scalars().dt == b.scalars().dt
         assert a.scalars().min_length_scale == b.scalars().min_length_scale
+        assert a.scalars().current_time == b.scalars().current_time
+        # element scalars of the dump files: strain rate, stress, hydroPressure, aps
+        ea, eb = a.element_scalars(), b.element_scalars()
+        for k in ("strain_rate", "stress", "hydro_pressure", "aps", "volume"):
+            assert np.array_equal(ea[k], eb[k]), (case, k)
 
 
 def test_plastic_case_actually_yields():
