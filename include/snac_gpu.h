@@ -140,6 +140,16 @@ typedef struct snac_gpu_desc {
     const double* init_velocity;     /* [nn*3] nodeICs, NULL = 0      */
     const double* init_temperature;  /* [nn], used when temperature_sweep_ic == 0 */
     const double* init_stress;       /* [ne*10*6] elementICs, NULL = 0 (hydrostatic_ic adds on top) */
+
+    /* SnacWinklerForce loaded (Snac/plugins/winkler/Force.c:56-168): bottom
+     * support on the j = 0 nodes from the isostatic pressure pisos and the
+     * reference bottom depth rzbo, both set by the hydrostatic IC
+     * (hydroStaticIC/VariableConditions.c:120-138; 0 without it). */
+    int    winkler;
+    /* SnacTractionBC loaded (Snac/plugins/tractionBC/Force.c:43-268): its one
+     * active branch applies the fixed stress sxx = 1e8 Pa on the right wall
+     * (i = nx).  Force hooks run in load order: Winkler, then traction. */
+    int    traction_bc;
 } snac_gpu_desc;
 
 /* Host-side view of the state for upload / download.  NULL members are

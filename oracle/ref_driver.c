@@ -22,7 +22,12 @@
 #include "common/snac_shim_maxwell.h"
 #include "common/snac_shim_temperature.h"
 #include "common/snac_shim_hydro.h"
+#include "common/snac_shim_winkler.h"
+#include "common/snac_shim_traction.h"
 #include "../include/snac_gpu.h"
+
+/* winkler/Register.c's globals (used by its spherical variant only) */
+double Spherical_RMin, Spherical_RMax;
 
 void SnacPlastic_Constitutive(void* context, Element_LocalIndex element_lI);
 void SnacViscoPlastic_Constitutive(void* context, Element_LocalIndex element_lI);
@@ -79,6 +84,7 @@ typedef struct ref_ctx {
     SnacTemperature_Node* tn;
     double vmax;
     double currentTime; /* AbstractContext.c:871, 891 */
+    int winkler, traction;
     double (*mass_store);
     double (*balance_store)[3];
     long timeStep_total;
@@ -279,6 +285,8 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
     c->dt = d->dt;
     c->strain_inert = d->strain_inert;
     c->gravity = d->gravity;
+    r->winkler = d->winkler;
+    r->traction = d->traction_bc;
     c->demf = d->demf;
     c->topo_kappa = 0.0;
     c->topoGradCriterion = 1.0e-16;
@@ -476,6 +484,12 @@ int ref_loop_nodes_momentum(ref_ctx* r) {
     for (unsigned n = 0; n < r->nn; n++) {
         Snac_Node* node = &r->mesh.node[n];
         Snac_Force(c, n, c->speedOfSound, &r->mass_store[n], &node->inertialMass, &node->force, &r->balance_store[n]);
+        if (r->winkler)  /* appended to Snac_EP_Force, winkler/Register.c:140-145 */
+            _SnacWinklerForce_Apply(c, n, c->speedOfSound, &r->mass_store[n], &node->inertialMass, &node->force,
+                                    &r->balance_store[n]);
+        if (r->traction)  /* tractionBC/Register.c:79-83 */
+            _SnacTractionBC_Force_Apply(c, n, c->speedOfSound, &r->mass_store[n], &node->inertialMass, &node->force,
+                                        &r->balance_store[n]);
     }
     for (unsigned n = 0; n < r->nn; n++) {
         Snac_Node* node = &r->mesh.node[n];

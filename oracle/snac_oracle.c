@@ -69,6 +69,10 @@ struct so_ctx {
     double speedOfSound, minLengthScale, initMinLengthScale, vmax;
     long timeStep;
     double currentTime; /* AbstractContext.c:871, 891 */
+    int winkler;        /* SnacWinklerForce loaded */
+    int traction;       /* SnacTractionBC loaded */
+    double pisos, rzbo; /* hydroStaticIC/VariableConditions.c:120, 138 */
+    double* residualFr; /* [nn] winkler/Force.c:154-161 */
     int nmat;
     snac_material* mat;
     unsigned* rheology;         /* per phase */
@@ -818,6 +822,83 @@ static void node_force(so_ctx* s, long n) {
     s->mass[n] = mass;
 }
 
+/* ---- tractionBC/Force.c:43-268: its active branch, a fixed stress on the right wall -- */
+static void traction_force(so_ctx* s, long n) {
+    const double factor4 = 1.0f / 4.0f;
+    double* f = s->force[n];
+    double* bal = s->balance[n];
+    const long i = n % s->nnx;
+    if (i != s->nnx - 1) return;
+    double stress[3][3] = {{1.0e+08, 0.0, 0.0}, {0.0, 0.0, 0.0}, {0.0, 0.0, 0.0}};
+    long els[8];
+    node_elements(s, n, els);
+    for (int ne = 0; ne < 8; ne++) {
+        long e = els[ne];
+        if (e < 0) continue;
+        const double* c1 = s->coord[enode(s, e, 1)];
+        const double* c2 = s->coord[enode(s, e, 2)];
+        const double* c5 = s->coord[enode(s, e, 5)];
+        const double* c6 = s->coord[enode(s, e, 6)];
+        double n1[3], n2[3], normal[3];
+        double area = so_tetrahedra_surface_area(c1, c2, c6) + so_tetrahedra_surface_area(c1, c6, c5);
+        so_tetrahedra_surface_normal(c1, c2, c6, n1);
+        so_tetrahedra_surface_normal(c1, c6, c5, n2);
+        normal[0] = 0.5f * (n1[0] + n2[0]);
+        normal[1] = 0.5f * (n1[1] + n2[1]);
+        normal[2] = 0.5f * (n1[2] + n2[2]);
+        f[0] += factor4 * area * (stress[0][0] * normal[0] + stress[0][1] * normal[1] + stress[0][2] * normal[2]);
+        f[1] += factor4 * area * (stress[1][0] * normal[0] + stress[1][1] * normal[1] + stress[1][2] * normal[2]);
+        f[2] += factor4 * area * (stress[2][0] * normal[0] + stress[2][1] * normal[1] + stress[2][2] * normal[2]);
+        bal[0] += fabs(f[0]);
+        bal[1] += fabs(f[1]);
+        bal[2] += fabs(f[2]);
+    }
+}
+
+/* ---- winkler/Force.c:56-168: bottom support (Winkler foundation) on j = 0 ---------- */
+static void winkler_force(so_ctx* s, long n) {
+    const double factor4 = 1.0f / 4.0f;
+    double* f = s->force[n];
+    const long j = (n / s->nnx) % s->nny;
+    if (!(s->gravity > 0.0) || j != 0) return;
+    long els[8];
+    node_elements(s, n, els);
+    const double nodeT = 0.0; /* the temperature lookup is compiled out (#if 0) */
+    for (int ne = 0; ne < 8; ne++) {
+        long e = els[ne];
+        if (e < 0) continue;
+        so_element* el = &s->el[e];
+        const snac_material* m = &s->mat[el->material];
+        const double phsDensity = m->density, drosub = 0.0f;
+        double p_est = s->pisos + 0.5f * (phsDensity + drosub) * s->gravity * (s->coord[n][1] - s->rzbo);
+        double rosubg = s->gravity * (phsDensity + drosub) * (1.0 - m->alpha * (nodeT - m->reftemp) + m->beta * p_est);
+        double area = 0.0f, normal[3];
+        double dhE = factor4 * (s->coord[enode(s, e, 0)][1] + s->coord[enode(s, e, 1)][1] +
+                                s->coord[enode(s, e, 4)][1] + s->coord[enode(s, e, 5)][1]);
+        const so_surface* s1 = &el->tet[1].surface[0];
+        const so_surface* s2 = &el->tet[2].surface[1];
+        const so_surface* s3 = &el->tet[6].surface[2];
+        const so_surface* s4 = &el->tet[8].surface[2];
+        area += s1->area;
+        area += s2->area;
+        area += s3->area;
+        area += s4->area;
+        normal[0] = factor4 * (s1->normal[0] + s2->normal[0] + s3->normal[0] + s4->normal[0]);
+        normal[1] = -1.0f * factor4 * (s1->normal[1] + s2->normal[1] + s3->normal[1] + s4->normal[1]);
+        normal[2] = factor4 * (s1->normal[2] + s2->normal[2] + s3->normal[2] + s4->normal[2]);
+        area *= 0.5f;
+        double press_norm = s->pisos + rosubg * (s->rzbo - dhE);
+        f[0] += factor4 * (press_norm * area * normal[0]);
+        f[1] += factor4 * (press_norm * area * normal[1]);
+        f[2] += factor4 * (press_norm * area * normal[2]);
+    }
+    if (s->timeStep == 1) { /* restartTimestep == 0 */
+        double Fy = f[1];
+        if (Fy != 0.0) s->residualFr[n] = Fy;
+    }
+    f[1] -= s->residualFr[n];
+}
+
 #define getsign(val) ((val) < 0 ? -1.0f : (val) > 0 ? +1.0f : 0.0f)
 
 /* ---- UpdateNode.c:74-158 (PreProcess) then :60-72 ------------------------------ */
@@ -985,12 +1066,20 @@ int so_calc_stresses(so_ctx* s) {
 /* Snac_Force for every node without the node update (the force loop of
  * _Snac_Context_LoopNodes, Context.c:1129-1140) */
 int so_node_forces(so_ctx* s) {
-    for (long n = 0; n < s->nn; n++) node_force(s, n);
+    for (long n = 0; n < s->nn; n++) {
+        node_force(s, n);
+        if (s->winkler) winkler_force(s, n); /* appended to Snac_EP_Force, winkler/Register.c:140-145 */
+        if (s->traction) traction_force(s, n); /* tractionBC/Register.c:79-83 */
+    }
     return s->status;
 }
 
 int so_loop_nodes_momentum(so_ctx* s) {
-    for (long n = 0; n < s->nn; n++) node_force(s, n);
+    for (long n = 0; n < s->nn; n++) {
+        node_force(s, n);
+        if (s->winkler) winkler_force(s, n); /* appended to Snac_EP_Force, winkler/Register.c:140-145 */
+        if (s->traction) traction_force(s, n); /* tractionBC/Register.c:79-83 */
+    }
     for (long n = 0; n < s->nn; n++) node_update(s, n);
     return s->status;
 }
@@ -1083,7 +1172,8 @@ static int wall_has(const so_ctx* s, int wall, int i, int j, int k) {
 }
 
 /* hydroStaticIC/VariableConditions.c:43-152, one rank */
-static void hydrostatic_ic(so_ctx* s) {
+static void hydrostatic_ic(so_ctx* s, double ymin) {
+    s->rzbo = ymin; /* element->rzbo = geometry->min[1], :120 */
     for (int elK = 0; elK < s->nz; elK++)
         for (int elI = 0; elI < s->nx; elI++) {
             double rogh = 0.0f;
@@ -1119,6 +1209,8 @@ static void hydrostatic_ic(so_ctx* s) {
                 }
                 el->hydroPressure = P;
                 rogh += dP;
+                /* the isostatic pressure at the bottom of column (0, 0), :133-140 */
+                if (elJ == 0 && elI == 0 && elK == 0) s->pisos = rogh + 0.0;
             }
         }
 }
@@ -1151,6 +1243,9 @@ so_ctx* so_create(const snac_gpu_desc* d, int* status) {
     s->force = calloc(s->nn, sizeof *s->force);
     s->balance = calloc(s->nn, sizeof *s->balance);
     s->imass = calloc(s->nn, sizeof(double));
+    s->winkler = d->winkler;
+    s->traction = d->traction_bc;
+    s->residualFr = calloc(s->nn, sizeof(double));
     s->mass = calloc(s->nn, sizeof(double));
     s->T = calloc(s->nn, sizeof(double));
     s->T0 = calloc(s->nn, sizeof(double));
@@ -1289,7 +1384,7 @@ so_ctx* so_create(const snac_gpu_desc* d, int* status) {
         double dtm = 1.0e-01 * s->mat[0].vis_min / s->mat[0].mu;
         if (s->dt > dtm && s->dt_type != SNAC_DT_CONSTANT) s->dt = dtm;
     }
-    if (d->hydrostatic_ic) hydrostatic_ic(s);
+    if (d->hydrostatic_ic) hydrostatic_ic(s, d->min[1]);
     s->timeStep = 0;
     *status = 0;
     return s;
@@ -1302,6 +1397,7 @@ void so_destroy(so_ctx* s) {
     free(s->force);
     free(s->balance);
     free(s->imass);
+    free(s->residualFr);
     free(s->mass);
     free(s->T);
     free(s->T0);

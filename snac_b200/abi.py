@@ -106,6 +106,7 @@ class Desc(C.Structure):
         ("n_velocity_bcs", C.c_int), ("velocity_bcs", C.POINTER(WallBC)),
         ("n_temperature_bcs", C.c_int), ("temperature_bcs", C.POINTER(WallBC)),
         ("init_velocity", _DP), ("init_temperature", _DP), ("init_stress", _DP),
+        ("winkler", C.c_int), ("traction_bc", C.c_int),
     ]
 
 
@@ -195,6 +196,8 @@ class SnacConfig:
     temperature: bool = False             # SnacTemperature loaded
     computeThermalStress: bool = False
     hydrostatic_ic: bool = False          # SnacHydroStaticIC loaded
+    winkler: bool = False                 # SnacWinklerForce loaded (bottom support)
+    traction_bc: bool = False             # SnacTractionBC loaded (right-wall stress)
     materials: List[Dict[str, Any]] = field(default_factory=list)
     element_material: Optional[np.ndarray] = None
     element_cohesion_scale: Optional[np.ndarray] = None
@@ -234,6 +237,8 @@ class SnacConfig:
         d.temperature = int(bool(self.temperature))
         d.compute_thermal_stress = int(bool(self.computeThermalStress))
         d.hydrostatic_ic = int(bool(self.hydrostatic_ic))
+        d.winkler = int(bool(self.winkler))
+        d.traction_bc = int(bool(self.traction_bc))
         if self.temperature_sweep is not None:
             d.temperature_sweep_ic = 1
             d.top_temp, d.bottom_temp = (float(x) for x in self.temperature_sweep)

@@ -87,6 +87,7 @@ struct snac_gpu {
     DevScalars* sc = nullptr;
     double* stage = nullptr;  // host-transfer staging, 3 doubles per node (first upload/download)
     double* escal = nullptr;  // [ne][4] element scalars for the dump files (allocated by snac_gpu_output_open)
+    double* residual_fr = nullptr;  // [nn] Winkler residual force
     OutputState* out = nullptr;
     // host mirror of the step bookkeeping
     int parity = 0;
@@ -221,6 +222,7 @@ Fields fields_at(const snac_gpu* h, int parity) {
     F.mat = h->mat;
     F.mats = h->mats;
     F.escal = h->escal;
+    F.residual_fr = h->residual_fr;
     F.coh_scale = h->coh_scale;
     F.fric_scale = h->fric_scale;
     F.visc_scale = h->visc_scale;
@@ -492,7 +494,9 @@ int node_out(snac_gpu* h, const double4* src, double* dst, int what) {
 // hydroStaticIC/VariableConditions.c:43-152 on one rank: lithostatic
 // pressure integrated down each element column; densities are the phase
 // densities (tet densities are still zero at this point of the reference's IC).
-void hydrostatic_ic(const snac_gpu_desc* d, const std::vector<double>& coord, std::vector<double>& stress) {
+// returns pisos, the bottom pressure of column (0, 0) (:133-140)
+double hydrostatic_ic(const snac_gpu_desc* d, const std::vector<double>& coord, std::vector<double>& stress) {
+    double pisos = 0.0;
     int nx = d->nx, ny = d->ny, nz = d->nz, nnx = nx + 1, nny = ny + 1;
     auto y_of = [&](long e, int corner) {
         static const int off[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
@@ -522,8 +526,10 @@ void hydrostatic_ic(const snac_gpu_desc* d, const std::vector<double>& coord, st
                 for (int t = 0; t < NT; t++)
                     for (int c = 0; c < 3; c++) stress[((size_t)e * NT + t) * 6 + c] = P;
                 rogh += dP;
+                if (elJ == 0 && elI == 0 && elK == 0) pisos = rogh + 0.0;
             }
         }
+    return pisos;
 }
 
 }  // namespace
@@ -603,6 +609,10 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     c.gravity = d->gravity;
     c.demf = d->demf;
     c.strain_inert = d->strain_inert;
+    c.winkler = d->winkler ? 1 : 0;
+    c.traction = d->traction_bc ? 1 : 0;
+    c.pisos = 0.0;
+    c.rzbo = 0.0;
     if (shared) {
         h->stream = shared;
         h->own_stream = false;
@@ -626,6 +636,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
         if ((rc = dalloc(h, &h->vol, nq * 2))) return rc;
     if (h->has_density)
         if ((rc = dalloc(h, &h->density, nq))) return rc;
+    if (d->winkler)
+        if ((rc = dalloc(h, &h->residual_fr, nn))) return rc;
     if (d->temperature) {
         if ((rc = dalloc(h, &h->hflux, nq * HF_STRIDE))) return rc;
         if (h->has_density && (rc = dalloc(h, &h->tpre, nn))) return rc;
@@ -671,7 +683,10 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
         if (d->temperature && idx[3] != 255) temp[n] = d->temperature_bcs[idx[3]].value[0];
     }
     if (d->init_stress) std::copy(d->init_stress, d->init_stress + nq * 6, stress.begin());
-    if (d->hydrostatic_ic) hydrostatic_ic(d, coord, stress);
+    if (d->hydrostatic_ic) {
+        h->cfg.pisos = hydrostatic_ic(d, coord, stress);
+        h->cfg.rzbo = d->min[1];  // element->rzbo = geometry->min[1]
+    }
 
     std::vector<double4> pos4(nn), vel4(nn);
     for (long long n = 0; n < nn; n++) {
@@ -764,7 +779,7 @@ void snac_gpu_destroy(snac_gpu* h) {
             if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
-                    h->visc_scale, h->sc, h->stage, h->escal};
+                    h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
@@ -1473,8 +1488,9 @@ int adjoint_supported(snac_gpu* h) {
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and visco-plastic hooks are differentiated");
     if (h->cfg.dt_type != SNAC_DT_CONSTANT)
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: dtType must be constant (dt may not depend on the state)");
-    if (h->has_density || h->cfg.thermal_stress)
-        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: density coupling and thermal stress are not differentiated");
+    if (h->has_density || h->cfg.thermal_stress || h->cfg.winkler || h->cfg.traction)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1,
+                       "adjoint: density coupling, thermal stress and the force-BC plugins are not differentiated");
     if (h->temperature) {
         std::vector<DevMaterial> dm(MAX_PHASES);
         CK(cudaMemcpy(dm.data(), h->mats, MAX_PHASES * sizeof(DevMaterial), cudaMemcpyDeviceToHost));

@@ -49,6 +49,7 @@ struct Fields {
     const double* tbc_val;   // [n_tc]
     const unsigned char* mat;        // [ne] phase, NULL = 0
     const DevMaterial* mats;         // phase table of this model
+    double* residual_fr;             // [nn] Winkler residual force of step 1 (winkler/Force.c:154-161)
     double* escal;                   // [ne][4] element strain rate, stress, hydroPressure, aps
                                      // (written on steps with sc->want_scalars; NULL = never)
     const double* coh_scale;         // [ne] or NULL
@@ -61,6 +62,9 @@ struct Config {
     int dt_type, constitutive, temperature, thermal_stress, has_density, time_step_zero;
     double gravity, demf;
     double strain_inert;
+    int winkler;          // SnacWinklerForce on Snac_EP_Force
+    int traction;         // SnacTractionBC on Snac_EP_Force (after Winkler)
+    double pisos, rzbo;   // its isostatic pressure and reference bottom depth
 };
 
 #ifndef SNAC_ELEM_MINB
@@ -631,6 +635,85 @@ __global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
 // are read from pos and written to pos_next, so every force sees the old
 // geometry, as in the reference where all forces are summed before any node moves.
 // ======================================================================================
+// SnacWinklerForce (Snac/plugins/winkler/Force.c:56-168), appended to the
+// force of a bottom node (j == 0): for each incident element, the isostatic
+// pressure corrected by the element's bottom height acts on its bottom face
+// (tets 1, 2, 6, 8, faces 0, 1, 2, 2); at step 1 the node's total y force is
+// kept as a residual and subtracted from then on.
+__device__ __noinline__ void winkler_force(const Mesh& m, const Fields& F, const Config& cfg, long long n, int i,
+                                           int k, double& fx, double& fy, double& fz) {
+    const double factor4 = 1.0f / 4.0f;
+    const double y_node = F.pos[n].y;
+    const double nodeT = 0.0;  // the temperature lookup is compiled out in the reference (#if 0)
+    for (int ne = 0; ne < 8; ne++) {
+        const int ei = i - 1 + (ne & 1), ej = -1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
+        if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
+        const long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
+        const DevMaterial& M = F.mats[phase_of(F, e)];
+        V3 corner[8];
+#pragma unroll
+        for (int cc = 0; cc < 8; cc++) {
+            double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
+            corner[cc] = {p.x, p.y, p.z};
+        }
+        const double phsDensity = M.density, drosub = 0.0f;
+        const double p_est = cfg.pisos + 0.5f * (phsDensity + drosub) * cfg.gravity * (y_node - cfg.rzbo);
+        const double rosubg = cfg.gravity * (phsDensity + drosub) * (1.0 - M.alpha * (nodeT - M.reftemp) + M.beta * p_est);
+        const double dhE = factor4 * (corner[0].y + corner[1].y + corner[4].y + corner[5].y);
+        const int ft[4][2] = {{1, 0}, {2, 1}, {6, 2}, {8, 2}};
+        double area = 0.0f, A[4];
+        V3 nr[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int t = ft[q][0], f = ft[q][1];
+            tet_face(corner[tet_node(t, face_node(f, 0))], corner[tet_node(t, face_node(f, 1))],
+                     corner[tet_node(t, face_node(f, 2))], A[q], nr[q]);
+            area += A[q];
+        }
+        const double nx_ = factor4 * (nr[0].x + nr[1].x + nr[2].x + nr[3].x);
+        const double ny_ = -1.0f * factor4 * (nr[0].y + nr[1].y + nr[2].y + nr[3].y);
+        const double nz_ = factor4 * (nr[0].z + nr[1].z + nr[2].z + nr[3].z);
+        area *= 0.5f;
+        const double press_norm = cfg.pisos + rosubg * (cfg.rzbo - dhE);
+        fx += factor4 * (press_norm * area * nx_);
+        fy += factor4 * (press_norm * area * ny_);
+        fz += factor4 * (press_norm * area * nz_);
+    }
+    if (F.sc->time_step == 1) {  // restartTimestep == 0
+        const double Fy = fy;
+        if (Fy != 0.0) F.residual_fr[n] = Fy;
+    }
+    fy -= F.residual_fr[n];
+}
+
+// SnacTractionBC's active branch (Snac/plugins/tractionBC/Force.c:43-268):
+// on a right-wall node (i == nx), each incident element's right face (the
+// triangles (1,2,6) and (1,6,5)) carries the fixed stress sxx = 1e8 Pa.
+__device__ __noinline__ void traction_force(const Mesh& m, const Fields& F, int j, int k, double& fx, double& fy,
+                                            double& fz) {
+    const double factor4 = 1.0f / 4.0f;
+    const double s00 = 1.0e+08, s01 = 0.0, s02 = 0.0, s10 = 0.0, s11 = 0.0, s12 = 0.0, s20 = 0.0, s21 = 0.0, s22 = 0.0;
+    const int i = m.nnx - 1;
+    for (int ne = 0; ne < 8; ne++) {
+        const int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
+        if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
+        auto P = [&](int c) {
+            const double4 p = F.pos[corner_node(m, ei, ej, ek, c)];
+            return V3{p.x, p.y, p.z};
+        };
+        const V3 c1 = P(1), c2 = P(2), c5 = P(5), c6 = P(6);
+        double a1, a2;
+        V3 n1, n2;
+        tet_face(c1, c2, c6, a1, n1);
+        tet_face(c1, c6, c5, a2, n2);
+        const double area = a1 + a2;
+        const double nx_ = 0.5f * (n1.x + n2.x), ny_ = 0.5f * (n1.y + n2.y), nz_ = 0.5f * (n1.z + n2.z);
+        fx += factor4 * area * (s00 * nx_ + s01 * ny_ + s02 * nz_);
+        fy += factor4 * area * (s10 * nx_ + s11 * ny_ + s12 * nz_);
+        fz += factor4 * area * (s20 * nx_ + s21 * ny_ + s22 * nz_);
+    }
+}
+
 template <int DTTYPE>
 __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     long long n = (long long)lb * blockDim.x + threadIdx.x;
@@ -660,6 +743,8 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 fy -= F.fgrav[q];
             }
         }
+        if (cfg.winkler && cfg.gravity > 0.0 && j == 0) winkler_force(m, F, cfg, n, i, k, fx, fy, fz);
+        if (cfg.traction && i == m.nnx - 1) traction_force(m, F, j, k, fx, fy, fz);
         // FLAC local damping with the pre-update velocity, then v and x
         double4 w = F.vel[n];
         const double demf = cfg.demf;

@@ -47,6 +47,23 @@ def lithostatic_small(nx=8, ny=4, nz=8):
     return W.c2_plastic(nx, ny, nz)
 
 
+def winkler_small(nx=8, ny=4, nz=8):
+    """The lithostatic plastic case with the SnacWinklerForce plugin holding the
+    bottom up instead of a roller: no vy condition on the bottom wall."""
+    cfg = W.c2_plastic(nx, ny, nz)
+    cfg.winkler = True
+    cfg.velocityBCs = [bc for bc in cfg.velocityBCs if bc["wall"] != "bottom"]
+    return cfg
+
+
+def traction_small(nx=8, ny=4, nz=8):
+    """Elastic, the right wall free in x and pushed by the SnacTractionBC stress."""
+    cfg = W.c1_elastic(nx, ny, nz)
+    cfg.traction_bc = True
+    cfg.velocityBCs = [bc for bc in cfg.velocityBCs if bc["wall"] != "right"]
+    return cfg
+
+
 def two_phase_density(nx=6, ny=4, nz=6):
     """Two phases with thermal expansion and compressibility (per-tet density
     path) under gravity, with temperature and thermal stress."""
@@ -98,5 +115,7 @@ CASES = {
     "viscoplastic": (viscoplastic_small, 120),
     "maxwell": (maxwell_small, 60),
     "lithostatic": (lithostatic_small, 60),
+    "winkler": (winkler_small, 60),
+    "traction": (traction_small, 60),
     "density": (two_phase_density, 40),
 }
