@@ -150,6 +150,11 @@ typedef struct snac_gpu_desc {
      * active branch applies the fixed stress sxx = 1e8 Pa on the right wall
      * (i = nx).  Force hooks run in load order: Winkler, then traction. */
     int    traction_bc;
+    /* Surface-topography diffusion of the top nodes (UpdateNode.c:161-857,
+     * cartesian geometry): "topo_kappa" (0 = off; the reference's dictionary
+     * default is 5e-6) and "topoGradCriterion" (default 1e-16). */
+    double topo_kappa;
+    double topo_grad_criterion;
 } snac_gpu_desc;
 
 /* Host-side view of the state for upload / download.  NULL members are

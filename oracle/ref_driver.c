@@ -212,6 +212,16 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
                 m->nodeElementTbl[n][q] = ei + ej * r->nx + ek * r->nx * r->ny;
         }
         m->nodeNeighbourTbl[n] = calloc(6, sizeof(Node_DomainIndex));
+        /* IJK6Topology.c:283-345: +x, +y, +z, -x, -y, -z; off the mesh = invalid (>= node count) */
+        {
+            const int step[6][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {-1, 0, 0}, {0, -1, 0}, {0, 0, -1}};
+            for (int q = 0; q < 6; q++) {
+                int a = i + step[q][0], b = j + step[q][1], cz = k + step[q][2];
+                m->nodeNeighbourTbl[n][q] = (a < 0 || b < 0 || cz < 0 || a >= r->nnx || b >= r->nny || cz >= r->nnz)
+                                                ? (Node_DomainIndex)r->nn
+                                                : (Node_DomainIndex)(a + b * r->nnx + cz * r->nnx * r->nny);
+            }
+        }
         /* coordinates: BlockGeometry.c:326-349 */
         int ijk[3] = {i, j, k}, size[3] = {r->nnx, r->nny, r->nnz};
         for (int q = 0; q < 3; q++) {
@@ -288,8 +298,8 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
     r->winkler = d->winkler;
     r->traction = d->traction_bc;
     c->demf = d->demf;
-    c->topo_kappa = 0.0;
-    c->topoGradCriterion = 1.0e-16;
+    c->topo_kappa = d->topo_kappa;
+    c->topoGradCriterion = d->topo_grad_criterion;
     c->computeThermalStress = d->compute_thermal_stress;
     c->velocityBCs = &r->vbc;
     c->constitutiveK = 0;

@@ -71,6 +71,7 @@ struct so_ctx {
     double currentTime; /* AbstractContext.c:871, 891 */
     int winkler;        /* SnacWinklerForce loaded */
     int traction;       /* SnacTractionBC loaded */
+    double topo_kappa, topoGradCriterion, topoGradMax; /* Context.c:759-764 */
     double pisos, rzbo; /* hydroStaticIC/VariableConditions.c:120, 138 */
     double* residualFr; /* [nn] winkler/Force.c:154-161 */
     int nmat;
@@ -901,6 +902,60 @@ static void winkler_force(so_ctx* s, long n) {
 
 #define getsign(val) ((val) < 0 ? -1.0f : (val) > 0 ? +1.0f : 0.0f)
 
+/* ---- UpdateNode.c:161-857, cartesian: surface-topography diffusion ----------------
+ * Run per node right after its coordinate update, in node order, so a top
+ * node sees its -x and -z neighbours already updated (diffused, edge-copied)
+ * and its +x and +z neighbours not yet moved this step. */
+static int top_interior(const so_ctx* s, long i, long k) { return i > 0 && i < s->nnx - 1 && k > 0 && k < s->nnz - 1; }
+
+/* :161-260 */
+static void get_max_topo_grad(so_ctx* s, long n) {
+    const long i = n % s->nnx, j = (n / s->nnx) % s->nny, k = n / ((long)s->nnx * s->nny);
+    if (s->timeStep <= 1 || j < s->nny - 1 || !top_interior(s, i, k)) return;
+    const double* X0 = s->coord[n];
+    const double* xR = s->coord[n + 1];
+    const double* xF = s->coord[n + (long)s->nnx * s->nny];
+    double dydx = (xR[1] - X0[1]) / (xR[0] - X0[0]);
+    double dydz = (xF[1] - X0[1]) / (xF[2] - X0[2]);
+    double localTopoGrad = sqrt(dydx * dydx + dydz * dydz);
+    s->topoGradMax = (s->topoGradMax > localTopoGrad) ? s->topoGradMax : localTopoGrad;
+}
+
+/* :359-506 and :647-715 (DiffTopo, UpdateInteriorTopo) */
+static void diff_topo(so_ctx* s, long n) {
+    const long i = n % s->nnx, j = (n / s->nnx) % s->nny, k = n / ((long)s->nnx * s->nny);
+    if (s->timeStep <= 1 || j < s->nny - 1 || s->topoGradMax < s->topoGradCriterion) return;
+    if (!top_interior(s, i, k)) return;
+    const long sz = (long)s->nnx * s->nny;
+    double* X0 = s->coord[n];
+    const double *xR = s->coord[n + 1], *xL = s->coord[n - 1], *xF = s->coord[n + sz], *xB = s->coord[n - sz];
+    double dydx1 = (xR[1] - X0[1]) / (xR[0] - X0[0]);
+    double dydx2 = (X0[1] - xL[1]) / (X0[0] - xL[0]);
+    double d2ydx2 = (dydx1 - dydx2) / (0.5f * (xR[0] - xL[0]));
+    double dydz1 = (xF[1] - X0[1]) / (xF[2] - X0[2]);
+    double dydz2 = (X0[1] - xB[1]) / (X0[2] - xB[2]);
+    double d2ydz2 = (dydz1 - dydz2) / (0.5f * (xF[2] - xB[2]));
+    double lapl_topo = d2ydx2 + d2ydz2;
+    double dh = s->topo_kappa * s->dt * lapl_topo;
+    X0[1] += dh;
+}
+
+/* :716-857 (AdjustEdgeTopo) */
+static void adjust_edge_topo(so_ctx* s, long n) {
+    const long i = n % s->nnx, j = (n / s->nnx) % s->nny, k = n / ((long)s->nnx * s->nny);
+    if (s->timeStep <= 1 || j < s->nny - 1 || s->topoGradMax < s->topoGradCriterion) return;
+    const long sz = (long)s->nnx * s->nny;
+    const double *xN1 = NULL, *xN2 = NULL;
+    if (i == 0) xN1 = s->coord[n + 1];
+    else if (i == s->nnx - 1) xN1 = s->coord[n - 1];
+    if (k == 0) xN2 = s->coord[n + sz];
+    else if (k == s->nnz - 1) xN2 = s->coord[n - sz];
+    double* X0 = s->coord[n];
+    if (xN1 && !xN2) X0[1] = xN1[1];
+    else if (!xN1 && xN2) X0[1] = xN2[1];
+    else if (xN1 && xN2) X0[1] = 0.5f * (xN1[1] + xN2[1]);
+}
+
 /* ---- UpdateNode.c:74-158 (PreProcess) then :60-72 ------------------------------ */
 static void node_update(so_ctx* s, long n) {
     double* v = s->vel[n];
@@ -921,6 +976,10 @@ static void node_update(so_ctx* s, long n) {
     c[0] += s->dt * v[0];
     c[1] += s->dt * v[1];
     c[2] += s->dt * v[2];
+    if (s->topo_kappa > 0) get_max_topo_grad(s, n);
+    /* the topography hooks appended after UpdateNodeMomentum, Context.c:578-592 */
+    diff_topo(s, n);
+    adjust_edge_topo(s, n);
 }
 
 /* ---- temperature/HeatFlux.c:60-200 --------------------------------------------- */
@@ -1245,6 +1304,14 @@ so_ctx* so_create(const snac_gpu_desc* d, int* status) {
     s->imass = calloc(s->nn, sizeof(double));
     s->winkler = d->winkler;
     s->traction = d->traction_bc;
+    s->topo_kappa = d->topo_kappa;
+    s->topoGradCriterion = d->topo_grad_criterion;
+    s->topoGradMax = 0.0f;
+    if (s->topo_kappa > 0 && (s->nnx <= 2 || s->nnz <= 2)) {
+        free(s);
+        *status = SNAC_GPU_ENOTSUP; /* the one-element-wide variants are not restated */
+        return NULL;
+    }
     s->residualFr = calloc(s->nn, sizeof(double));
     s->mass = calloc(s->nn, sizeof(double));
     s->T = calloc(s->nn, sizeof(double));

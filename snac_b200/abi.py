@@ -107,6 +107,7 @@ class Desc(C.Structure):
         ("n_temperature_bcs", C.c_int), ("temperature_bcs", C.POINTER(WallBC)),
         ("init_velocity", _DP), ("init_temperature", _DP), ("init_stress", _DP),
         ("winkler", C.c_int), ("traction_bc", C.c_int),
+        ("topo_kappa", C.c_double), ("topo_grad_criterion", C.c_double),
     ]
 
 
@@ -198,6 +199,8 @@ class SnacConfig:
     hydrostatic_ic: bool = False          # SnacHydroStaticIC loaded
     winkler: bool = False                 # SnacWinklerForce loaded (bottom support)
     traction_bc: bool = False             # SnacTractionBC loaded (right-wall stress)
+    topo_kappa: float = 0.0               # surface-topography diffusivity (0 = off)
+    topoGradCriterion: float = 1.0e-16
     materials: List[Dict[str, Any]] = field(default_factory=list)
     element_material: Optional[np.ndarray] = None
     element_cohesion_scale: Optional[np.ndarray] = None
@@ -239,6 +242,8 @@ class SnacConfig:
         d.hydrostatic_ic = int(bool(self.hydrostatic_ic))
         d.winkler = int(bool(self.winkler))
         d.traction_bc = int(bool(self.traction_bc))
+        d.topo_kappa = float(self.topo_kappa)
+        d.topo_grad_criterion = float(self.topoGradCriterion)
         if self.temperature_sweep is not None:
             d.temperature_sweep_ic = 1
             d.top_temp, d.bottom_temp = (float(x) for x in self.temperature_sweep)

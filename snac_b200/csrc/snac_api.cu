@@ -88,6 +88,7 @@ struct snac_gpu {
     double* stage = nullptr;  // host-transfer staging, 3 doubles per node (first upload/download)
     double* escal = nullptr;  // [ne][4] element scalars for the dump files (allocated by snac_gpu_output_open)
     double* residual_fr = nullptr;  // [nn] Winkler residual force
+    double* topo_scratch = nullptr;  // [nnx * nnz] topography-diffusion scratch
     OutputState* out = nullptr;
     // host mirror of the step bookkeeping
     int parity = 0;
@@ -249,6 +250,10 @@ int launch_check_named(snac_gpu* h, const char* name) {
 }
 #define launch_check(h) launch_check_named((h), __func__)
 
+// the topography hooks do something when diffusion is on, or when a
+// non-positive criterion lets the edge copy run with topoGradMax = 0
+bool topo_on(const Config& c) { return c.topo_kappa > 0 || !(c.topo_crit > 0); }
+
 template <int P>
 void launch_stress(snac_gpu* h, const Fields& F, const Config& c) {
     k_calc_stresses<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
@@ -302,7 +307,11 @@ int op_loop_nodes(snac_gpu* h) {
     }
     h->launches++;
     h->parity ^= 1;  // the new coordinates are current from here on
-    return launch_check_named(h, "k_loop_nodes");
+    int rc = launch_check_named(h, "k_loop_nodes");
+    if (rc || !topo_on(h->cfg)) return rc;
+    k_topo<<<1, 1024, 0, h->stream>>>(h->mesh, h->pos[h->parity ^ 1], h->pos[h->parity], h->cfg, h->sc, h->topo_scratch);
+    h->launches++;
+    return launch_check_named(h, "k_topo");
 }
 
 int op_update_elements(snac_gpu* h, bool step_zero, int pending = 0) {
@@ -569,6 +578,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     if ((d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC || d->constitutive == SNAC_RHEOLOGY_MAXWELL) && !d->temperature)
         return SNAC_GPU_EINVAL;  // both hooks read the temperature plugin's node extension
     if (d->dt_type < SNAC_DT_CONSTANT || d->dt_type > SNAC_DT_WAVE) return SNAC_GPU_EINVAL;
+    if ((d->topo_kappa > 0 || !(d->topo_grad_criterion > 0)) && (d->nx < 2 || d->nz < 2))
+        return SNAC_GPU_ENOTSUP;  // diffTopo_alongX / alongZ (one element wide) are not built
     bool per_elem = d->element_cohesion_scale || d->element_friction_scale || d->element_visc_scale;
     if (per_elem && d->constitutive == SNAC_RHEOLOGY_MAXWELL) return SNAC_GPU_ENOTSUP;
     for (int p = 0; p < d->n_materials; p++) {
@@ -611,6 +622,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     c.strain_inert = d->strain_inert;
     c.winkler = d->winkler ? 1 : 0;
     c.traction = d->traction_bc ? 1 : 0;
+    c.topo_kappa = d->topo_kappa;
+    c.topo_crit = d->topo_grad_criterion;
     c.pisos = 0.0;
     c.rzbo = 0.0;
     if (shared) {
@@ -638,6 +651,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
         if ((rc = dalloc(h, &h->density, nq))) return rc;
     if (d->winkler)
         if ((rc = dalloc(h, &h->residual_fr, nn))) return rc;
+    if (topo_on(c))
+        if ((rc = dalloc(h, &h->topo_scratch, (size_t)m.nnx * m.nnz))) return rc;
     if (d->temperature) {
         if ((rc = dalloc(h, &h->hflux, nq * HF_STRIDE))) return rc;
         if (h->has_density && (rc = dalloc(h, &h->tpre, nn))) return rc;
@@ -779,7 +794,7 @@ void snac_gpu_destroy(snac_gpu* h) {
             if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
-                    h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr};
+                    h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr, h->topo_scratch};
     for (void* b : bufs)
         if (b) cudaFree(b);
     if (h->stream && h->own_stream) cudaStreamDestroy(h->stream);
@@ -1256,6 +1271,8 @@ int snac_gpu_batch_create(const snac_gpu_desc* descs, int n_models, snac_gpu_bat
             return bset_err(b, rc, i, "model %d: %s", i, msg[0] ? msg : "invalid descriptor");
         }
         b->any_temp = b->any_temp || b->models[i]->temperature;
+        if (topo_on(b->models[i]->cfg))
+            return bset_err(b, SNAC_GPU_ENOTSUP, i, "model %d: topography diffusion is not batched", i);
     }
     cudaError_t e = cudaMalloc((void**)&b->desc[0], n_models * sizeof(ModelDesc));
     if (e == cudaSuccess) e = cudaMalloc((void**)&b->desc[1], n_models * sizeof(ModelDesc));
@@ -1488,9 +1505,9 @@ int adjoint_supported(snac_gpu* h) {
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and visco-plastic hooks are differentiated");
     if (h->cfg.dt_type != SNAC_DT_CONSTANT)
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: dtType must be constant (dt may not depend on the state)");
-    if (h->has_density || h->cfg.thermal_stress || h->cfg.winkler || h->cfg.traction)
+    if (h->has_density || h->cfg.thermal_stress || h->cfg.winkler || h->cfg.traction || topo_on(h->cfg))
         return set_err(h, SNAC_GPU_ENOTSUP, -1,
-                       "adjoint: density coupling, thermal stress and the force-BC plugins are not differentiated");
+                       "adjoint: density coupling, thermal stress, force-BC plugins and topography diffusion are not differentiated");
     if (h->temperature) {
         std::vector<DevMaterial> dm(MAX_PHASES);
         CK(cudaMemcpy(dm.data(), h->mats, MAX_PHASES * sizeof(DevMaterial), cudaMemcpyDeviceToHost));

@@ -102,6 +102,7 @@ struct DevScalars {
     unsigned long long vmax_bits;    // running max of |v| over velocity-BC nodes
     long long time_step;
     double current_time;             // AbstractContext currentTime: the sum of the steps' dt
+    double topo_grad_max;            // Snac_Context topoGradMax: running max of |grad y| on the top surface
     int pos_parity;                  // which of the two coordinate buffers is current
     int want_scalars;                // the next step stores the element scalars (a dump follows it)
     int status;                      // first error (SNAC_GPU_E*), 0 if none

@@ -20,6 +20,8 @@
 // gives the same bits the reference stored in its element structs.
 #pragma once
 
+#include <math_constants.h>
+
 #include "snac_device.cuh"
 
 namespace snac {
@@ -64,6 +66,7 @@ struct Config {
     double strain_inert;
     int winkler;          // SnacWinklerForce on Snac_EP_Force
     int traction;         // SnacTractionBC on Snac_EP_Force (after Winkler)
+    double topo_kappa, topo_crit;  // surface-topography diffusion
     double pisos, rzbo;   // its isostatic pressure and reference bottom depth
 };
 
@@ -992,6 +995,109 @@ __device__ __forceinline__ void k_vmax_body(const Mesh& m, const Fields& F, int 
 
 __global__ void __launch_bounds__(256) k_vmax(Mesh m, Fields F) {
     k_vmax_body(m, F, blockIdx.x);
+}
+
+// ======================================================================================
+// Surface-topography diffusion (UpdateNode.c:161-857, cartesian), after the node update.
+// The reference runs getMaxTopoGrad, DiffTopo + UpdateInteriorTopo and
+// AdjustEdgeTopo inside its node loop, node after node: a top node sees its
+// -x and -z neighbours already finished (moved, diffused, edge-copied) and
+// its +x and +z neighbours not yet moved this step (their start-of-step
+// coordinates).  That is a wavefront over the top surface's anti-diagonals
+// i + k = d: one block walks the diagonals in order, the nodes of a diagonal
+// in parallel.  topoGradMax is the running max in node order (a prefix max,
+// exact in any association), never reset between steps.
+// old: start-of-step coordinates; cur: after this step's node update (updated in place).
+// tgrad: scratch of (nnx * nnz) doubles.
+// ======================================================================================
+__global__ void __launch_bounds__(1024) k_topo(Mesh m, const double4* __restrict__ old, double4* cur, Config cfg,
+                                               DevScalars* sc, double* tgrad) {
+    __shared__ double chunk_max[1024];
+    if (sc->time_step <= 1) return;
+    const int nnx = m.nnx, nnz = m.nnz, T = blockDim.x, tid = threadIdx.x;
+    const long long top = (long long)(m.nny - 1) * nnx, plane = (long long)nnx * m.nny;
+    const long long N = (long long)nnx * nnz;
+    auto id = [&](int i, int k) { return (long long)i + top + (long long)k * plane; };
+    auto interior = [&](int i, int k) { return i > 0 && i < nnx - 1 && k > 0 && k < nnz - 1; };
+    // getMaxTopoGrad (:161-260), called from UpdateNodeMomentum when topo_kappa > 0
+    for (long long p = tid; p < N; p += T) {
+        const int i = (int)(p % nnx), k = (int)(p / nnx);
+        double g = -CUDART_INF;
+        if (cfg.topo_kappa > 0 && interior(i, k)) {
+            const double4 X0 = cur[id(i, k)], xR = old[id(i + 1, k)], xF = old[id(i, k + 1)];
+            const double dydx = (xR.y - X0.y) / (xR.x - X0.x);
+            const double dydz = (xF.y - X0.y) / (xF.z - X0.z);
+            g = sqrt(dydx * dydx + dydz * dydz);
+        }
+        tgrad[p] = g;
+    }
+    __syncthreads();
+    // running max in node order: each thread a contiguous chunk, then the chunk prefixes
+    const long long C = (N + T - 1) / T, lo = tid * C, hi = lo + C < N ? lo + C : N;
+    double cm = -CUDART_INF;
+    for (long long p = lo; p < hi; p++) cm = cm > tgrad[p] ? cm : tgrad[p];
+    chunk_max[tid] = cm;
+    __syncthreads();
+    if (tid == 0) {
+        double run = sc->topo_grad_max;
+        for (int t = 0; t < T; t++) {
+            const double c = chunk_max[t];
+            chunk_max[t] = run;  // the max before chunk t
+            run = run > c ? run : c;
+        }
+        sc->topo_grad_max = run;
+    }
+    __syncthreads();
+    double run = chunk_max[tid];
+    for (long long p = lo; p < hi; p++) {
+        run = run > tgrad[p] ? run : tgrad[p];
+        tgrad[p] = run;  // topoGradMax as node p's DiffTopo sees it
+    }
+    __syncthreads();
+    const double kdt = cfg.topo_kappa * sc->dt;
+    for (int d = 0; d <= (nnx - 1) + (nnz - 1); d++) {
+        const int i0 = d - (nnz - 1) > 0 ? d - (nnz - 1) : 0, i1 = d < nnx - 1 ? d : nnx - 1;
+        for (int i = i0 + tid; i <= i1; i += T) {
+            const int k = d - i;
+            if (tgrad[i + (long long)k * nnx] < cfg.topo_crit) continue;  // "topoGradMax < topoGradCriterion"
+            double4& X0 = cur[id(i, k)];
+            if (interior(i, k)) {
+                // DiffTopo (:359-506) and UpdateInteriorTopo (:647-715)
+                const double4 xR = old[id(i + 1, k)], xF = old[id(i, k + 1)];
+                const double4 xL = cur[id(i - 1, k)], xB = cur[id(i, k - 1)];
+                const double dydx1 = (xR.y - X0.y) / (xR.x - X0.x);
+                const double dydx2 = (X0.y - xL.y) / (X0.x - xL.x);
+                const double d2ydx2 = (dydx1 - dydx2) / (0.5f * (xR.x - xL.x));
+                const double dydz1 = (xF.y - X0.y) / (xF.z - X0.z);
+                const double dydz2 = (X0.y - xB.y) / (X0.z - xB.z);
+                const double d2ydz2 = (dydz1 - dydz2) / (0.5f * (xF.z - xB.z));
+                const double lapl_topo = d2ydx2 + d2ydz2;
+                X0.y += kdt * lapl_topo;
+            } else {
+                // AdjustEdgeTopo (:716-857): copy the neighbour's height inward
+                bool h1 = false, h2 = false;
+                double y1 = 0.0, y2 = 0.0;
+                if (i == 0) {
+                    h1 = true;
+                    y1 = old[id(1, k)].y;
+                } else if (i == nnx - 1) {
+                    h1 = true;
+                    y1 = cur[id(nnx - 2, k)].y;
+                }
+                if (k == 0) {
+                    h2 = true;
+                    y2 = old[id(i, 1)].y;
+                } else if (k == nnz - 1) {
+                    h2 = true;
+                    y2 = cur[id(i, nnz - 2)].y;
+                }
+                if (h1 && !h2) X0.y = y1;
+                else if (!h1 && h2) X0.y = y2;
+                else if (h1 && h2) X0.y = 0.5f * (y1 + y2);
+            }
+        }
+        __syncthreads();
+    }
 }
 
 // ---- self-test of the straight-line division against the IEEE quotient -------------------

@@ -64,6 +64,13 @@ def traction_small(nx=8, ny=4, nz=8):
     return cfg
 
 
+def topo_small(nx=8, ny=4, nz=8, kappa=0.5):
+    """The lithostatic plastic case with surface-topography diffusion on."""
+    cfg = W.c2_plastic(nx, ny, nz)
+    cfg.topo_kappa = kappa
+    return cfg
+
+
 def two_phase_density(nx=6, ny=4, nz=6):
     """Two phases with thermal expansion and compressibility (per-tet density
     path) under gravity, with temperature and thermal stress."""
@@ -117,5 +124,6 @@ CASES = {
     "lithostatic": (lithostatic_small, 60),
     "winkler": (winkler_small, 60),
     "traction": (traction_small, 60),
+    "topo": (topo_small, 60),
     "density": (two_phase_density, 40),
 }

@@ -49,7 +49,7 @@ def assert_bitwise(g, c):
     assert a.time_step == b.time_step
 
 
-@pytest.mark.parametrize("case", ["elastic", "plastic", "lithostatic", "winkler", "traction"])
+@pytest.mark.parametrize("case", ["elastic", "plastic", "lithostatic", "winkler", "traction", "topo"])
 def test_bitwise_equal_to_oracle(case):
     make, steps = S.CASES[case]
     g, c = run_both(make(), steps, chunks=2)
@@ -152,6 +152,38 @@ def test_upload_download_roundtrip():
     s2 = h.state()
     for f in ("coord", "velocity", "stress", "plastic_strain"):
         assert np.array_equal(getattr(s, f), getattr(s2, f)), f
+
+
+def remesh_on_host(s, cfg):
+    """A stand-in for the host remesher (Snac/plugins/remesher): moves the
+    interior nodes toward their initial positions and zeroes the plastic
+    strain of the bottom elements, as a remesh-and-interpolate would change
+    the state between two steps."""
+    out = type(s)(**{f: getattr(s, f).copy() for f in s.__dataclass_fields__})
+    c = out.coord.reshape(cfg.nz + 1, cfg.ny + 1, cfg.nx + 1, 3)
+    c[1:-1, 1:-1, 1:-1] *= (1.0 - 1e-6)
+    out.plastic_strain.reshape(cfg.nz, cfg.ny, cfg.nx, 10)[:, 0] = 0.0
+    return out
+
+
+def test_remesher_hand_off():
+    """Remesh trigger: state down to the host, host remesh, state back up, then
+    the element update the remesher runs after interpolating
+    (remesher/RemeshElements.c:232-250, every element's
+    Snac_UpdateElementMomentum) and a Sync; the run continues bit for bit with
+    the oracle given the same remeshed state."""
+    cfg = S.plastic_small()
+    g, c = run_both(cfg, 30)
+    fields = ["coord", "velocity", "stress", "plastic_strain"]
+    new = remesh_on_host(g.state(), cfg)
+    assert np.array_equal(g.state().coord, c.state().coord)
+    for m in (g, c):
+        m.set_state(new, fields)
+        m.loop_elements_momentum()
+        m.sync()
+    g.step(30)
+    c.step(30)
+    assert_bitwise(g, c)
 
 
 # ---- failure detection: every fault is made on the host, none on the GPU ----------------
