@@ -352,6 +352,8 @@ typedef struct snac_batch_tuning {
     int node_blocks_per_sm; /* the same for the node launches                                */
     int steps_per_graph;    /* steps captured in one CUDA graph (1..256)                     */
     int order;              /* tile order: 0 = largest model first, 1 = model order          */
+    int split_classes;      /* 1: one element launch per rheology class present (specialised
+                               kernels), 0: one launch with a run-time switch               */
 } snac_batch_tuning;
 
 int  snac_gpu_batch_create(const snac_gpu_desc* descs, int n_models, snac_gpu_batch** out);

@@ -122,7 +122,8 @@ class KernelTime(C.Structure):
 
 class BatchTuning(C.Structure):
     _fields_ = [("node_threads", C.c_int), ("minls_threads", C.c_int), ("elem_blocks_per_sm", C.c_int),
-                ("node_blocks_per_sm", C.c_int), ("steps_per_graph", C.c_int), ("order", C.c_int)]
+                ("node_blocks_per_sm", C.c_int), ("steps_per_graph", C.c_int), ("order", C.c_int),
+                ("split_classes", C.c_int)]
 
     def as_dict(self) -> Dict[str, int]:
         return {k: int(getattr(self, k)) for k, _ in self._fields_}

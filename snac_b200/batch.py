@@ -134,6 +134,7 @@ SEARCH_SPACE: Dict[str, List[int]] = {
     "node_blocks_per_sm": [0, 8, 16],
     "minls_threads": [64, 128, 256],
     "order": [0, 1],
+    "split_classes": [1, 0],
 }
 
 

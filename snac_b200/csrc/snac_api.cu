@@ -996,8 +996,9 @@ struct snac_gpu_batch {
         int n = 0;
     };
     List elem_all, elem_temp, node_all, node_temp, minls_all;
+    List elem_cls[NCLASS];  // element tiles grouped by rheology class (plugin, temperature)
     bool any_temp = false;
-    snac_batch_tuning tune{128, 128, 0, 0, 8, 0};
+    snac_batch_tuning tune{128, 128, 0, 0, 8, 0, 1};
     bool tiles_dirty = true;
     cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [multi-step chunk][start parity]
     int graph_kernels[2] = {0, 0};
@@ -1078,6 +1079,17 @@ int build_tiles(snac_gpu_batch* b) {
     };
     add(b->elem_all, false, 0);
     add(b->elem_temp, true, 0);
+    for (int c = 0; c < NCLASS; c++) {  // the same element tiles, class by class
+        snac_gpu_batch::List& L = b->elem_cls[c];
+        L.off = (long long)t.size();
+        for (int i : order) {
+            const snac_gpu* h = b->models[i];
+            if (plugin_slot(h->constitutive) * 2 + (h->temperature ? 1 : 0) != c) continue;
+            const long long nb = (long long)elem_blocks(h->mesh);
+            for (long long k = 0; k < nb; k++) t.push_back(make_int2(i, (int)k));
+        }
+        L.n = (int)((long long)t.size() - L.off);
+    }
     add(b->node_all, false, 1);
     add(b->node_temp, true, 1);
     add(b->minls_all, false, 2);
@@ -1124,20 +1136,52 @@ int blaunch_nodes(snac_gpu_batch* b, const ModelDesc* D, const snac_gpu_batch::L
     return bcheck_launch(b, "kb_nodes");
 }
 
+template <int OP, int P, int TEMP>
+int blaunch_elem_c(snac_gpu_batch* b, const ModelDesc* D, const snac_gpu_batch::List& L) {
+    if (L.n == 0) return 0;
+    kb_elements_c<OP, P, TEMP><<<tile_grid(b, L.n, b->tune.elem_blocks_per_sm), ELEM_WARPS * 32, 0, b->stream>>>(
+        D, b->tiles + L.off, L.n);
+    return bcheck_launch(b, "kb_elements_c");
+}
+
+// one launch per rheology class present; temp_only skips the classes without temperature
+template <int OP>
+int blaunch_elem_classes(snac_gpu_batch* b, const ModelDesc* D, bool temp_only) {
+    int rc = 0;
+    const auto& C = b->elem_cls;
+    if (!temp_only) {
+        if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_ELASTIC, 0>(b, D, C[0]);
+        if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_PLASTIC, 0>(b, D, C[2]);
+    }
+    if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_ELASTIC, 1>(b, D, C[1]);
+    if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_PLASTIC, 1>(b, D, C[3]);
+    if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_VISCOPLASTIC, 1>(b, D, C[5]);
+    if (!rc) rc = blaunch_elem_c<OP, SNAC_RHEOLOGY_MAXWELL, 1>(b, D, C[7]);
+    return rc;  // classes 4 and 6 (visco-plastic / Maxwell without temperature) cannot be created
+}
+
 // one step of every model, in the order of record_step
 int record_batch_step(snac_gpu_batch* b, bool fused, int parity) {
     const ModelDesc* D = b->desc[parity];
     const unsigned mb = (unsigned)((b->n + 127) / 128);
     int rc;
+    const bool by_class = b->tune.split_classes != 0;
     if (fused) {
-        if ((rc = blaunch_elem<BOP_FUSED>(b, D, b->elem_all))) return rc;
+        if ((rc = by_class ? blaunch_elem_classes<BOP_FUSED>(b, D, false) : blaunch_elem<BOP_FUSED>(b, D, b->elem_all)))
+            return rc;
     } else {
         kb_begin_step<<<mb, 128, 0, b->stream>>>(D, b->n);
         if ((rc = bcheck_launch(b, "kb_begin_step"))) return rc;
-        if ((rc = blaunch_elem<BOP_HEAT_FLUX>(b, D, b->elem_temp))) return rc;
+        if ((rc = by_class ? blaunch_elem_classes<BOP_HEAT_FLUX>(b, D, true)
+                           : blaunch_elem<BOP_HEAT_FLUX>(b, D, b->elem_temp)))
+            return rc;
     }
     if ((rc = blaunch_nodes<BOP_HEAT_NODES>(b, D, b->node_temp, b->tune.node_threads))) return rc;
-    if ((rc = blaunch_elem<BOP_STRESS>(b, D, fused ? b->elem_temp : b->elem_all))) return rc;
+    if (by_class)
+        rc = blaunch_elem_classes<BOP_STRESS>(b, D, fused);
+    else
+        rc = blaunch_elem<BOP_STRESS>(b, D, fused ? b->elem_temp : b->elem_all);
+    if (rc) return rc;
     if ((rc = blaunch_nodes<BOP_LOOP_NODES>(b, D, b->node_all, b->tune.node_threads))) return rc;
     // the node loop wrote the new coordinates into the other buffer
     const ModelDesc* Dn = b->desc[parity ^ 1];
@@ -1352,14 +1396,15 @@ int snac_gpu_batch_set_tuning(snac_gpu_batch* b, const snac_batch_tuning* t) {
     auto threads_ok = [](int x) { return x >= 32 && x <= 256 && x % 32 == 0; };
     if (!threads_ok(t->node_threads) || !threads_ok(t->minls_threads) || t->elem_blocks_per_sm < 0 ||
         t->elem_blocks_per_sm > 32 || t->node_blocks_per_sm < 0 || t->node_blocks_per_sm > 32 ||
-        t->steps_per_graph < 1 || t->steps_per_graph > 256 || (t->order != 0 && t->order != 1))
+        t->steps_per_graph < 1 || t->steps_per_graph > 256 || (t->order != 0 && t->order != 1) ||
+        (t->split_classes != 0 && t->split_classes != 1))
         return bset_err(b, SNAC_GPU_EINVAL, -1, "launch shape out of range");
     const snac_batch_tuning o = b->tune;
     b->tune = *t;
     if (o.node_threads != t->node_threads || o.minls_threads != t->minls_threads || o.order != t->order)
         b->tiles_dirty = true;
     else if (o.elem_blocks_per_sm != t->elem_blocks_per_sm || o.node_blocks_per_sm != t->node_blocks_per_sm ||
-             o.steps_per_graph != t->steps_per_graph)
+             o.steps_per_graph != t->steps_per_graph || o.split_classes != t->split_classes)
         drop_graphs(b);
     return 0;
 }

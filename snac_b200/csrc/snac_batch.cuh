@@ -84,6 +84,40 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
     }
 }
 
+// The same element-tile kernels specialised for one rheology class (plugin,
+// temperature on/off): the tile lists are grouped by class, and each class
+// present gets its own launch, without the run-time switch (fewer registers).
+template <int OP, int P, int TEMP>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
+    kb_elements_c(const ModelDesc* __restrict__ D, const int2* __restrict__ tiles, int ntiles) {
+    __shared__ ModelDesc md;
+    for (int i = blockIdx.x; i < ntiles; i += gridDim.x) {
+        const int2 t = tiles[i];
+        __syncthreads();
+        load_desc(md, D + t.x);
+        __syncthreads();
+        if (OP == BOP_FUSED) {
+            if (TEMP)
+                k_fused_heat_body<P == SNAC_RHEOLOGY_MAXWELL ? SNAC_RHEOLOGY_MAXWELL : SNAC_RHEOLOGY_ELASTIC>(md.m, md.F,
+                                                                                                          md.cfg, t.y);
+            else
+                k_fused_step_body<P>(md.m, md.F, md.cfg, t.y);
+        } else if (OP == BOP_STRESS) {
+            k_calc_stresses_body<P>(md.m, md.F, md.cfg, t.y);
+        } else {
+            k_heat_flux_body(md.m, md.F, md.cfg, t.y);
+        }
+    }
+}
+
+// rheology classes of a batch: index = plugin slot * 2 + temperature
+constexpr int NCLASS = 8;
+__host__ __device__ constexpr int plugin_slot(int constitutive) {
+    return constitutive == SNAC_RHEOLOGY_ELASTIC ? 0 : constitutive == SNAC_RHEOLOGY_PLASTIC ? 1
+           : constitutive == SNAC_RHEOLOGY_VISCOPLASTIC                                  ? 2
+                                                                                          : 3;
+}
+
 // Node-tile kernels (one thread per node, or per element for the minimum
 // length scale); the block size is the tile size the tile list was built for.
 template <int OP>

@@ -37,7 +37,7 @@ def test_signature_depends_on_shapes_only():
 def test_search_finds_the_separable_minimum():
     # a cost that is separable in the knobs: coordinate descent must find its minimum
     target = {"steps_per_graph": 16, "elem_blocks_per_sm": 8, "node_threads": 256,
-              "node_blocks_per_sm": 0, "minls_threads": 64, "order": 1}
+              "node_blocks_per_sm": 0, "minls_threads": 64, "order": 1, "split_classes": 0}
     calls = []
 
     def measure(t):
@@ -45,7 +45,7 @@ def test_search_finds_the_separable_minimum():
         return 1.0 + sum(abs(SEARCH_SPACE[k].index(t[k]) - SEARCH_SPACE[k].index(target[k])) for k in target)
 
     start = {"steps_per_graph": 1, "elem_blocks_per_sm": 0, "node_threads": 128,
-             "node_blocks_per_sm": 8, "minls_threads": 128, "order": 0}
+             "node_blocks_per_sm": 8, "minls_threads": 128, "order": 0, "split_classes": 1}
     best, ms, tried = search(measure, start)
     assert best == target and ms == 1.0
     assert len(tried) == len(calls) == 1 + sum(len(v) - 1 for v in SEARCH_SPACE.values())
@@ -53,5 +53,5 @@ def test_search_finds_the_separable_minimum():
 
 def test_tuning_struct_round_trip():
     d = {"node_threads": 64, "minls_threads": 256, "elem_blocks_per_sm": 4, "node_blocks_per_sm": 0,
-         "steps_per_graph": 8, "order": 1}
+         "steps_per_graph": 8, "order": 1, "split_classes": 0}
     assert BatchTuning.from_dict(d).as_dict() == d

@@ -74,6 +74,8 @@ def test_batch_against_oracle():
     {"elem_blocks_per_sm": 2, "node_blocks_per_sm": 1},
     {"steps_per_graph": 3, "order": 1},
     {"steps_per_graph": 1, "node_threads": 256, "elem_blocks_per_sm": 16},
+    {"split_classes": 0, "steps_per_graph": 2},
+    {"split_classes": 1, "elem_blocks_per_sm": 3},
 ])
 def test_launch_shape_does_not_change_results(tuning):
     cfgs = small_ensemble(5, seed=3)
