@@ -288,8 +288,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
         const double refvisc = M.refvisc * vsc;
         // unclipped viscosity without the element's scale: d eta / d scale
-        R.eta_base = M.refvisc * pow(dvz(J, M.refsrate, M.vp_zrs), M.vp_expo) *
-                     exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+        R.eta_base = arrhenius_base(M, M.refvisc, J, avgTemp);
         double eta = arrhenius_viscosity(M, refvisc, J, avgTemp);
         R.eta_free = (eta > M.vis_min && eta < M.vis_max);
         R.eta = eta;

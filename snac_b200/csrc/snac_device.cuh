@@ -495,10 +495,15 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
 
 // Power-law / Arrhenius viscosity, viscoplastic/Constitutive.c:186-210 and
 // maxwell/Constitutive.c:122-142, clipped to [vis_min, vis_max].
+// The unclipped viscosity: refvisc (srJ2/refsrate)^expo exp(H/R (1/T - 1/Tref)).
+__device__ __forceinline__ double arrhenius_base(const DevMaterial& M, double refvisc, double srJ2, double avgTemp) {
+    return refvisc * pow(dvz(srJ2, M.refsrate, M.vp_zrs), M.vp_expo) *
+           exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+}
+
 __device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, double refvisc, double srJ2,
                                                       double avgTemp) {
-    double eta = refvisc * pow(dvz(srJ2, M.refsrate, M.vp_zrs), M.vp_expo) *
-                 exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+    double eta = arrhenius_base(M, refvisc, srJ2, avgTemp);
     if (eta < M.vis_min) eta = M.vis_min;
     if (eta > M.vis_max) eta = M.vis_max;
     return eta;

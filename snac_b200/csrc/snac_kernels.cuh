@@ -805,26 +805,30 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
         tsr = -1.0f * M.alpha * bulkm * (temp - temp0);
     }
     // flux BC on the x and z walls: remove the wall-normal part of grad T
+    const bool on_wall = s.active && (s.i == 0 || s.i == m.nx - 1 || s.k == 0 || s.k == m.nz - 1);
     double nrm[4][3];
-    // (tet, face) pairs averaged for each wall, VariableConditions.c:311-367
-    const int W[4][4][2] = {{{0, 2}, {1, 2}, {5, 0}, {6, 0}},
-                            {{2, 0}, {3, 0}, {7, 0}, {8, 0}},
-                            {{0, 1}, {2, 2}, {6, 1}, {7, 1}},
-                            {{1, 1}, {3, 2}, {5, 1}, {8, 1}}};
+    // (tet, face) pairs averaged for each wall, VariableConditions.c:311-367;
+    // the shuffles run only in warps that hold a wall element (warp-uniform)
+    if (__any_sync(FULL, on_wall)) {
+        const int W[4][4][2] = {{{0, 2}, {1, 2}, {5, 0}, {6, 0}},
+                                {{2, 0}, {3, 0}, {7, 0}, {8, 0}},
+                                {{0, 1}, {2, 2}, {6, 1}, {7, 1}},
+                                {{1, 1}, {3, 2}, {5, 1}, {8, 1}}};
 #pragma unroll
-    for (int w = 0; w < 4; w++)
+        for (int w = 0; w < 4; w++)
 #pragma unroll
-        for (int d = 0; d < 3; d++) {
-            double a[4];
+            for (int d = 0; d < 3; d++) {
+                double a[4];
 #pragma unroll
-            for (int r = 0; r < 4; r++) {
-                const int f = W[w][r][1];
-                double val = f == 0 ? comp(g.n[0], d) : f == 1 ? comp(g.n[1], d) : f == 2 ? comp(g.n[2], d) : comp(g.n[3], d);
-                a[r] = __shfl_sync(FULL, val, s.base + W[w][r][0]);
+                for (int r = 0; r < 4; r++) {
+                    const int f = W[w][r][1];
+                    double val = f == 0 ? comp(g.n[0], d) : f == 1 ? comp(g.n[1], d) : f == 2 ? comp(g.n[2], d) : comp(g.n[3], d);
+                    a[r] = __shfl_sync(FULL, val, s.base + W[w][r][0]);
+                }
+                nrm[w][d] = 0.25f * (a[0] + a[1] + a[2] + a[3]);
             }
-            nrm[w][d] = 0.25f * (a[0] + a[1] + a[2] + a[3]);
-        }
-    if (s.active && (s.i == 0 || s.i == m.nx - 1 || s.k == 0 || s.k == m.nz - 1)) {
+    }
+    if (on_wall) {
         double normal[3];
         if (s.i == 0)
             for (int d = 0; d < 3; d++) normal[d] = nrm[0][d];
