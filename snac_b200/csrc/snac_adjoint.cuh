@@ -726,7 +726,8 @@ __global__ void __launch_bounds__(128) k_adj_nodes(Mesh m, Fields F, AdjState cu
     if (n >= m.nn) return;
     double4 xb = B.xbar[n], vb = B.vbar[n];
     if (gather) {
-        int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
+        int i, j, k;
+        split3(n, m.nnx, m.nny, i, j, k);
         for (int ne = 0; ne < 8; ne++) {
             int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
             if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
@@ -782,10 +783,10 @@ __global__ void k_adj_loss(Mesh m, const double4* pos, const double4* vel, const
                            double wv, double wh, double* terms, AdjBufs B) {
     long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= m.nn) return;
-    int j = (int)((n / m.nnx) % m.nny);
+    int i, j, k;
+    split3(n, m.nnx, m.nny, i, j, k);
     double4 xb = make_double4(0, 0, 0, 0), vb = make_double4(0, 0, 0, 0);
     if (j == m.nny - 1) {
-        int i = (int)(n % m.nnx), k = (int)(n / ((long long)m.nnx * m.nny));
         long long t = (long long)i + (long long)k * m.nnx;
         const double dv_ = vel[n].y - tv[t], dy = pos[n].y - ty[t];
         terms[t] = wv * dv_ * dv_ + wh * dy * dy;

@@ -85,10 +85,24 @@ __device__ __forceinline__ long long node_id(const Mesh& m, int i, int j, int k)
     return (long long)i + (long long)j * m.nnx + (long long)k * m.nnx * m.nny;
 }
 
+// x = i + j a + k a b.  Index arithmetic in 32 bits whenever the index fits:
+// a 64-bit integer division is a long software routine on the GPU, a 32-bit
+// one a few instructions (the branch is uniform across a launch).
+__device__ __forceinline__ void split3(long long x, int a, int b, int& i, int& j, int& k) {
+    if (x >= 0 && x < 0x7fffffffLL) {
+        const unsigned u = (unsigned)x, q = u / (unsigned)a, r = q / (unsigned)b;
+        i = (int)(u - q * (unsigned)a);
+        j = (int)(q - r * (unsigned)b);
+        k = (int)r;
+    } else {
+        i = (int)(x % a);
+        j = (int)((x / a) % b);
+        k = (int)(x / ((long long)a * b));
+    }
+}
+
 __device__ __forceinline__ void elem_ijk(const Mesh& m, long long e, int& i, int& j, int& k) {
-    i = (int)(e % m.nx);
-    j = (int)((e / m.nx) % m.ny);
-    k = (int)(e / ((long long)m.nx * m.ny));
+    split3(e, m.nx, m.ny, i, j, k);
 }
 
 __device__ __forceinline__ long long corner_node(const Mesh& m, int i, int j, int k, int corner) {
@@ -724,7 +738,8 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
     double vcand = 0.0;
     if (active) {
         const double dt = F.sc->dt;
-        int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
+        int i, j, k;
+        split3(n, m.nnx, m.nny, i, j, k);
         double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
         // Snac_Force: the 8 incident hexes in HexaEL.c:529-573 order, 5 tets each
         // (NodeToTetra/NodeToSurface); absent hexes are skipped (Force.c:92)
@@ -918,7 +933,8 @@ __device__ __forceinline__ void k_heat_nodes_body(const Mesh& m, const Fields& F
     long long n = (long long)lb * blockDim.x + threadIdx.x;
     if (n >= m.nn) return;
     const double dt = F.sc->dt;
-    int i = (int)(n % m.nnx), j = (int)((n / m.nnx) % m.nny), k = (int)(n / ((long long)m.nnx * m.nny));
+    int i, j, k;
+    split3(n, m.nnx, m.nny, i, j, k);
     double energy = 0.0f, lumpVolume = 0.0f;
     // the volumetric source of Snac_Heat is called with sourceterm = 0
     // (Heat.c:59), which adds +0 to the energy
