@@ -606,6 +606,7 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     m.nnz = d->nz + 1;
     m.ne = (long long)d->nx * d->ny * d->nz;
     m.nn = (long long)m.nnx * m.nny * m.nnz;
+    m.ner = (m.ne + 3) & ~3LL;
     h->constitutive = d->constitutive;
     h->temperature = d->temperature;
     h->n_phases = d->n_materials;
@@ -638,8 +639,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     if ((rc = dalloc(h, &h->pos[0], nn)) || (rc = dalloc(h, &h->pos[1], nn)) || (rc = dalloc(h, &h->vel, nn)) ||
         (rc = dalloc(h, &h->force, nn)) || (rc = dalloc(h, &h->stress, nq * 6)) || (rc = dalloc(h, &h->bc, nn)) ||
         (rc = dalloc(h, &h->sc, 1)) || (rc = dalloc(h, &h->mats, MAX_PHASES)) ||
-        (rc = dalloc(h, &h->fterm, nq * 12)) || (rc = dalloc(h, &h->fgrav, nq)) ||
-        (rc = dalloc(h, &h->fmass, d->dt_type == SNAC_DT_CONSTANT ? nq * 4 : nq)))
+        (rc = dalloc(h, &h->fterm, m.ner * NT * 12)) || (rc = dalloc(h, &h->fgrav, m.ner * NT)) ||
+        (rc = dalloc(h, &h->fmass, m.ner * NT * (d->dt_type == SNAC_DT_CONSTANT ? 4 : 1))))
         return rc;
     if (d->constitutive == SNAC_RHEOLOGY_PLASTIC || d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC)
         if ((rc = dalloc(h, &h->eps_p, nq))) return rc;
@@ -654,7 +655,7 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     if (topo_on(c))
         if ((rc = dalloc(h, &h->topo_scratch, (size_t)m.nnx * m.nnz))) return rc;
     if (d->temperature) {
-        if ((rc = dalloc(h, &h->hflux, nq * HF_STRIDE))) return rc;
+        if ((rc = dalloc(h, &h->hflux, m.ner * NT * HF_STRIDE))) return rc;
         if (h->has_density && (rc = dalloc(h, &h->tpre, nn))) return rc;
     }
 

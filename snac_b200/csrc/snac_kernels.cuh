@@ -29,7 +29,14 @@ namespace snac {
 struct Mesh {
     int nx, ny, nz, nnx, nny, nnz;
     long long ne, nn;
+    long long ner;  // row length of the tet-major per-tet arrays: ne rounded up to 4 (32-byte rows)
 };
+
+// Per-tet force and energy terms are stored tet-major, one row per
+// (tet-in-hex, face, component) holding every element: entry (e, t, ...) sits
+// at row(t, ...) * ner + e.  The element kernels write a row segment per
+// group of elements, and the node gathers, which read a fixed (t, face) for
+// consecutive elements along x, load consecutive addresses.
 
 struct Fields {
     const double4* pos;      // current coordinates (x, y, z) and temperature (w)
@@ -41,11 +48,11 @@ struct Fields {
     double* visc;            // [ne*10]  viscosity (visco-plastic, Maxwell)
     double* density;         // [ne*10]  only when some phase has alpha or beta != 0
     double* vol;             // [ne*10][2] volume, old volume (Maxwell)
-    double* hflux;           // [ne*10][6] face energy terms (q.n A/6), Cp rho V/8, thermal stress
+    double* hflux;           // rows (t, 0..5): face energy terms (q.n A/6), Cp rho V/8, thermal stress
     double* tpre;            // [nn] temperature before the BCs (temperature + density)
-    double* fterm;           // [ne*10][4 faces][3] stress.n.A/6 of each face (Force.c:154-165)
-    double* fgrav;           // [ne*10] g rho V / 8 (Force.c:173)
-    double* fmass;           // [ne*10][4] (constant dt) or [ne*10] inertial-mass term (Force.c:107-140)
+    double* fterm;           // rows (t, face, xyz): stress.n.A/6 of each face (Force.c:154-165)
+    double* fgrav;           // rows (t): g rho V / 8 (Force.c:173)
+    double* fmass;           // rows (t, face) (constant dt) or (t): inertial-mass term (Force.c:107-140)
     const uchar4* bc;        // per node: velocity-VC index of x, y, z and temperature-VC index (255 = free)
     const double* vbc_val;   // [n_vc][3]
     const double* tbc_val;   // [n_tc]
@@ -269,7 +276,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             // visco-plastic Maxwell step, viscoplastic/Constitutive.c:158-257
             const double bulkm = M.lambda + dv3(2.0f * M.mu);
             if (cfg.thermal_stress) {
-                double ts = s.active ? F.hflux[s.q * HF_STRIDE + 5] : 0.0;
+                double ts = s.active ? F.hflux[(long long)(s.t * HF_STRIDE + 5) * m.ner + s.e] : 0.0;
                 st[0] += ts;
                 st[1] += ts;
                 st[2] += ts;
@@ -439,21 +446,23 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     // the reference's node-centred order, so the sums keep their bits.
     if (s.active) {
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
+        const long long R = m.ner;
+        double* o = F.fterm + (long long)(s.t * 12) * R + s.e;
 #pragma unroll
         for (int f = 0; f < 4; f++) {
             const V3& nr = g.n[f];
             const double A = g.A[f];
-            double* o = F.fterm + s.q * 12 + f * 3;
-            o[0] = dv6((st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A);
-            o[1] = dv6((st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A);
-            o[2] = dv6((st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A);
+            o[(f * 3 + 0) * R] = dv6((st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A);
+            o[(f * 3 + 1) * R] = dv6((st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A);
+            o[(f * 3 + 2) * R] = dv6((st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A);
         }
-        F.fgrav[s.q] = cfg.gravity * rho * g.V / 8.0f;
+        const long long qt = (long long)s.t * R + s.e;  // row t
+        F.fgrav[qt] = cfg.gravity * rho * g.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
             const double sos = F.sc->speed_of_sound;
             const double inertialDensity = dv(M.lambda + 2.0f * M.mu, sos * sos);
-            F.fmass[s.q] = factor4 * inertialDensity * g.V;
+            F.fmass[qt] = factor4 * inertialDensity * g.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
             const double nineV = 9.0f * g.V, z9V = recip(nineV);
@@ -468,10 +477,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
                 if (temp > area_sum) area_sum = temp;
                 temp = (nr.z * A) * (nr.z * A);
                 if (temp > area_sum) area_sum = temp;
-                F.fmass[s.q * 4 + f] = dvz(alpha1 * area_sum, nineV, z9V) * (dt * dt);
+                F.fmass[(long long)(s.t * 4 + f) * R + s.e] = dvz(alpha1 * area_sum, nineV, z9V) * (dt * dt);
             }
         } else {
-            F.fmass[s.q] = factor4 * rho * g.V;
+            F.fmass[qt] = factor4 * rho * g.V;
         }
     }
 
@@ -752,13 +761,13 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
             for (int idx = 0; idx < 5; idx++) {
                 const int t = node_tet(ne, idx);
                 const int f = node_face(ne, idx);
-                const long long q = e * NT + t;
-                imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[q * 4 + f] : F.fmass[q];
-                const double* o = F.fterm + q * 12 + f * 3;
+                const long long R = m.ner;
+                imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[(t * 4 + f) * R + e] : F.fmass[t * R + e];
+                const double* o = F.fterm + (t * 12 + f * 3) * R + e;
                 fx += o[0];
-                fy += o[1];
-                fz += o[2];
-                fy -= F.fgrav[q];
+                fy += o[R];
+                fz += o[2 * R];
+                fy -= F.fgrav[t * R + e];
             }
         }
         if (cfg.winkler && cfg.gravity > 0.0 && j == 0) winkler_force(m, F, cfg, n, i, k, fx, fy, fz);
@@ -866,14 +875,15 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
     // gather: (q . n) A / 6 of each face, the lumped heat capacity
     // Cp rho V / 8, and the thermal stress for the visco-plastic hook.
     if (s.active) {
-        double* h = F.hflux + s.q * HF_STRIDE;
+        const long long R = m.ner;
+        double* h = F.hflux + (long long)(s.t * HF_STRIDE) * R + s.e;
 #pragma unroll
-        for (int f = 0; f < 4; f++) h[f] = dv6((q[0] * g.n[f].x + q[1] * g.n[f].y + q[2] * g.n[f].z) * g.A[f]);
+        for (int f = 0; f < 4; f++) h[f * R] = dv6((q[0] * g.n[f].x + q[1] * g.n[f].y + q[2] * g.n[f].z) * g.A[f]);
         // tetra density is set from TimeStepZero on, so the reference's
         // "density == 0" fallback (Heat.c:120-125) is never taken
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
-        h[4] = M.heat_capacity * ((rho)*g.V) / 8.0f;
-        if (cfg.thermal_stress) h[5] = tsr;
+        h[4 * R] = M.heat_capacity * ((rho)*g.V) / 8.0f;
+        if (cfg.thermal_stress) h[5 * R] = tsr;
         if (s.t == 0) {
             // Heat.c:127-135, once per element
             double dt_thermal_to_mech = sqrt((M.lambda + 2.0f * M.mu) / M.density) * F.sc->min_length_scale /
@@ -946,10 +956,10 @@ __device__ __forceinline__ void k_heat_nodes_body(const Mesh& m, const Fields& F
         long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
 #pragma unroll
         for (int idx = 0; idx < 5; idx++) {
-            const long long q = e * NT + node_tet(ne, idx);
-            const double* h = F.hflux + q * HF_STRIDE;
-            energy += h[node_face(ne, idx)];
-            lumpVolume += h[4];
+            const long long R = m.ner;
+            const double* h = F.hflux + (node_tet(ne, idx) * HF_STRIDE) * R + e;
+            energy += h[node_face(ne, idx) * R];
+            lumpVolume += h[4 * R];
         }
     }
     // only the w slots are written: other threads read this node's x, y, z
