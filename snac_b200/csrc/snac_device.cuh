@@ -161,13 +161,19 @@ __host__ __device__ __forceinline__ bool exp_within(double x) {
     return biased_exp(x) - (unsigned)(1023 + LO) <= (unsigned)(HI - LO);
 }
 
+// The IEEE division for the rare operands outside the window, as a call: its
+// code (with its own special-case paths) then is not inlined at each of the
+// few dozen division sites of an element kernel, where it cost registers and
+// instruction scheduling on the common path.
+__host__ __device__ __noinline__ double ieee_div(double x, double y) { return x / y; }
+
 // RN(x / c) for a constant c with z = RN(1/c) and 1 <= c <= 16
 __host__ __device__ __forceinline__ double dvk(double x, double c, double z) {
 #if SNAC_MARKSTEIN_DIV >= 1
     const double q0 = x * z;
     const double q = fma(fma(-q0, c, x), z, q0);
     if (is_zero(x)) return q0;
-    if (!exp_within<-900, 900>(x)) return x / c;
+    if (!exp_within<-900, 900>(x)) return ieee_div(x, c);
     return q;
 #else
     (void)z;
@@ -181,7 +187,7 @@ __host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
     const double q0 = x * z;
     const double q = fma(fma(-q0, y, x), z, q0);
     if (is_zero(x)) return q0;
-    if (!(exp_within<-450, 450>(x) && exp_within<-450, 450>(y))) return x / y;
+    if (!(exp_within<-450, 450>(x) && exp_within<-450, 450>(y))) return ieee_div(x, y);
     return q;
 #else
     (void)z;
@@ -281,7 +287,7 @@ __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g,
 // zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
     // RN(0.5 / V) = 0.5 RN(1 / V) exactly while 1 / V is a normal number
-    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : dv(0.5, g.V);
+    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : ieee_div(0.5, g.V);
     double r01 = dv3(-(hV) * (spin_sum(v, g, 0, 1)));
     double r02 = dv3(-(hV) * (spin_sum(v, g, 0, 2)));
     double r12 = dv3(-(hV) * (spin_sum(v, g, 1, 2)));
