@@ -128,9 +128,10 @@ __device__ __forceinline__ void report(DevScalars* sc, int code, long long index
 // ch. 4).  So a division by a constant (z a literal) or several divisions by
 // one divisor (z computed once) cost a multiply and two FMAs each instead of
 // a full division.  The theorem needs the quotient and divisor in the normal
-// range without overflow or underflow: zeros keep the sign of x z, and
-// operands outside a safe exponent window (checked with integer operations
-// on the exponent field) take the IEEE division.  SNAC_MARKSTEIN_DIV = 1
+// range without overflow or underflow: operands outside a safe exponent
+// window and negative divisors (checked with integer operations on the high
+// and low words) take the IEEE division; zeros get their sign from the form
+// of the correction step (markstein() below).  SNAC_MARKSTEIN_DIV = 1
 // uses it for the constant divisors only, 2 also for shared divisors.  The device self-test
 // (snac_gpu_selftest_division) compares every helper with the hardware '/'
 // on random operands, near-ties included.
@@ -150,15 +151,38 @@ __host__ __device__ __forceinline__ unsigned biased_exp(double x) {
     memcpy(&b, &x, 8);
     return (unsigned)(b >> 52) & 0x7ffu;
 }
-__host__ __device__ __forceinline__ bool is_zero(double x) {
-    unsigned long long b;
-    memcpy(&b, &x, 8);
-    return (b << 1) == 0ull;
-}
 // |x| in [2^lo, 2^(hi+1)) by integer tests (keeps the checks off the FP64 pipe)
 template <int LO, int HI>
 __host__ __device__ __forceinline__ bool exp_within(double x) {
     return biased_exp(x) - (unsigned)(1023 + LO) <= (unsigned)(HI - LO);
+}
+__host__ __device__ __forceinline__ void hi_lo(double x, unsigned& h, unsigned& l) {
+#ifdef __CUDA_ARCH__
+    h = (unsigned)__double2hiint(x);
+    l = (unsigned)__double2loint(x);
+#else
+    unsigned long long b;
+    memcpy(&b, &x, 8);
+    h = (unsigned)(b >> 32);
+    l = (unsigned)b;
+#endif
+}
+// x = +-0 or |x| in [2^lo, 2^(hi+1)), on the high and low words: the sign
+// is shifted out of the high word and the window is one unsigned compare
+template <int LO, int HI>
+__host__ __device__ __forceinline__ bool zero_or_within(double x) {
+    unsigned h, l;
+    hi_lo(x, h, l);
+    const bool win = (h << 1) - ((unsigned)(1023 + LO) << 21) <= ((unsigned)(HI - LO + 1) << 21) - 1u;
+    return win || ((h & 0x7fffffffu) | l) == 0u;
+}
+// y in [2^lo, 2^(hi+1)) and positive (a set sign bit puts the high word
+// above the window)
+template <int LO, int HI>
+__host__ __device__ __forceinline__ bool positive_within(double y) {
+    unsigned h, l;
+    hi_lo(y, h, l);
+    return h - ((unsigned)(1023 + LO) << 20) <= ((unsigned)(HI - LO + 1) << 20) - 1u;
 }
 
 // The IEEE division for the rare operands outside the window, as a call: its
@@ -167,13 +191,21 @@ __host__ __device__ __forceinline__ bool exp_within(double x) {
 // instruction scheduling on the common path.
 __host__ __device__ __noinline__ double ieee_div(double x, double y) { return x / y; }
 
+// The correction step RN(q0 + r z), r = x - q0 y, written as
+// -RN(-r z - q0): the same value (round-to-nearest is symmetric), and for
+// y > 0 a zero x also gets the IEEE quotient's sign (+-0 / y = +-0), which
+// RN(q0 + r z) gives -0 / y as +0.  So zeros need no test of their own.
+__host__ __device__ __forceinline__ double markstein(double x, double y, double z, double q0) {
+    const double r = fma(-q0, y, x);
+    return -fma(-r, z, -q0);
+}
+
 // RN(x / c) for a constant c with z = RN(1/c) and 1 <= c <= 16
 __host__ __device__ __forceinline__ double dvk(double x, double c, double z) {
 #if SNAC_MARKSTEIN_DIV >= 1
     const double q0 = x * z;
-    const double q = fma(fma(-q0, c, x), z, q0);
-    if (is_zero(x)) return q0;
-    if (!exp_within<-900, 900>(x)) return ieee_div(x, c);
+    const double q = markstein(x, c, z, q0);
+    if (!zero_or_within<-900, 900>(x)) return ieee_div(x, c);
     return q;
 #else
     (void)z;
@@ -185,9 +217,8 @@ __host__ __device__ __forceinline__ double dvk(double x, double c, double z) {
 __host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
 #if SNAC_MARKSTEIN_DIV >= 2
     const double q0 = x * z;
-    const double q = fma(fma(-q0, y, x), z, q0);
-    if (is_zero(x)) return q0;
-    if (!(exp_within<-450, 450>(x) && exp_within<-450, 450>(y))) return ieee_div(x, y);
+    const double q = markstein(x, y, z, q0);
+    if (!(zero_or_within<-450, 450>(x) && positive_within<-450, 450>(y))) return ieee_div(x, y);
     return q;
 #else
     (void)z;

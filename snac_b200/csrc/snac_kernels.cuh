@@ -1151,6 +1151,11 @@ __global__ void k_selftest_division(long long n, unsigned long long seed, unsign
         double y = __longlong_as_double((long long)((b & 0x800fffffffffffffull) | ((unsigned long long)(1023 + (int)((c >> 20) % 261) - 130) << 52)));
         if ((c >> 40) % 5 == 0) x = rint(x * 1e-3) * y;         // quotients that are exact or near ties
         if ((c >> 44) % 97 == 0) x = ((c >> 50) & 1) ? 0.0 : -0.0;
+        // about 1 in 16: an operand drawn from every exponent (subnormals,
+        // zeros' neighbours, overflow range, Inf and NaN) to exercise the window tests
+        unsigned long long d = splitmix64(st);
+        if ((d & 15) == 0) x = __longlong_as_double((long long)((a & 0x800fffffffffffffull) | ((d >> 8) % 2048) << 52));
+        if (((d >> 4) & 15) == 0) y = __longlong_as_double((long long)((b & 0x800fffffffffffffull) | ((d >> 20) % 2048) << 52));
         local += !same_bits(dv(x, y), x / y);
         local += !same_bits(dvz(x, y, recip(y)), x / y);
         local += !same_bits(dv3(x), x / 3.0) + !same_bits(dv6(x), x / 6.0);
