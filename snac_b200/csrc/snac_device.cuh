@@ -174,7 +174,7 @@ __host__ __device__ __forceinline__ bool zero_or_within(double x) {
     unsigned h, l;
     hi_lo(x, h, l);
     const bool win = (h << 1) - ((unsigned)(1023 + LO) << 21) <= ((unsigned)(HI - LO + 1) << 21) - 1u;
-    return win || ((h & 0x7fffffffu) | l) == 0u;
+    return win | (((h & 0x7fffffffu) | l) == 0u);
 }
 // y in [2^lo, 2^(hi+1)) and positive (a set sign bit puts the high word
 // above the window)
@@ -226,6 +226,56 @@ __host__ __device__ __forceinline__ double dvz(double x, double y, double z) {
 #endif
 }
 
+// Groups of quotients, in place: one window test and one branch for the
+// group instead of one per quotient (a branch per division splits the
+// instruction schedule); a group with any operand outside the window takes
+// the IEEE division for all of its members.
+template <int N>
+__host__ __device__ __forceinline__ void dvk_n(double (&x)[N], double c, double z) {
+#if defined(__CUDA_ARCH__) && SNAC_MARKSTEIN_DIV >= 1
+    double q[N];
+    bool ok = true;
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        q[i] = markstein(x[i], c, z, x[i] * z);
+        ok = ok & zero_or_within<-900, 900>(x[i]);
+    }
+    if (ok) {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = q[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = ieee_div(x[i], c);
+    }
+#else
+    (void)z;
+    for (int i = 0; i < N; i++) x[i] = x[i] / c;
+#endif
+}
+template <int N>
+__host__ __device__ __forceinline__ void dvz_n(double (&x)[N], double y, double z) {
+#if defined(__CUDA_ARCH__) && SNAC_MARKSTEIN_DIV >= 2
+    double q[N];
+    bool ok = positive_within<-450, 450>(y);
+#pragma unroll
+    for (int i = 0; i < N; i++) {
+        q[i] = markstein(x[i], y, z, x[i] * z);
+        ok = ok & zero_or_within<-450, 450>(x[i]);
+    }
+    if (ok) {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = q[i];
+    } else {
+#pragma unroll
+        for (int i = 0; i < N; i++) x[i] = ieee_div(x[i], y);
+    }
+#else
+    (void)z;
+    for (int i = 0; i < N; i++) x[i] = x[i] / y;
+#endif
+}
+constexpr double Z3 = 0x1.5555555555555p-2, Z6 = 0x1.5555555555555p-3;  // RN(1/3), RN(1/6)
+
 __host__ __device__ __forceinline__ double dv(double x, double y) { return x / y; }
 // division by the constants the reference uses; the reciprocal is RN(1/c)
 __host__ __device__ __forceinline__ double dv3(double x) { return dvk(x, 3.0, 0x1.5555555555555p-2); }
@@ -256,10 +306,9 @@ __device__ __forceinline__ void tet_face(const V3& c1, const V3& c2, const V3& c
     double c = x2 * y3 - y2 * x3;
     double s = sqrt(a * a + b * b + c * c);
     area = s / 2.0;
-    const double zs = recip(s);
-    n.x = dvz(a, s, zs);
-    n.y = dvz(b, s, zs);
-    n.z = dvz(c, s, zs);
+    double t[3] = {a, b, c};
+    dvz_n(t, s, recip(s));
+    n = {t[0], t[1], t[2]};
 }
 
 struct TetGeom {
@@ -305,13 +354,12 @@ __device__ __forceinline__ double shear_sum(const V3 v[4], const TetGeom& g, int
 // StrainRate.c:65-184, before the mixed-discretisation correction;
 // sr = (xx, yy, zz, xy, xz, yz)
 __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g, double sr[6]) {
-    const double zV = g.zV;
-    sr[0] = dvz(dv3(-1.0f * (face_sum(v, 0, g, 0))), g.V, zV);
-    sr[1] = dvz(dv3(-1.0f * (face_sum(v, 1, g, 1))), g.V, zV);
-    sr[2] = dvz(dv3(-1.0f * (face_sum(v, 2, g, 2))), g.V, zV);
-    sr[3] = dvz(dv3(-0.5f * (shear_sum(v, g, 0, 1))), g.V, zV);
-    sr[4] = dvz(dv3(-0.5f * (shear_sum(v, g, 0, 2))), g.V, zV);
-    sr[5] = dvz(dv3(-0.5f * (shear_sum(v, g, 1, 2))), g.V, zV);
+    double t[6] = {-1.0f * (face_sum(v, 0, g, 0)), -1.0f * (face_sum(v, 1, g, 1)), -1.0f * (face_sum(v, 2, g, 2)),
+                   -0.5f * (shear_sum(v, g, 0, 1)), -0.5f * (shear_sum(v, g, 0, 2)), -0.5f * (shear_sum(v, g, 1, 2))};
+    dvk_n(t, 3.0, Z3);
+    dvz_n(t, g.V, g.zV);
+#pragma unroll
+    for (int a = 0; a < 6; a++) sr[a] = t[a];
 }
 
 // Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
@@ -319,9 +367,9 @@ __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g,
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
     // RN(0.5 / V) = 0.5 RN(1 / V) exactly while 1 / V is a normal number
     const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : ieee_div(0.5, g.V);
-    double r01 = dv3(-(hV) * (spin_sum(v, g, 0, 1)));
-    double r02 = dv3(-(hV) * (spin_sum(v, g, 0, 2)));
-    double r12 = dv3(-(hV) * (spin_sum(v, g, 1, 2)));
+    double r[3] = {-(hV) * (spin_sum(v, g, 0, 1)), -(hV) * (spin_sum(v, g, 0, 2)), -(hV) * (spin_sum(v, g, 1, 2))};
+    dvk_n(r, 3.0, Z3);
+    const double r01 = r[0], r02 = r[1], r12 = r[2];
     s[0] += (2.0f * r01 * s[3] + 2.0f * r02 * s[4]) * dt;
     s[1] += (2.0f * (-1.0f * r01) * s[3] + 2.0f * r12 * s[5]) * dt;
     s[2] += (2.0f * (-1.0f * r02) * s[4] + 2.0f * (-1.0f * r12) * s[5]) * dt;

@@ -452,9 +452,12 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         for (int f = 0; f < 4; f++) {
             const V3& nr = g.n[f];
             const double A = g.A[f];
-            o[(f * 3 + 0) * R] = dv6((st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A);
-            o[(f * 3 + 1) * R] = dv6((st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A);
-            o[(f * 3 + 2) * R] = dv6((st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A);
+            double t[3] = {(st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A, (st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A,
+                           (st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A};
+            dvk_n(t, 6.0, Z6);
+            o[(f * 3 + 0) * R] = t[0];
+            o[(f * 3 + 1) * R] = t[1];
+            o[(f * 3 + 2) * R] = t[2];
         }
         const long long qt = (long long)s.t * R + s.e;  // row t
         F.fgrav[qt] = cfg.gravity * rho * g.V / 8.0f;
@@ -779,10 +782,11 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
         fx -= demf * sgn(w.x) * fabs(fx);
         fy -= demf * sgn(w.y) * fabs(fy);
         fz -= demf * sgn(w.z) * fabs(fz);
-        const double zm = recip(imass);
-        w.x += dvz(dt * fx, imass, zm);
-        w.y += dvz(dt * fy, imass, zm);
-        w.z += dvz(dt * fz, imass, zm);
+        double dw[3] = {dt * fx, dt * fy, dt * fz};
+        dvz_n(dw, imass, recip(imass));
+        w.x += dw[0];
+        w.y += dw[1];
+        w.z += dw[2];
         uchar4 b = F.bc[n];
         if (b.x != 255) w.x = F.vbc_val[b.x * 3 + 0];
         if (b.y != 255) w.y = F.vbc_val[b.y * 3 + 1];
@@ -817,11 +821,13 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
     const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
     double q[3], tsr = 0.0;
     const double zV = g.zV;
+#pragma unroll
     for (int d = 0; d < 3; d++)
-        q[d] = dvz(dv3(1.0f * M.thermal_conduct *
-                       (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] +
-                        T[2] * comp(g.n[3], d) * g.A[3] + T[3] * comp(g.n[0], d) * g.A[0])),
-                   g.V, zV);
+        q[d] = 1.0f * M.thermal_conduct *
+               (T[0] * comp(g.n[1], d) * g.A[1] + T[1] * comp(g.n[2], d) * g.A[2] + T[2] * comp(g.n[3], d) * g.A[3] +
+                T[3] * comp(g.n[0], d) * g.A[0]);
+    dvk_n(q, 3.0, Z3);
+    dvz_n(q, g.V, zV);
     if (cfg.thermal_stress) {
         const double bulkm = M.lambda + dv3(2.0f * M.mu);
         double temp = 0.25f * (T[0] + T[1] + T[2] + T[3]);
@@ -877,8 +883,12 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
     if (s.active) {
         const long long R = m.ner;
         double* h = F.hflux + (long long)(s.t * HF_STRIDE) * R + s.e;
+        double hf[4];
 #pragma unroll
-        for (int f = 0; f < 4; f++) h[f * R] = dv6((q[0] * g.n[f].x + q[1] * g.n[f].y + q[2] * g.n[f].z) * g.A[f]);
+        for (int f = 0; f < 4; f++) hf[f] = (q[0] * g.n[f].x + q[1] * g.n[f].y + q[2] * g.n[f].z) * g.A[f];
+        dvk_n(hf, 6.0, Z6);
+#pragma unroll
+        for (int f = 0; f < 4; f++) h[f * R] = hf[f];
         // tetra density is set from TimeStepZero on, so the reference's
         // "density == 0" fallback (Heat.c:120-125) is never taken
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
