@@ -245,7 +245,9 @@ def run_ours(args, ws, rank, local):
     torch.cuda.synchronize()
 
     # ---- device-timed steps ------------------------------------------------------------
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    # each step: a 512 MiB write that evicts the model state from L2, then the
+    # step's graph between two CUDA events on the library's stream; the
+    # status is read once after the K steps (snac_gpu_time_steps)
     sampler = ClockSampler(local) if rank == 0 else None
     if sampler:
         sampler.start()
@@ -254,19 +256,12 @@ def run_ours(args, ws, rank, local):
     barrier(ws)
     torch.cuda.synchronize()
     wall0 = time.perf_counter()
-    for k in range(args.steps):
-        with torch.cuda.stream(stream):
-            flush.fill_(float(k))  # 512 MiB write: evicts the model state from L2
-            ev[k][0].record(stream)
-        ctx.lib.snac_gpu_step(ctx.h, 1)  # graph launch + status read
-        with torch.cuda.stream(stream):
-            ev[k][1].record(stream)
+    step_ms = ctx.time_steps(args.steps, flush.data_ptr(), flush.numel() * flush.element_size())
     torch.cuda.synchronize()
     barrier(ws)
     wall = time.perf_counter() - wall0
     launches = ctx.launches - l0
     clocks = sampler.stop() if sampler else None
-    step_ms = [a.elapsed_time(b) for a, b in ev]
     t_dev = sum(step_ms) / 1e3
     value = replica_throughput(ws, ne * args.steps, t_dev)
 

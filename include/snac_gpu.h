@@ -199,6 +199,12 @@ int  snac_gpu_time_step_zero(snac_gpu* h);
  * (_Snac_Context_Sync, Context.c:1208-1268).  The step loop runs from a CUDA
  * graph; nothing is copied to the host. */
 int  snac_gpu_step(snac_gpu* h, int nsteps);
+/* Measurement helper (no counterpart in the reference): nsteps steps as in
+ * snac_gpu_step, each preceded on the handle's stream by a write of
+ * flush_bytes to flush (NULL / 0: none; a buffer larger than L2 evicts the
+ * model state), and bracketed by CUDA events; ms[i] receives the device time
+ * of step i alone.  The status is read once, after all steps. */
+int  snac_gpu_time_steps(snac_gpu* h, int nsteps, void* flush, size_t flush_bytes, double* ms);
 
 /* Loop-level entry points, one per StGermain entry point a plugin replaces
  * with EntryPoint_Replace (StGermain/Base/Extensibility/src/EntryPoint.c:735):

@@ -50,6 +50,8 @@ def load_library(path: str = LIB_PATH):
         f.restype = C.c_int
     lib.snac_gpu_step.argtypes = [vp, C.c_int]
     lib.snac_gpu_step.restype = C.c_int
+    lib.snac_gpu_time_steps.argtypes = [vp, C.c_int, vp, C.c_size_t, C.POINTER(C.c_double)]
+    lib.snac_gpu_time_steps.restype = C.c_int
     lib.snac_gpu_upload.argtypes = [vp, C.POINTER(StateView)]
     lib.snac_gpu_upload.restype = C.c_int
     lib.snac_gpu_download.argtypes = [vp, C.POINTER(StateView)]
@@ -175,6 +177,13 @@ class SnacContext:
 
     def step(self, n: int = 1):
         return self._check(self.lib.snac_gpu_step(self.h, int(n)))
+
+    def time_steps(self, n: int, flush_ptr: int = 0, flush_bytes: int = 0):
+        """n steps, each after a write of flush_bytes at flush_ptr (an L2
+        flush) and timed alone with CUDA events: [ms of step i]."""
+        ms = (C.c_double * int(n))()
+        self._check(self.lib.snac_gpu_time_steps(self.h, int(n), C.c_void_p(flush_ptr or None), int(flush_bytes), ms))
+        return list(ms)
 
     def begin_step(self):
         return self._check(self.lib.snac_gpu_begin_step(self.h))

@@ -349,10 +349,11 @@ int op_fused(snac_gpu* h) {
     return launch_check_named(h, h->temperature ? "k_fused_heat" : "k_fused_step");
 }
 
-int op_min_length_scale(snac_gpu* h) {
-    k_min_length_scale<<<(unsigned)((h->mesh.ne + 127) / 128), 128, 0, h->stream>>>(h->mesh, fields(h));
+int op_min_length_scale_sync(snac_gpu* h) {
+    k_min_length_scale_sync<<<(unsigned)((h->mesh.ne + 127) / 128), 128, 0, h->stream>>>(h->mesh, fields(h), h->cfg,
+                                                                                       h->wave_speed);
     h->launches++;
-    return launch_check_named(h, "k_min_length_scale");
+    return launch_check_named(h, "k_min_length_scale_sync");
 }
 
 int op_sync(snac_gpu* h) {
@@ -394,8 +395,7 @@ int record_step(snac_gpu* h, bool fused) {
         return rc;
     }
     if ((rc = op_loop_nodes(h))) return rc;
-    if ((rc = op_min_length_scale(h))) return rc;
-    return op_sync(h);
+    return op_min_length_scale_sync(h);
 }
 
 // apply a deferred element update so that the state matches the reference's
@@ -834,6 +834,32 @@ int snac_gpu_step(snac_gpu* h, int nsteps) {
         if (rc) return rc;
     }
     return read_status(h);
+}
+
+int snac_gpu_time_steps(snac_gpu* h, int nsteps, void* flush, size_t flush_bytes, double* ms) {
+    if (!h || nsteps < 1 || !ms || (flush_bytes && !flush)) return SNAC_GPU_EINVAL;
+    if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
+    std::vector<cudaEvent_t> ev((size_t)nsteps * 2, nullptr);
+    int rc = 0;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) rc = set_err(h, SNAC_GPU_ECUDA, -1, "cudaEventCreate failed");
+    for (int s = 0; s < nsteps && !rc; s++) {
+        if (flush_bytes && cudaMemsetAsync(flush, s & 0xff, flush_bytes, h->stream) != cudaSuccess)
+            rc = set_err(h, SNAC_GPU_ECUDA, -1, "cudaMemsetAsync of the flush buffer failed");
+        if (!rc) cudaEventRecord(ev[2 * s], h->stream);
+        if (!rc) rc = launch_step(h);
+        if (!rc) cudaEventRecord(ev[2 * s + 1], h->stream);
+    }
+    if (cudaStreamSynchronize(h->stream) != cudaSuccess && !rc)
+        rc = set_err(h, SNAC_GPU_ECUDA, -1, "%s", cudaGetErrorString(cudaGetLastError()));
+    for (int s = 0; s < nsteps && !rc; s++) {
+        float t = 0.f;
+        cudaEventElapsedTime(&t, ev[2 * s], ev[2 * s + 1]);
+        ms[s] = t;
+    }
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    return rc ? rc : read_status(h);
 }
 
 int snac_gpu_begin_step(snac_gpu* h) {

@@ -108,6 +108,8 @@ struct DevScalars {
     int status;                      // first error (SNAC_GPU_E*), 0 if none
     long long err_index;
     long long launches;
+    unsigned blocks_done;            // blocks of k_min_length_scale_sync finished (0 between launches)
+    unsigned pad;
 };
 
 __device__ __forceinline__ void report(DevScalars* sc, int code, long long index) {

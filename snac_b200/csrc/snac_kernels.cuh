@@ -7,6 +7,10 @@
 //   k_loop_nodes     Snac_EP_LoopNodesMomentum   Force.c + UpdateNode.c
 //   k_update_elements Snac_EP_LoopElementsMomentum UpdateElement.c
 //   k_sync           AbstractContext_EP_Sync     Context.c:1208-1268
+// In a steady step the element update of step n runs fused with the stress
+// update of step n+1 (k_fused_step, or k_fused_heat + k_calc_stresses), and
+// the minimum length scale of the element update runs fused with Sync
+// (k_min_length_scale_sync).
 //
 // Element kernels run one thread per tetrahedron: a warp holds three
 // elements in lanes 0-9, 10-19, 20-29 (lanes 30-31 idle).  Element sums
@@ -127,6 +131,23 @@ __device__ __forceinline__ double grp_sum(double v, int base) {
 #pragma unroll
     for (int u = 0; u < NT; u++) s += grp(v, base, u);
     return s;
+}
+
+// a tet's six stress components as three 16-byte accesses (the [nq][6]
+// rows start on 48-byte boundaries)
+__device__ __forceinline__ void load_stress(const Fields& F, long long q, double st[6]) {
+    const double2* p = reinterpret_cast<const double2*>(F.stress + q * 6);
+#pragma unroll
+    for (int a = 0; a < 3; a++) {
+        const double2 v = p[a];
+        st[2 * a] = v.x;
+        st[2 * a + 1] = v.y;
+    }
+}
+__device__ __forceinline__ void store_stress(const Fields& F, long long q, const double st[6]) {
+    double2* p = reinterpret_cast<double2*>(F.stress + q * 6);
+#pragma unroll
+    for (int a = 0; a < 3; a++) p[a] = make_double2(st[2 * a], st[2 * a + 1]);
 }
 
 struct TetSlot {
@@ -315,9 +336,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
             if (eps_p >= pl1 && eps_p <= pl2) {
                 const double dpl = pl2 - pl1, zpl = M.zpl[i];  // = RN(1 / dpl)
-                const double tgf = dvz(f1 - f0, dpl, zpl);
-                const double tgd = dvz(M.dil[i + 1] - M.dil[i], dpl, zpl);
-                const double tgc = dvz(c1 - c0, dpl, zpl);
+                double tg[3] = {f1 - f0, M.dil[i + 1] - M.dil[i], c1 - c0};
+                dvz_n(tg, dpl, zpl);
+                const double tgf = tg[0], tgd = tg[1], tgc = tg[2];
                 fa = f0 + tgf * (eps_p - pl1);
                 da = M.dil[i] + tgd * (eps_p - pl1);
                 co = c0 + tgc * (eps_p - pl1);
@@ -488,12 +509,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     }
 
     if (s.active) {
+        store_stress(F, s.q, st);
         bool ok = true;
 #pragma unroll
-        for (int a = 0; a < 6; a++) {
-            F.stress[s.q * 6 + a] = st[a];
-            ok = ok && isfinite(st[a]);
-        }
+        for (int a = 0; a < 6; a++) ok = ok & (bool)isfinite(st[a]);
         if (!ok) report(F.sc, SNAC_GPU_ENAN, s.e);  // Stress.c:161-166
         if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC) F.eps_p[s.q] = eps_p;
         if (PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC || (PLUGIN == SNAC_RHEOLOGY_MAXWELL && ph == 0)) F.visc[s.q] = eta;
@@ -510,8 +529,7 @@ __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields
     tet_geometry(c, g);
     double st[6] = {0, 0, 0, 0, 0, 0};
     if (s.active) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+        load_stress(F, s.q, st);
     }
     stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
@@ -532,8 +550,7 @@ __device__ __forceinline__ void element_update_tet(const Fields& F, const Config
         F.vol[s.q * 2 + 0] = g.V;
     }
     if (s.active) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) st[a] = F.stress[s.q * 6 + a];
+        load_stress(F, s.q, st);
         rotate_stress(v, g, dt, st);
     }
 }
@@ -580,8 +597,7 @@ __device__ __forceinline__ void k_update_elements_body(const Mesh& m, const Fiel
     double st[6];
     element_update_tet<PLUGIN>(F, cfg, s, v, g, pending ? F.sc->dt_rot : F.sc->dt, st);
     if (s.active) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
+        store_stress(F, s.q, st);
     }
     if (pending) return;  // the minimum length scale of this geometry is already known
     double ls = 1.0e+27f;
@@ -597,7 +613,10 @@ __device__ __forceinline__ void k_update_elements_body(const Mesh& m, const Fiel
     if (s.active && g.V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, s.e);
     // global minimum (exact: min does not round)
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
-    if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
+        __threadfence();  // visible device-wide before this block is counted as done
+    }
 }
 
 template <int PLUGIN>
@@ -653,9 +672,6 @@ __device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fie
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
 
-__global__ void __launch_bounds__(128) k_min_length_scale(Mesh m, Fields F) {
-    k_min_length_scale_body(m, F, blockIdx.x);
-}
 
 // ======================================================================================
 // Snac_EP_LoopNodesMomentum: Snac_Force (Force.c:53-188), then
@@ -934,8 +950,7 @@ __device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F
     double st[6];
     element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
     if (s.active) {
-#pragma unroll
-        for (int a = 0; a < 6; a++) F.stress[s.q * 6 + a] = st[a];
+        store_stress(F, s.q, st);
     }
     heat_flux_tet(m, F, cfg, s, T, T0, g);
 }
@@ -992,11 +1007,12 @@ __global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg
 // AbstractContext_EP_Sync: _Snac_Context_Sync (Context.c:1208-1268), one thread
 // ======================================================================================
 __device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, double wave_speed) {
-    double vmax = __longlong_as_double((long long)sc->vmax_bits);
+    // the reductions are read where the other blocks' atomics left them (L2)
+    double vmax = __longlong_as_double((long long)atomicOr(&sc->vmax_bits, 0ull));
     const double vlb = 3.0e-11f;
     if (vmax < vlb) vmax = vlb;
     sc->vmax = vmax;
-    double minLS = __longlong_as_double((long long)sc->minls_bits);
+    double minLS = __longlong_as_double((long long)atomicOr(&sc->minls_bits, 0ull));
     sc->min_length_scale = minLS;
     if (sc->time_step == 0) sc->init_min_length_scale = minLS;
     sc->dt_rot = sc->dt;  // the element update of this step (done now, or deferred into the next kernel) used this dt
@@ -1009,6 +1025,22 @@ __device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, doub
     }
     sc->vmax_bits = 0ull;
     sc->minls_bits = 0x7ff0000000000000ull;  // +inf
+}
+
+// The minimum length scale of the new coordinates and Sync in one launch:
+// the last block to finish (counted in DevScalars, reset by that block) runs
+// Sync on the completed reductions.
+__global__ void __launch_bounds__(128) k_min_length_scale_sync(Mesh m, Fields F, Config cfg, double wave_speed) {
+    k_min_length_scale_body(m, F, blockIdx.x);
+    __shared__ bool last;
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(&F.sc->blocks_done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (last && threadIdx.x == 0) {
+        __threadfence();
+        sync_one(cfg, F.sc, wave_speed);
+        F.sc->blocks_done = 0u;
+    }
 }
 
 __global__ void k_sync(Config cfg, DevScalars* sc, double wave_speed) {

@@ -125,6 +125,25 @@ def test_run_to_run_bit_reproducible():
         assert np.array_equal(getattr(out[0], f), getattr(out[1], f)), f
 
 
+def test_timed_steps_equal_plain_steps():
+    """the measurement entry point (a flush write and events around each
+    step) runs the same steps as snac_gpu_step"""
+    import torch
+    make, steps = S.CASES["plastic"]
+    a = SnacContext(make())
+    b = SnacContext(make())
+    a.time_step_zero()
+    b.time_step_zero()
+    a.step(6)
+    flush = torch.empty(1 << 20, dtype=torch.uint8, device="cuda")
+    ms = b.time_steps(6, flush.data_ptr(), flush.numel())
+    assert len(ms) == 6 and all(t > 0 for t in ms)
+    assert b.scalars().time_step == 6
+    sa, sb = a.state(), b.state()
+    for f in FIELDS:
+        assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
+
+
 def test_pull_test_known_answer_on_gpu():
     """testUpdateNode-velocity-4-4-4: 10 hook-by-hook iterations of the unit cube."""
     cfg = W.libsnac_unit_cube()
