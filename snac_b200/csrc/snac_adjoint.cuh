@@ -225,11 +225,12 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     double s_mid[6];  // stress after each in-place rotation update (for the reverse)
     double r01 = 0, r02 = 0, r12 = 0;
     if (rotate) {
-        const double hV = dv(0.5, g.V);
-        r01 = dv3(-(hV) * (spin_sum(v, g, 0, 1)));
-        r02 = dv3(-(hV) * (spin_sum(v, g, 0, 2)));
-        r12 = dv3(-(hV) * (spin_sum(v, g, 1, 2)));
         rotate_stress(v, g, dt, s_pre);
+        double r[3];
+        spin_rates(v, g, r);  // the same values rotate_stress used
+        r01 = r[0];
+        r02 = r[1];
+        r12 = r[2];
     }
 #pragma unroll
     for (int a = 0; a < 6; a++) s_mid[a] = s_pre[a];
@@ -241,11 +242,12 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     for (int a = 0; a < 6; a++) sr_raw[a] = sr[a];
     const double vsum = grp_sum(g.V, s.base);
     const double VS = 2.0 * (vsum * 0.5);
+    const double zVS = recip(VS);
     const double tr1 = dv3(sr[0] + sr[1] + sr[2]);
     double P1 = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) P1 += grp(tr1, s.base, u) * grp(g.V, s.base, u);
-    const double corr1 = -1.0f * tr1 + dv(P1, VS);
+    const double corr1 = -1.0f * tr1 + dvz(P1, VS, zVS);
     sr[0] += corr1;
     sr[1] += corr1;
     sr[2] += corr1;
@@ -310,9 +312,11 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         if (eps_p >= pl1 && eps_p <= pl2) {
             const double dpl = pl2 - pl1;
             R.dpl = dpl;
-            R.tgf_b = (M.fric[i + 1] - M.fric[i]) / dpl;
-            R.tgc_b = (M.coh[i + 1] - M.coh[i]) / dpl;
-            R.tgd = (M.dil[i + 1] - M.dil[i]) / dpl;
+            double tg[3] = {M.fric[i + 1] - M.fric[i], M.coh[i + 1] - M.coh[i], M.dil[i + 1] - M.dil[i]};
+            dvz_n(tg, dpl, M.zpl[i]);
+            R.tgf_b = tg[0];
+            R.tgc_b = tg[1];
+            R.tgd = tg[2];
             R.fa_b = M.fric[i] + R.tgf_b * (eps_p - pl1);
             R.co_b = M.coh[i] + R.tgc_b * (eps_p - pl1);
             R.da = M.dil[i] + R.tgd * (eps_p - pl1);
@@ -342,9 +346,9 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
             double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
             double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
             if (eps_p >= pl1 && eps_p <= pl2) {
-                const double dpl = pl2 - pl1, zpl = recip(dpl);
-                const double tgf = dvz(f1 - f0, dpl, zpl);
-                const double tgc = dvz(c1 - c0, dpl, zpl);
+                double tg[2] = {f1 - f0, c1 - c0};
+                dvz_n(tg, pl2 - pl1, M.zpl[i]);
+                const double tgf = tg[0], tgc = tg[1];
                 fa = f0 + tgf * (eps_p - pl1);
                 co = c0 + tgc * (eps_p - pl1);
                 hd = tgc;
@@ -364,8 +368,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     if (s.active && !phi_ok) report(F.sc, SNAC_GPU_ENOTSUP, s.e);
     R.stc = M.ten_off;
     R.stc_from_co = false;
+    // constant-angle values as the forward takes them (host-evaluated, same bits)
+    const bool fconst = M.fric_const && R.fa == M.fric0;
     if (R.fa > 0.0) {
-        double tmp = dv(R.co, tan_fric(M, R.fa));
+        double tmp = fconst ? dvz(R.co, M.tan_fric0, M.ztan_fric0) : dv(R.co, tan_fric(M, R.fa));
         if (tmp < R.stc) {
             R.stc = tmp;
             R.stc_from_co = true;
@@ -373,8 +379,8 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     }
     R.sphi = sin_fric(M, R.fa);
     R.spsi = sin_dil(M, R.da);
-    R.anphi = dv(1.0f + R.sphi, 1.0f - R.sphi);
-    R.anpsi = dv(1.0f + R.spsi, 1.0f - R.spsi);
+    R.anphi = fconst ? M.anphi0 : dv(1.0f + R.sphi, 1.0f - R.sphi);
+    R.anpsi = (M.dil_const && R.da == M.dil0) ? M.anpsi0 : dv(1.0f + R.spsi, 1.0f - R.spsi);
     const double a1 = M.lambda + 2.0f * M.mu;
     const double a2 = M.lambda;
     double st_trial[6];
@@ -384,7 +390,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     R.tension = false;
     R.alam = 0.0;
     R.inc = 0.0;
-    if (!surely_elastic(st, R.co, R.anphi, sqrt(R.anphi), R.stc)) {
+    if (!surely_elastic(st, R.co, R.anphi, fconst ? M.sq_anphi0 : sqrt(R.anphi), R.stc)) {
         principal_stresses(st, R.sp, R.cn);
         double sp[3] = {R.sp[0], R.sp[1], R.sp[2]};
         double fs = sp[0] - sp[2] * R.anphi + 2 * R.co * sqrt(R.anphi);
@@ -410,7 +416,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     double P2 = 0.0f;
 #pragma unroll
     for (int u = 0; u < NT; u++) P2 += grp(trS, s.base, u) * grp(g.V, s.base, u);
-    const double corr2 = -1.0f * trS + dv(P2, VS);
+    const double corr2 = -1.0f * trS + dvz(P2, VS, zVS);
     double sa[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) sa[a] = st[a];
@@ -419,6 +425,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     sa[2] += corr2;
 
     // ---------------- reverse ----------------------------------------------------------------
+    // The reverse sweep needs no reference rounding: divisions by constants and
+    // by the tet volume are multiplications by reciprocals.
+    constexpr double K16 = 1.0 / 6.0, K13 = 1.0 / 3.0;
+    const double iVS = zVS, i9V = (1.0 / 9.0) * g.zV, i3V = K13 * g.zV, i6V = K16 * g.zV;
     D3 wb[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     D3 vb[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
     double Vb = 0.0;
@@ -437,15 +447,15 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
             const int f = (k + 1) & 3;
             const double4 fb = B.fbar[nid[k]];
             const D3& wf = w[f];
-            sab[0] += fb.x * wf.x / 6.0;
-            sab[1] += fb.y * wf.y / 6.0;
-            sab[2] += fb.z * wf.z / 6.0;
-            sab[3] += (fb.x * wf.y + fb.y * wf.x) / 6.0;
-            sab[4] += (fb.x * wf.z + fb.z * wf.x) / 6.0;
-            sab[5] += (fb.y * wf.z + fb.z * wf.y) / 6.0;
-            wb[f].x += (sa[0] * fb.x + sa[3] * fb.y + sa[4] * fb.z) / 6.0;
-            wb[f].y += (sa[3] * fb.x + sa[1] * fb.y + sa[5] * fb.z) / 6.0;
-            wb[f].z += (sa[4] * fb.x + sa[5] * fb.y + sa[2] * fb.z) / 6.0;
+            sab[0] += fb.x * wf.x * K16;
+            sab[1] += fb.y * wf.y * K16;
+            sab[2] += fb.z * wf.z * K16;
+            sab[3] += (fb.x * wf.y + fb.y * wf.x) * K16;
+            sab[4] += (fb.x * wf.z + fb.z * wf.x) * K16;
+            sab[5] += (fb.y * wf.z + fb.z * wf.y) * K16;
+            wb[f].x += (sa[0] * fb.x + sa[3] * fb.y + sa[4] * fb.z) * K16;
+            wb[f].y += (sa[3] * fb.x + sa[1] * fb.y + sa[5] * fb.z) * K16;
+            wb[f].z += (sa[4] * fb.x + sa[5] * fb.y + sa[2] * fb.z) * K16;
             Vb += -cfg.gravity * rho / 8.0 * fb.y;
             // inertial mass of face f
             int dstar = 0;
@@ -458,9 +468,9 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
                 best = wf.z * wf.z;
                 dstar = 2;
             }
-            const double mf = alpha1 * best / (9.0 * g.V) * (dt * dt);
-            addc(wb[f], dstar, fb.w * alpha1 * 2.0 * cmp(wf, dstar) / (9.0 * g.V) * (dt * dt));
-            Vb += -fb.w * mf / g.V;
+            const double mf = alpha1 * best * i9V * (dt * dt);
+            addc(wb[f], dstar, fb.w * alpha1 * 2.0 * cmp(wf, dstar) * i9V * (dt * dt));
+            Vb += -fb.w * mf * g.zV;
         }
     }
     // trace averaging: sa_dd = st_dd - trS + P2 / VS
@@ -468,14 +478,14 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
 #pragma unroll
     for (int a = 0; a < 6; a++) stb[a] = sab[a];
     const double c2b = sab[0] + sab[1] + sab[2];
-    const double P2b_own = c2b / VS;  // summed over the hex below
+    const double P2b_own = c2b * iVS;  // summed over the hex below
     const double P2b = grp_sum(s.active ? P2b_own : 0.0, s.base);
-    double VSb = -(P2 / (VS * VS)) * grp_sum(s.active ? c2b : 0.0, s.base);
+    double VSb = -(P2 * (iVS * iVS)) * grp_sum(s.active ? c2b : 0.0, s.base);
     double trSb = -c2b + P2b * g.V;
     Vb += P2b * trS;
-    stb[0] += trSb / 3.0;
-    stb[1] += trSb / 3.0;
-    stb[2] += trSb / 3.0;
+    stb[0] += trSb * K13;
+    stb[1] += trSb * K13;
+    stb[2] += trSb * K13;
 
     // constitutive reverse: MC return map
     double epb = (s.active && !first_rev) ? B.epbar[s.q] : 0.0;  // adjoint of eps_p^{n+1}
@@ -517,12 +527,12 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         for (int a = 0; a < 3; a++) eb[a] = 2.0 * M.mu * trialb[a] + M.lambda * lsum;
         for (int a = 3; a < 6; a++) eb[a] = 2.0 * M.mu * trialb[a];
     } else {
-        const double bulkm = M.lambda + 2.0 * M.mu / 3.0;
+        const double bulkm = M.lambda + 2.0 * M.mu * K13;
         const double mu = M.mu;
         double sdb[3], db[3] = {0, 0, 0};
         double vic1b = 0.0, vic2b = 0.0;
         const double VSb2 = trialb[0] + trialb[1] + trialb[2];
-        double trsb = VSb2 / 3.0, treb = bulkm * VSb2;
+        double trsb = VSb2 * K13, treb = bulkm * VSb2;
         for (int a = 0; a < 3; a++) {
             const double sdo = trialb[a];
             sdb[a] = sdo * R.vic1 * R.vic2;
@@ -551,9 +561,9 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         }
         for (int a = 0; a < 3; a++) {
             eb[a] = db[a];
-            treb -= db[a] / 3.0;
+            treb -= db[a] * K13;
             sprb[a] = sdb[a];
-            trsb -= sdb[a] / 3.0;
+            trsb -= sdb[a] * K13;
         }
         for (int a = 0; a < 3; a++) {
             sprb[a] += trsb;
@@ -565,21 +575,21 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
 #pragma unroll
     for (int a = 0; a < 6; a++) srb[a] = eb[a] * dt;
     const double c1b = srb[0] + srb[1] + srb[2];
-    const double P1b = grp_sum(s.active ? c1b / VS : 0.0, s.base);
-    VSb += -(P1 / (VS * VS)) * grp_sum(s.active ? c1b : 0.0, s.base);
+    const double P1b = grp_sum(s.active ? c1b * iVS : 0.0, s.base);
+    VSb += -(P1 * (iVS * iVS)) * grp_sum(s.active ? c1b : 0.0, s.base);
     const double tr1b = -c1b + P1b * g.V;
     Vb += P1b * tr1;
-    srb[0] += tr1b / 3.0;
-    srb[1] += tr1b / 3.0;
-    srb[2] += tr1b / 3.0;
+    srb[0] += tr1b * K13;
+    srb[1] += tr1b * K13;
+    srb[2] += tr1b * K13;
     // raw strain rate: sr_d = -S_dd / (3V), sr_ab = -(S_ab + S_ba) / (6V), S_ab = sum_k v_k,a w_k,b
     {
         double Sb[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        for (int d = 0; d < 3; d++) Sb[d][d] = -srb[d] / (3.0 * g.V);
-        Sb[0][1] = Sb[1][0] = -srb[3] / (6.0 * g.V);
-        Sb[0][2] = Sb[2][0] = -srb[4] / (6.0 * g.V);
-        Sb[1][2] = Sb[2][1] = -srb[5] / (6.0 * g.V);
-        for (int a = 0; a < 6; a++) Vb += srb[a] * (-sr_raw[a] / g.V);
+        for (int d = 0; d < 3; d++) Sb[d][d] = -srb[d] * i3V;
+        Sb[0][1] = Sb[1][0] = -srb[3] * i6V;
+        Sb[0][2] = Sb[2][0] = -srb[4] * i6V;
+        Sb[1][2] = Sb[2][1] = -srb[5] * i6V;
+        for (int a = 0; a < 6; a++) Vb += srb[a] * (-sr_raw[a] * g.zV);
 #pragma unroll
         for (int k = 0; k < 4; k++) {
             const D3& wk = w[(k + 1) & 3];
@@ -644,8 +654,8 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         const double rb[3] = {r01b, r02b, r12b};
         const int pa[3] = {0, 0, 1}, pb[3] = {1, 2, 2};
         for (int r = 0; r < 3; r++) {
-            const double SPb = -rb[r] / (6.0 * g.V);
-            Vb += rb[r] * (-rr[r] / g.V);
+            const double SPb = -rb[r] * i6V;
+            Vb += rb[r] * (-rr[r] * g.zV);
 #pragma unroll
             for (int k = 0; k < 4; k++) {
                 const D3& wk = w[(k + 1) & 3];
@@ -668,7 +678,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     {
         const D3 x2 = C[1] - C[0], x3 = C[2] - C[0], x4 = C[3] - C[0];
         const double det = dot(x4, cross(x2, x3));
-        const double detb = Vb * sgnd(det) / 6.0;
+        const double detb = Vb * sgnd(det) * K16;
         const D3 g2 = detb * cross(x3, x4), g3 = detb * cross(x4, x2), g4 = detb * cross(x2, x3);
         cb[1] = cb[1] + g2;
         cb[2] = cb[2] + g3;
@@ -759,13 +769,14 @@ __global__ void __launch_bounds__(128) k_adj_nodes(Mesh m, Fields F, AdjState cu
         const double vpc[3] = {vp.x, vp.y, vp.z};
         const bool fixed[3] = {bc.x != 255, bc.y != 255, bc.z != 255};
         double vout[3];
+        const double im = 1.0 / mass;
         for (int c = 0; c < 3; c++) {
             if (fixed[c]) {
                 fb[c] = 0.0;
                 vout[c] = 0.0;
             } else {
-                const double fdb = vbc[c] * dt / mass;
-                mb += -vbc[c] * dt * fdc[c] / (mass * mass);
+                const double fdb = vbc[c] * dt * im;
+                mb += -vbc[c] * dt * fdc[c] * (im * im);
                 fb[c] = fdb * (1.0 - demf * sgnd(vpc[c]) * sgnd(fdc[c]));
                 vout[c] = vbc[c];
             }

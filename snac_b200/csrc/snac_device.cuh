@@ -364,13 +364,22 @@ __device__ __forceinline__ void tet_strain_rate(const V3 v[4], const TetGeom& g,
     for (int a = 0; a < 6; a++) sr[a] = t[a];
 }
 
+// spin rates r01, r02, r12 of a tet, UpdateElement.c:145-219
+__device__ __forceinline__ void spin_rates(const V3 v[4], const TetGeom& g, double (&r)[3]) {
+    // RN(0.5 / V) = 0.5 RN(1 / V) exactly while 1 / V is a normal number
+    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : ieee_div(0.5, g.V);
+    r[0] = -(hV) * (spin_sum(v, g, 0, 1));
+    r[1] = -(hV) * (spin_sum(v, g, 0, 2));
+    r[2] = -(hV) * (spin_sum(v, g, 1, 2));
+    dvk_n(r, 3.0, Z3);
+}
+
 // Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
 // zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {
     // RN(0.5 / V) = 0.5 RN(1 / V) exactly while 1 / V is a normal number
-    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : ieee_div(0.5, g.V);
-    double r[3] = {-(hV) * (spin_sum(v, g, 0, 1)), -(hV) * (spin_sum(v, g, 0, 2)), -(hV) * (spin_sum(v, g, 1, 2))};
-    dvk_n(r, 3.0, Z3);
+    double r[3];
+    spin_rates(v, g, r);
     const double r01 = r[0], r02 = r[1], r12 = r[2];
     s[0] += (2.0f * r01 * s[3] + 2.0f * r02 * s[4]) * dt;
     s[1] += (2.0f * (-1.0f * r01) * s[3] + 2.0f * r12 * s[5]) * dt;
