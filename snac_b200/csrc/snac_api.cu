@@ -256,7 +256,10 @@ bool topo_on(const Config& c) { return c.topo_kappa > 0 || !(c.topo_crit > 0); }
 
 template <int P>
 void launch_stress(snac_gpu* h, const Fields& F, const Config& c) {
-    k_calc_stresses<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    if (h->mat)
+        k_calc_stresses<P, false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    else
+        k_calc_stresses<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
 template <int P>
 void launch_update(snac_gpu* h, const Fields& F, const Config& c, int pending) {
@@ -264,7 +267,10 @@ void launch_update(snac_gpu* h, const Fields& F, const Config& c, int pending) {
 }
 template <int P>
 void launch_fused(snac_gpu* h, const Fields& F, const Config& c) {
-    k_fused_step<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    if (h->mat)
+        k_fused_step<P, false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    else
+        k_fused_step<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
 template <int P>
 void launch_fused_heat(snac_gpu* h, const Fields& F, const Config& c) {
@@ -777,6 +783,7 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     CK(cudaMemcpyAsync(h->vbc_val, vbc.data(), vbc.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->tbc_val, tbc.data(), tbc.size() * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaMemcpyAsync(h->mats, dm.data(), MAX_PHASES * sizeof(DevMaterial), cudaMemcpyHostToDevice, h->stream));
+    h->cfg.m0 = dm[0];
     CK(cudaMemcpyAsync(h->sc, &sc, sizeof sc, cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return 0;

@@ -41,6 +41,23 @@ __device__ __forceinline__ void load_desc(ModelDesc& dst, const ModelDesc* __res
     for (int i = threadIdx.x; i < W; i += blockDim.x) d[i] = s[i];
 }
 
+// the element bodies for a tile's model: phase 0 from the descriptor (in
+// shared memory) when the model has one phase, else the model's phase table
+template <int P>
+__device__ __forceinline__ void fused_step_any(const ModelDesc& md, int lb) {
+    if (md.F.mat)
+        k_fused_step_body<P, false>(md.m, md.F, md.cfg, lb);
+    else
+        k_fused_step_body<P, true>(md.m, md.F, md.cfg, lb);
+}
+template <int P>
+__device__ __forceinline__ void calc_stresses_any(const ModelDesc& md, int lb) {
+    if (md.F.mat)
+        k_calc_stresses_body<P, false>(md.m, md.F, md.cfg, lb);
+    else
+        k_calc_stresses_body<P, true>(md.m, md.F, md.cfg, lb);
+}
+
 // Element-tile kernels: the fused end-of-step/next-stress kernel (or its
 // heat variant for models with temperature), the heat flux, the stress update.
 template <int OP>
@@ -61,22 +78,22 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
                     k_fused_heat_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y);
             } else {
                 switch (P) {
-                    case SNAC_RHEOLOGY_ELASTIC: k_fused_step_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y); break;
-                    case SNAC_RHEOLOGY_PLASTIC: k_fused_step_body<SNAC_RHEOLOGY_PLASTIC>(md.m, md.F, md.cfg, t.y); break;
+                    case SNAC_RHEOLOGY_ELASTIC: fused_step_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y); break;
+                    case SNAC_RHEOLOGY_PLASTIC: fused_step_any<SNAC_RHEOLOGY_PLASTIC>(md, t.y); break;
                     case SNAC_RHEOLOGY_VISCOPLASTIC:
-                        k_fused_step_body<SNAC_RHEOLOGY_VISCOPLASTIC>(md.m, md.F, md.cfg, t.y);
+                        fused_step_any<SNAC_RHEOLOGY_VISCOPLASTIC>(md, t.y);
                         break;
-                    default: k_fused_step_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y); break;
+                    default: fused_step_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y); break;
                 }
             }
         } else if (OP == BOP_STRESS) {
             switch (P) {
-                case SNAC_RHEOLOGY_ELASTIC: k_calc_stresses_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y); break;
-                case SNAC_RHEOLOGY_PLASTIC: k_calc_stresses_body<SNAC_RHEOLOGY_PLASTIC>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_RHEOLOGY_ELASTIC: calc_stresses_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y); break;
+                case SNAC_RHEOLOGY_PLASTIC: calc_stresses_any<SNAC_RHEOLOGY_PLASTIC>(md, t.y); break;
                 case SNAC_RHEOLOGY_VISCOPLASTIC:
-                    k_calc_stresses_body<SNAC_RHEOLOGY_VISCOPLASTIC>(md.m, md.F, md.cfg, t.y);
+                    calc_stresses_any<SNAC_RHEOLOGY_VISCOPLASTIC>(md, t.y);
                     break;
-                default: k_calc_stresses_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y); break;
+                default: calc_stresses_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y); break;
             }
         } else {
             k_heat_flux_body(md.m, md.F, md.cfg, t.y);
@@ -101,9 +118,9 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
                 k_fused_heat_body<P == SNAC_RHEOLOGY_MAXWELL ? SNAC_RHEOLOGY_MAXWELL : SNAC_RHEOLOGY_ELASTIC>(md.m, md.F,
                                                                                                           md.cfg, t.y);
             else
-                k_fused_step_body<P>(md.m, md.F, md.cfg, t.y);
+                fused_step_any<P>(md, t.y);
         } else if (OP == BOP_STRESS) {
-            k_calc_stresses_body<P>(md.m, md.F, md.cfg, t.y);
+            calc_stresses_any<P>(md, t.y);
         } else {
             k_heat_flux_body(md.m, md.F, md.cfg, t.y);
         }

@@ -79,6 +79,10 @@ struct Config {
     int traction;         // SnacTractionBC on Snac_EP_Force (after Winkler)
     double topo_kappa, topo_crit;  // surface-topography diffusion
     double pisos, rzbo;   // its isostatic pressure and reference bottom depth
+    // phase 0, the only phase of a model without a per-element phase array:
+    // the element kernels of such models read it from their parameters
+    // (constant-bank operands) instead of loading it from the phase table
+    DevMaterial m0;
 };
 
 #ifndef SNAC_ELEM_MINB
@@ -205,7 +209,7 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
 // st holds the tet's stress on entry (already rotated when fused with the
 // element update); the new stress, plastic strain, viscosity, density and
 // the Force terms are stored.
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const V3 v[4], const double T[4], const TetGeom& g, double st[6],
                                               const double dt) {
@@ -242,7 +246,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     for (int a = 0; a < 6; a++) e[a] = sr[a] * dt;
 
     const int ph = s.active ? phase_of(F, s.e) : 0;
-    const DevMaterial& M = F.mats[ph];
+    const DevMaterial& M = ONE ? cfg.m0 : F.mats[ph];  // ONE: the model has one phase
     double eps_p = 0.0, eta = 0.0;
     if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
         eps_p = s.active ? F.eps_p[s.q] : 0.0;
@@ -519,7 +523,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     }
 }
 
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
     V3 c[4], v[4];
@@ -531,12 +535,12 @@ __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields
     if (s.active) {
         load_stress(F, s.q, st);
     }
-    stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
 
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stresses(Mesh m, Fields F, Config cfg) {
-    k_calc_stresses_body<PLUGIN>(m, F, cfg, blockIdx.x);
+    k_calc_stresses_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
 }
 
 // UpdateElement.c:84-91 volume bookkeeping (Maxwell reads V/V_old) and the
@@ -559,7 +563,7 @@ __device__ __forceinline__ void element_update_tet(const Fields& F, const Config
 // are already final) fused with the stress update of step n+1 (dt_{n+1},
 // same geometry and velocities): one geometry evaluation, one stress
 // read-modify-write.  Used when no energy hook sits between the two.
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
     if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
@@ -573,12 +577,12 @@ __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F
     tet_geometry(c, g);
     double st[6] = {0, 0, 0, 0, 0, 0};
     element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
-    stress_update<PLUGIN>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
 
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
-    k_fused_step_body<PLUGIN>(m, F, cfg, blockIdx.x);
+    k_fused_step_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
 }
 
 // ======================================================================================
@@ -685,25 +689,44 @@ __device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fie
 // pressure corrected by the element's bottom height acts on its bottom face
 // (tets 1, 2, 6, 8, faces 0, 1, 2, 2); at step 1 the node's total y force is
 // kept as a residual and subtracted from then on.
-__device__ __noinline__ void winkler_force(const Mesh& m, const Fields& F, const Config& cfg, long long n, int i,
-                                           int k, double& fx, double& fy, double& fz) {
+// The force-BC plugins run for a few boundary nodes only, as calls.  Their
+// arguments are plain values: a reference to the kernel's parameter structs
+// (or to the caller's force registers) would make every thread copy those to
+// its stack before the call.
+struct WinklerArgs {
+    const double4* pos;
+    const unsigned char* mat;
+    const DevMaterial* mats;
+    double* residual_fr;
+    long long time_step;
+    double pisos, gravity, rzbo;
+};
+
+__device__ __noinline__ V3 winkler_force(WinklerArgs a, int nx, int ny, int nz, long long n, int i, int k, V3 f) {
+    Mesh m{};
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.nnx = nx + 1;
+    m.nny = ny + 1;
+    double fx = f.x, fy = f.y, fz = f.z;
     const double factor4 = 1.0f / 4.0f;
-    const double y_node = F.pos[n].y;
+    const double y_node = a.pos[n].y;
     const double nodeT = 0.0;  // the temperature lookup is compiled out in the reference (#if 0)
     for (int ne = 0; ne < 8; ne++) {
         const int ei = i - 1 + (ne & 1), ej = -1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
         if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
         const long long e = (long long)ei + (long long)ej * m.nx + (long long)ek * m.nx * m.ny;
-        const DevMaterial& M = F.mats[phase_of(F, e)];
+        const DevMaterial& M = a.mats[a.mat ? (int)a.mat[e] : 0];
         V3 corner[8];
 #pragma unroll
         for (int cc = 0; cc < 8; cc++) {
-            double4 p = F.pos[corner_node(m, ei, ej, ek, cc)];
+            double4 p = a.pos[corner_node(m, ei, ej, ek, cc)];
             corner[cc] = {p.x, p.y, p.z};
         }
         const double phsDensity = M.density, drosub = 0.0f;
-        const double p_est = cfg.pisos + 0.5f * (phsDensity + drosub) * cfg.gravity * (y_node - cfg.rzbo);
-        const double rosubg = cfg.gravity * (phsDensity + drosub) * (1.0 - M.alpha * (nodeT - M.reftemp) + M.beta * p_est);
+        const double p_est = a.pisos + 0.5f * (phsDensity + drosub) * a.gravity * (y_node - a.rzbo);
+        const double rosubg = a.gravity * (phsDensity + drosub) * (1.0 - M.alpha * (nodeT - M.reftemp) + M.beta * p_est);
         const double dhE = factor4 * (corner[0].y + corner[1].y + corner[4].y + corner[5].y);
         const int ft[4][2] = {{1, 0}, {2, 1}, {6, 2}, {8, 2}};
         double area = 0.0f, A[4];
@@ -719,23 +742,30 @@ __device__ __noinline__ void winkler_force(const Mesh& m, const Fields& F, const
         const double ny_ = -1.0f * factor4 * (nr[0].y + nr[1].y + nr[2].y + nr[3].y);
         const double nz_ = factor4 * (nr[0].z + nr[1].z + nr[2].z + nr[3].z);
         area *= 0.5f;
-        const double press_norm = cfg.pisos + rosubg * (cfg.rzbo - dhE);
+        const double press_norm = a.pisos + rosubg * (a.rzbo - dhE);
         fx += factor4 * (press_norm * area * nx_);
         fy += factor4 * (press_norm * area * ny_);
         fz += factor4 * (press_norm * area * nz_);
     }
-    if (F.sc->time_step == 1) {  // restartTimestep == 0
+    if (a.time_step == 1) {  // restartTimestep == 0
         const double Fy = fy;
-        if (Fy != 0.0) F.residual_fr[n] = Fy;
+        if (Fy != 0.0) a.residual_fr[n] = Fy;
     }
-    fy -= F.residual_fr[n];
+    fy -= a.residual_fr[n];
+    return V3{fx, fy, fz};
 }
 
 // SnacTractionBC's active branch (Snac/plugins/tractionBC/Force.c:43-268):
 // on a right-wall node (i == nx), each incident element's right face (the
 // triangles (1,2,6) and (1,6,5)) carries the fixed stress sxx = 1e8 Pa.
-__device__ __noinline__ void traction_force(const Mesh& m, const Fields& F, int j, int k, double& fx, double& fy,
-                                            double& fz) {
+__device__ __noinline__ V3 traction_force(const double4* pos, int nx, int ny, int nz, int j, int k, V3 f) {
+    Mesh m{};
+    m.nx = nx;
+    m.ny = ny;
+    m.nz = nz;
+    m.nnx = nx + 1;
+    m.nny = ny + 1;
+    double fx = f.x, fy = f.y, fz = f.z;
     const double factor4 = 1.0f / 4.0f;
     const double s00 = 1.0e+08, s01 = 0.0, s02 = 0.0, s10 = 0.0, s11 = 0.0, s12 = 0.0, s20 = 0.0, s21 = 0.0, s22 = 0.0;
     const int i = m.nnx - 1;
@@ -743,7 +773,7 @@ __device__ __noinline__ void traction_force(const Mesh& m, const Fields& F, int 
         const int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
         if (ei < 0 || ej < 0 || ek < 0 || ei >= m.nx || ej >= m.ny || ek >= m.nz) continue;
         auto P = [&](int c) {
-            const double4 p = F.pos[corner_node(m, ei, ej, ek, c)];
+            const double4 p = pos[corner_node(m, ei, ej, ek, c)];
             return V3{p.x, p.y, p.z};
         };
         const V3 c1 = P(1), c2 = P(2), c5 = P(5), c6 = P(6);
@@ -757,6 +787,7 @@ __device__ __noinline__ void traction_force(const Mesh& m, const Fields& F, int 
         fy += factor4 * area * (s10 * nx_ + s11 * ny_ + s12 * nz_);
         fz += factor4 * area * (s20 * nx_ + s21 * ny_ + s22 * nz_);
     }
+    return V3{fx, fy, fz};
 }
 
 template <int DTTYPE>
@@ -789,8 +820,19 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 fy -= F.fgrav[t * R + e];
             }
         }
-        if (cfg.winkler && cfg.gravity > 0.0 && j == 0) winkler_force(m, F, cfg, n, i, k, fx, fy, fz);
-        if (cfg.traction && i == m.nnx - 1) traction_force(m, F, j, k, fx, fy, fz);
+        if (cfg.winkler && cfg.gravity > 0.0 && j == 0) {
+            const WinklerArgs a{F.pos, F.mat, F.mats, F.residual_fr, F.sc->time_step, cfg.pisos, cfg.gravity, cfg.rzbo};
+            const V3 r = winkler_force(a, m.nx, m.ny, m.nz, n, i, k, V3{fx, fy, fz});
+            fx = r.x;
+            fy = r.y;
+            fz = r.z;
+        }
+        if (cfg.traction && i == m.nnx - 1) {
+            const V3 r = traction_force(F.pos, m.nx, m.ny, m.nz, j, k, V3{fx, fy, fz});
+            fx = r.x;
+            fy = r.y;
+            fz = r.z;
+        }
         // FLAC local damping with the pre-update velocity, then v and x
         double4 w = F.vel[n];
         const double demf = cfg.demf;
