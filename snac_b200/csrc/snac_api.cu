@@ -274,12 +274,18 @@ void launch_fused(snac_gpu* h, const Fields& F, const Config& c) {
 }
 template <int P>
 void launch_fused_heat(snac_gpu* h, const Fields& F, const Config& c) {
-    k_fused_heat<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    if (h->mat)
+        k_fused_heat<P, false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    else
+        k_fused_heat<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
 
 int op_energy_elements(snac_gpu* h) {
     if (!h->temperature) return 0;
-    k_heat_flux<<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
+    if (h->mat)
+        k_heat_flux<false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
+    else
+        k_heat_flux<true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
     h->launches++;
     return launch_check_named(h, "k_heat_flux");
 }

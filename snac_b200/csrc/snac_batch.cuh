@@ -58,6 +58,20 @@ __device__ __forceinline__ void calc_stresses_any(const ModelDesc& md, int lb) {
         k_calc_stresses_body<P, true>(md.m, md.F, md.cfg, lb);
 }
 
+template <int P>
+__device__ __forceinline__ void fused_heat_any(const ModelDesc& md, int lb) {
+    if (md.F.mat)
+        k_fused_heat_body<P, false>(md.m, md.F, md.cfg, lb);
+    else
+        k_fused_heat_body<P, true>(md.m, md.F, md.cfg, lb);
+}
+__device__ __forceinline__ void heat_flux_any(const ModelDesc& md, int lb) {
+    if (md.F.mat)
+        k_heat_flux_body<false>(md.m, md.F, md.cfg, lb);
+    else
+        k_heat_flux_body<true>(md.m, md.F, md.cfg, lb);
+}
+
 // Element-tile kernels: the fused end-of-step/next-stress kernel (or its
 // heat variant for models with temperature), the heat flux, the stress update.
 template <int OP>
@@ -73,9 +87,9 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
         if (OP == BOP_FUSED) {
             if (md.cfg.temperature) {
                 if (P == SNAC_RHEOLOGY_MAXWELL)
-                    k_fused_heat_body<SNAC_RHEOLOGY_MAXWELL>(md.m, md.F, md.cfg, t.y);
+                    fused_heat_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y);
                 else
-                    k_fused_heat_body<SNAC_RHEOLOGY_ELASTIC>(md.m, md.F, md.cfg, t.y);
+                    fused_heat_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y);
             } else {
                 switch (P) {
                     case SNAC_RHEOLOGY_ELASTIC: fused_step_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y); break;
@@ -96,7 +110,7 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
                 default: calc_stresses_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y); break;
             }
         } else {
-            k_heat_flux_body(md.m, md.F, md.cfg, t.y);
+            heat_flux_any(md, t.y);
         }
     }
 }
@@ -115,14 +129,13 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
         __syncthreads();
         if (OP == BOP_FUSED) {
             if (TEMP)
-                k_fused_heat_body<P == SNAC_RHEOLOGY_MAXWELL ? SNAC_RHEOLOGY_MAXWELL : SNAC_RHEOLOGY_ELASTIC>(md.m, md.F,
-                                                                                                          md.cfg, t.y);
+                fused_heat_any<P == SNAC_RHEOLOGY_MAXWELL ? SNAC_RHEOLOGY_MAXWELL : SNAC_RHEOLOGY_ELASTIC>(md, t.y);
             else
                 fused_step_any<P>(md, t.y);
         } else if (OP == BOP_STRESS) {
             calc_stresses_any<P>(md, t.y);
         } else {
-            k_heat_flux_body(md.m, md.F, md.cfg, t.y);
+            heat_flux_any(md, t.y);
         }
     }
 }

@@ -874,9 +874,10 @@ __global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg
 // Snac_EP_LoopElementsEnergy: Snac_HeatFlux (temperature/HeatFlux.c:60-200) and
 // SnacTemperature_HeatFluxBC (temperature/VariableConditions.c:280-413)
 // ======================================================================================
+template <bool ONE>
 __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const double T[4], const double T0[4], const TetGeom& g) {
-    const DevMaterial& M = F.mats[s.active ? phase_of(F, s.e) : 0];
+    const DevMaterial& M = ONE ? cfg.m0 : F.mats[s.active ? phase_of(F, s.e) : 0];
     double q[3], tsr = 0.0;
     const double zV = g.zV;
 #pragma unroll
@@ -961,6 +962,7 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
     }
 }
 
+template <bool ONE>
 __device__ __forceinline__ void k_heat_flux_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
     V3 c[4], v[4];
@@ -968,16 +970,17 @@ __device__ __forceinline__ void k_heat_flux_body(const Mesh& m, const Fields& F,
     load_tet(m, F, s, c, v, T, T0);
     TetGeom g;
     tet_geometry(c, g);
-    heat_flux_tet(m, F, cfg, s, T, T0, g);
+    heat_flux_tet<ONE>(m, F, cfg, s, T, T0, g);
 }
 
+template <bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg) {
-    k_heat_flux_body(m, F, cfg, blockIdx.x);
+    k_heat_flux_body<ONE>(m, F, cfg, blockIdx.x);
 }
 
 // End of step n (element update) fused with the heat flux of step n+1: both
 // need the geometry of the same coordinates.
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
     if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
@@ -994,12 +997,12 @@ __device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F
     if (s.active) {
         store_stress(F, s.q, st);
     }
-    heat_flux_tet(m, F, cfg, s, T, T0, g);
+    heat_flux_tet<ONE>(m, F, cfg, s, T, T0, g);
 }
 
-template <int PLUGIN>
+template <int PLUGIN, bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(Mesh m, Fields F, Config cfg) {
-    k_fused_heat_body<PLUGIN>(m, F, cfg, blockIdx.x);
+    k_fused_heat_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
 }
 
 // ======================================================================================
