@@ -298,7 +298,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         R.vic1 = 1.0f - R.tmp;
         R.vic2 = dv(1.0f, 1.0f + R.tmp);
         double stressd[3] = {R.sd[0], R.sd[1], R.sd[2]};
-        maxwell_update(st, e, stressd, R.d, R.trs, R.tre, M.mu, eta, dt, bulkm);
+        maxwell_update(st, e, stressd, R.d, dv3(R.trs), R.tre, M.mu, eta, dt, bulkm);
     }
     // softening lookup: this tet's own segment (plastic: first match, clamp past the end;
     // visco-plastic: last match)

@@ -594,7 +594,7 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
 // The unclipped viscosity: refvisc (srJ2/refsrate)^expo exp(H/R (1/T - 1/Tref)).
 __device__ __forceinline__ double arrhenius_base(const DevMaterial& M, double refvisc, double srJ2, double avgTemp) {
     return refvisc * pow(dvz(srJ2, M.refsrate, M.vp_zrs), M.vp_expo) *
-           exp(M.vp_hr * (dv(1., avgTemp + 273.15) - M.vp_irt));
+           exp(M.vp_hr * (recip(avgTemp + 273.15) - M.vp_irt));
 }
 
 __device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, double refvisc, double srJ2,
@@ -608,18 +608,18 @@ __device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, doub
 // Maxwell visco-elastic update of one tet, viscoplastic/Constitutive.c:211-257
 // and maxwell/Constitutive.c:146-183 (identical arithmetic).
 __device__ __forceinline__ void maxwell_update(double s[6], const double e[6], double stressd[3],
-                                               const double straind[3], double trace_stress, double trace_strain,
+                                               const double straind[3], double trace_stress3, double trace_strain,
                                                double rmu, double eta, double dt, double bulkm) {
     double temp = dv(rmu, 2.0f * (eta)) * dt;
     double vic1 = 1.0f - temp;
-    double vic2 = dv(1.0f, 1.0f + temp);
+    double vic2 = recip(1.0f + temp);  // RN(1 / x), the same bits as 1.0 / x
     stressd[0] = (stressd[0] * vic1 + 2.0f * rmu * straind[0]) * vic2;
     stressd[1] = (stressd[1] * vic1 + 2.0f * rmu * straind[1]) * vic2;
     stressd[2] = (stressd[2] * vic1 + 2.0f * rmu * straind[2]) * vic2;
     s[3] = (s[3] * vic1 + 2.0f * rmu * e[3]) * vic2;
     s[4] = (s[4] * vic1 + 2.0f * rmu * e[4]) * vic2;
     s[5] = (s[5] * vic1 + 2.0f * rmu * e[5]) * vic2;
-    double VolumicStress = dv3(trace_stress) + bulkm * trace_strain;
+    double VolumicStress = trace_stress3 + bulkm * trace_strain;
     s[0] = stressd[0] + VolumicStress;
     s[1] = stressd[1] + VolumicStress;
     s[2] = stressd[2] + VolumicStress;

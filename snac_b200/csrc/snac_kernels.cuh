@@ -275,8 +275,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         double trace_stress = st[0] + st[1] + st[2];
         double trace_strain = dv(vcur, vold) - 1.0f;
         double straind[3], stressd[3];
-        for (int a = 0; a < 3; a++) straind[a] = e[a] - dv3(trace_strain);
-        for (int a = 0; a < 3; a++) stressd[a] = st[a] - dv3(trace_stress);
+        const double tn3 = dv3(trace_strain), ts3 = dv3(trace_stress);
+        for (int a = 0; a < 3; a++) straind[a] = e[a] - tn3;
+        for (int a = 0; a < 3; a++) stressd[a] = st[a] - ts3;
         double srJ2 = sqrt(fabs(straind[1] * straind[2] + straind[2] * straind[0] + straind[0] * straind[1] -
                                 e[3] * e[3] - e[4] * e[4] - e[5] * e[5])) /
                       dt;
@@ -285,7 +286,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
         eta = arrhenius_viscosity(M, M.refvisc, srJ2, avgTemp);
         if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
-        if (ph == 0) maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
+        if (ph == 0) maxwell_update(st, e, stressd, straind, ts3, trace_strain, M.mu, eta, dt, bulkm);
     } else {
         if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) {
             // elastic trial, plastic/Constitutive.c:114-121
@@ -309,8 +310,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double trace_stress = st[0] + st[1] + st[2];
             double trace_strain = e[0] + e[1] + e[2];
             double straind[3], stressd[3];
-            for (int a = 0; a < 3; a++) straind[a] = e[a] - dv3(trace_strain);
-            for (int a = 0; a < 3; a++) stressd[a] = st[a] - dv3(trace_stress);
+            const double tn3 = dv3(trace_strain), ts3 = dv3(trace_stress);
+            for (int a = 0; a < 3; a++) straind[a] = e[a] - tn3;
+            for (int a = 0; a < 3; a++) stressd[a] = st[a] - ts3;
             // viscoplastic/Constitutive.c:189 reads strain[1][0], strain[2][0] and stress[2][0]
             // (the pointer, not the tensor, is indexed); those entries are always zero.
             const double lower = 0.0;
@@ -324,7 +326,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             if (F.visc_scale && s.active) refvisc = M.refvisc * F.visc_scale[s.e];
             eta = arrhenius_viscosity(M, refvisc, srJ2, avgTemp);
             if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
-            maxwell_update(st, e, stressd, straind, trace_stress, trace_strain, M.mu, eta, dt, bulkm);
+            maxwell_update(st, e, stressd, straind, ts3, trace_strain, M.mu, eta, dt, bulkm);
         }
         // piecewise-linear softening (plastic/Constitutive.c:133-159 with break and
         // clamp; viscoplastic/Constitutive.c:279-293 without either: the last
