@@ -460,8 +460,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             // UpdateAverageTemp_LoopElements (Heat.c:143-172) ran before the
             // temperature BCs were re-applied: use the pre-BC temperatures
             avgT = 0.0;
+            int ei = 0, ej = 0, ek = 0;  // recomputed here: the slot's i, j, k need not stay live
+            if (s.active) elem_ijk(m, s.e, ei, ej, ek);
             for (int qn = 0; qn < 4; qn++) {
-                long long n = s.active ? corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn)) : 0;
+                long long n = s.active ? corner_node(m, ei, ej, ek, tet_node_rt(s.t, qn)) : 0;
                 avgT += F.tpre[n] / (1.0f * 4);
             }
         }
