@@ -621,10 +621,7 @@ __device__ __forceinline__ void k_update_elements_body(const Mesh& m, const Fiel
     if (s.active && g.V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, s.e);
     // global minimum (exact: min does not round)
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
-    if ((threadIdx.x & 31) == 0) {
-        atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
-        __threadfence();  // visible device-wide before this block is counted as done
-    }
+    if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
 
 template <int PLUGIN>
@@ -638,7 +635,7 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elem
 // tet, min_f RN(V/A_f) = RN(V / max_f A_f) because correctly rounded
 // division is monotonic, and max_f A_f = RN(sqrt(max_f s_f))/2 for the same
 // reason; faces with A = 0 are skipped as in the reference.
-__device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fields& F, int lb) {
+__device__ __forceinline__ double hex_min_length_scale(const Mesh& m, const Fields& F, int lb) {
     long long e = (long long)lb * blockDim.x + threadIdx.x;
     double ls = 1.0e+27f;
     if (e < m.ne) {
@@ -676,6 +673,11 @@ __device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fie
             if (V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, e);
         }
     }
+    return ls;
+}
+
+__device__ __forceinline__ void k_min_length_scale_body(const Mesh& m, const Fields& F, int lb) {
+    double ls = hex_min_length_scale(m, F, lb);
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
     if ((threadIdx.x & 31) == 0) atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(ls));
 }
@@ -1080,10 +1082,20 @@ __device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, doub
 // the last block to finish (counted in DevScalars, reset by that block) runs
 // Sync on the completed reductions.
 __global__ void __launch_bounds__(128) k_min_length_scale_sync(Mesh m, Fields F, Config cfg, double wave_speed) {
-    k_min_length_scale_body(m, F, blockIdx.x);
+    double ls = hex_min_length_scale(m, F, blockIdx.x);
+    for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
+    // the block's minimum in one atomic (fewer atomics on the one address),
+    // fenced so that it is visible device-wide before the block is counted
+    __shared__ double wmin[4];
     __shared__ bool last;
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = ls;
     __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&F.sc->blocks_done, 1u) == gridDim.x - 1;
+    if (threadIdx.x == 0) {
+        const double b = fmin(fmin(wmin[0], wmin[1]), fmin(wmin[2], wmin[3]));
+        atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(b));
+        __threadfence();
+        last = atomicAdd(&F.sc->blocks_done, 1u) == gridDim.x - 1;
+    }
     __syncthreads();
     if (last && threadIdx.x == 0) {
         __threadfence();
