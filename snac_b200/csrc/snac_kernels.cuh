@@ -209,6 +209,38 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
 // st holds the tet's stress on entry (already rotated when fused with the
 // element update); the new stress, plastic strain, viscosity, density and
 // the Force terms are stored.
+// The tet's four face areas and normals are needed again only by the force
+// terms at the end of the stress update; across the constitutive update
+// (the eigen-solve of a yielding tet needs ~60 registers) they wait in
+// shared memory, one 16-double column per thread, instead of in registers
+// that the compiler would otherwise spill to local memory.
+__shared__ double face_stash[16 * ELEM_WARPS * 32];
+
+__device__ __forceinline__ void stash_faces(const TetGeom& g) {
+    constexpr int W = ELEM_WARPS * 32;
+    const int tid = threadIdx.x;
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        face_stash[(f * 4 + 0) * W + tid] = g.A[f];
+        face_stash[(f * 4 + 1) * W + tid] = g.n[f].x;
+        face_stash[(f * 4 + 2) * W + tid] = g.n[f].y;
+        face_stash[(f * 4 + 3) * W + tid] = g.n[f].z;
+    }
+    asm volatile("" ::: "memory");  // keep the copies in shared memory, not in registers
+}
+__device__ __forceinline__ void unstash_faces(TetGeom& g) {
+    constexpr int W = ELEM_WARPS * 32;
+    const int tid = threadIdx.x;
+    asm volatile("" ::: "memory");
+#pragma unroll
+    for (int f = 0; f < 4; f++) {
+        g.A[f] = face_stash[(f * 4 + 0) * W + tid];
+        g.n[f].x = face_stash[(f * 4 + 1) * W + tid];
+        g.n[f].y = face_stash[(f * 4 + 2) * W + tid];
+        g.n[f].z = face_stash[(f * 4 + 3) * W + tid];
+    }
+}
+
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const V3 v[4], const double T[4], const TetGeom& g, double st[6],
@@ -245,6 +277,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 #pragma unroll
     for (int a = 0; a < 6; a++) e[a] = sr[a] * dt;
 
+    stash_faces(g);
     const int ph = s.active ? phase_of(F, s.e) : 0;
     const DevMaterial& M = ONE ? cfg.m0 : F.mats[ph];  // ONE: the model has one phase
     double eps_p = 0.0, eta = 0.0;
@@ -473,14 +506,18 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     // Per-tet terms of Snac_Force (Force.c:107-180), evaluated here where the
     // tet's geometry and new stress already are.  k_loop_nodes adds them in
     // the reference's node-centred order, so the sums keep their bits.
+    TetGeom gf;  // the faces back from shared memory
+    gf.V = g.V;
+    gf.zV = g.zV;
+    unstash_faces(gf);
     if (s.active) {
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
         const long long R = m.ner;
         double* o = F.fterm + (long long)(s.t * 12) * R + s.e;
 #pragma unroll
         for (int f = 0; f < 4; f++) {
-            const V3& nr = g.n[f];
-            const double A = g.A[f];
+            const V3& nr = gf.n[f];
+            const double A = gf.A[f];
             double t[3] = {(st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A, (st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A,
                            (st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A};
             dvk_n(t, 6.0, Z6);
@@ -489,19 +526,19 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             o[(f * 3 + 2) * R] = t[2];
         }
         const long long qt = (long long)s.t * R + s.e;  // row t
-        F.fgrav[qt] = cfg.gravity * rho * g.V / 8.0f;
+        F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
             const double sos = F.sc->speed_of_sound;
             const double inertialDensity = dv(M.lambda + 2.0f * M.mu, sos * sos);
-            F.fmass[qt] = factor4 * inertialDensity * g.V;
+            F.fmass[qt] = factor4 * inertialDensity * gf.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
-            const double nineV = 9.0f * g.V, z9V = recip(nineV);
+            const double nineV = 9.0f * gf.V, z9V = recip(nineV);
 #pragma unroll
             for (int f = 0; f < 4; f++) {
-                const V3& nr = g.n[f];
-                const double A = g.A[f];
+                const V3& nr = gf.n[f];
+                const double A = gf.A[f];
                 double area_sum = 0.0, temp;
                 temp = (nr.x * A) * (nr.x * A);
                 if (temp > area_sum) area_sum = temp;
@@ -512,7 +549,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
                 F.fmass[(long long)(s.t * 4 + f) * R + s.e] = dvz(alpha1 * area_sum, nineV, z9V) * (dt * dt);
             }
         } else {
-            F.fmass[qt] = factor4 * rho * g.V;
+            F.fmass[qt] = factor4 * rho * gf.V;
         }
     }
 
