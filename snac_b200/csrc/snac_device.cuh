@@ -591,10 +591,15 @@ __device__ __forceinline__ int mc_return_map(double sp[3], const double cn[3][3]
 
 // Power-law / Arrhenius viscosity, viscoplastic/Constitutive.c:186-210 and
 // maxwell/Constitutive.c:122-142, clipped to [vis_min, vis_max].
-// The unclipped viscosity: refvisc (srJ2/refsrate)^expo exp(H/R (1/T - 1/Tref)).
+// The unclipped viscosity refvisc (srJ2/refsrate)^expo exp(H/R (1/T - 1/Tref)),
+// evaluated as one exponential, refvisc exp(expo ln(srJ2/refsrate) +
+// H/R (1/T - 1/Tref)): the same value to a few ulp (the exponent is O(10)),
+// one transcendental instead of pow and exp.  The reference's libm pow/exp
+// are not reproduced bit for bit on the device either way, so visco-plastic
+// and Maxwell runs are compared with the oracle at a tolerance.
 __device__ __forceinline__ double arrhenius_base(const DevMaterial& M, double refvisc, double srJ2, double avgTemp) {
-    return refvisc * pow(dvz(srJ2, M.refsrate, M.vp_zrs), M.vp_expo) *
-           exp(M.vp_hr * (recip(avgTemp + 273.15) - M.vp_irt));
+    return refvisc * exp(M.vp_expo * log(dvz(srJ2, M.refsrate, M.vp_zrs)) +
+                         M.vp_hr * (recip(avgTemp + 273.15) - M.vp_irt));
 }
 
 __device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, double refvisc, double srJ2,
