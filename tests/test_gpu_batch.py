@@ -63,7 +63,7 @@ def test_batch_against_oracle():
             sg, sc = b.models[i].state(), c.state()
             if cfg.plugin == "SnacPlastic":  # constant friction angle: bitwise
                 assert_same(sg, sc, f"model {i}")
-            else:  # device pow/exp in the viscosity: plastic tolerance
+            else:  # device log/exp in the viscosity: plastic tolerance
                 for f in ("coord", "velocity", "stress", "temperature"):
                     x, y = getattr(sg, f), getattr(sc, f)
                     assert np.max(np.abs(x - y)) <= 1e-6 * np.max(np.abs(y)), (i, f)

@@ -114,7 +114,7 @@ def test_output_files_bitwise(tmp_path, case):
 
 
 def test_output_files_viscoplastic(tmp_path):
-    """Device pow/exp/log10: the records agree with the oracle's to float rounding."""
+    """Device log/exp/log10: the records agree with the oracle's to float rounding."""
     out, expect, _, _ = run(tmp_path, "viscoplastic", nsteps=5, dump_every=2, cp_every=5)
     for name, recs in expect.items():
         want = np.concatenate(recs)

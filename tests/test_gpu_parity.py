@@ -3,7 +3,7 @@
 Elastic and constant-friction plastic runs must agree with the oracle to the
 last bit (the kernels keep the reference's operation order, without FMA
 contraction; sin/tan of a constant friction angle come from the host C
-library).  Runs that evaluate pow/exp on the device (visco-plastic, Maxwell)
+library).  Runs that evaluate the Arrhenius viscosity on the device (visco-plastic, Maxwell)
 are compared with a normwise relative tolerance: max|gpu - cpu| / max|cpu|
 per field <= 1e-9 (elastic bar of the target) or <= 1e-6 (plastic bar).
 """
@@ -64,7 +64,7 @@ def test_plastic_case_yields_on_gpu():
     assert np.count_nonzero(g.state().plastic_strain) > 100
 
 
-# pow/exp on the device differ from the host libm in the last bit; through the
+# the device viscosity differs from the host libm pow * exp in the last bits; through the
 # yield branch the difference stays far below the plastic bar (1e-6), and
 # without plasticity (Maxwell) below the elastic bar (1e-9).
 @pytest.mark.parametrize("case,tol", [("viscoplastic", 1e-6), ("maxwell", 1e-9), ("density", 1e-6)])
