@@ -362,6 +362,8 @@ KERNEL_BYTES = {
     "k_fused_heat": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + 8.0 * NODES_PER_HEX[w],
     "k_calc_stresses": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
                                  + (8.0 * NODES_PER_HEX[w] if w == "c3" else 0.0),
+    "k_fused_stress": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
+                                + (8.0 * NODES_PER_HEX[w] if w == "c3" else 0.0),
     "k_loop_nodes": lambda w: 480.0 + 96.0 * NODES_PER_HEX[w],
     "k_update_elements": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w],
 }

@@ -272,22 +272,42 @@ void launch_fused(snac_gpu* h, const Fields& F, const Config& c) {
     else
         k_fused_step<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
 }
-template <int P>
-void launch_fused_heat(snac_gpu* h, const Fields& F, const Config& c) {
-    if (h->mat)
-        k_fused_heat<P, false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
-    else
-        k_fused_heat<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
-}
-
-int op_energy_elements(snac_gpu* h) {
+// count_step: this launch opens the step (timeStep++, currentTime += dt)
+int op_energy_elements(snac_gpu* h, int count_step = 0) {
     if (!h->temperature) return 0;
     if (h->mat)
-        k_heat_flux<false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
+        k_heat_flux<false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg,
+                                                                                   count_step);
     else
-        k_heat_flux<true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
+        k_heat_flux<true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg,
+                                                                                  count_step);
     h->launches++;
+    if (count_step) h->time_step++;
     return launch_check_named(h, "k_heat_flux");
+}
+
+template <int P>
+void launch_fused_stress(snac_gpu* h, const Fields& F, const Config& c) {
+    if (h->mat)
+        k_fused_stress<P, false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+    else
+        k_fused_stress<P, true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c);
+}
+
+// temperature runs: the pending element update of the previous step with
+// this step's stress update, after the energy hooks
+int op_fused_stress(snac_gpu* h) {
+    Fields F = fields(h);
+    Config c = h->cfg;
+    c.time_step_zero = 0;
+    switch (h->constitutive) {
+        case SNAC_RHEOLOGY_ELASTIC: launch_fused_stress<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_PLASTIC: launch_fused_stress<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused_stress<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_MAXWELL: launch_fused_stress<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
+    }
+    h->launches++;
+    return launch_check_named(h, "k_fused_stress");
 }
 
 int op_energy_nodes(snac_gpu* h) {
@@ -338,27 +358,21 @@ int op_update_elements(snac_gpu* h, bool step_zero, int pending = 0) {
     return launch_check_named(h, "k_update_elements");
 }
 
-// the end of the previous step fused with the start of this one
+// the end of the previous step fused with the start of this one (runs
+// without temperature: no energy hook sits between the two)
 int op_fused(snac_gpu* h) {
     Fields F = fields(h);
     Config c = h->cfg;
     c.time_step_zero = 0;
-    if (h->temperature) {
-        switch (h->constitutive) {
-            case SNAC_RHEOLOGY_MAXWELL: launch_fused_heat<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
-            default: launch_fused_heat<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
-        }
-    } else {
-        switch (h->constitutive) {
-            case SNAC_RHEOLOGY_ELASTIC: launch_fused<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
-            case SNAC_RHEOLOGY_PLASTIC: launch_fused<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
-            case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
-            case SNAC_RHEOLOGY_MAXWELL: launch_fused<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
-        }
+    switch (h->constitutive) {
+        case SNAC_RHEOLOGY_ELASTIC: launch_fused<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_PLASTIC: launch_fused<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_MAXWELL: launch_fused<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
     }
     h->launches++;
     h->time_step++;
-    return launch_check_named(h, h->temperature ? "k_fused_heat" : "k_fused_step");
+    return launch_check_named(h, "k_fused_step");
 }
 
 int op_min_length_scale_sync(snac_gpu* h) {
@@ -394,17 +408,19 @@ int op_begin(snac_gpu* h) {
 // update is pending (fused), otherwise the step starts from scratch.
 int record_step(snac_gpu* h, bool fused) {
     int rc;
-    if (fused) {
-        if ((rc = op_fused(h))) return rc;
+    if (fused && h->temperature) {
+        // heat flux (opens the step), temperature update, then the pending
+        // element update fused with the stress update
+        if ((rc = op_energy_elements(h, 1))) return rc;
+        if ((rc = op_energy_nodes(h))) return rc;
+        if ((rc = op_fused_stress(h))) return rc;
+    } else if (fused) {
+        if ((rc = op_fused(h))) return rc;  // element update + stress update
     } else {
         if ((rc = op_begin(h))) return rc;
         if ((rc = op_energy_elements(h))) return rc;
-    }
-    if ((rc = op_energy_nodes(h))) return rc;
-    if (fused && !h->temperature) {
-        // stress already updated by the fused kernel
-    } else if ((rc = op_calc_stresses(h))) {
-        return rc;
+        if ((rc = op_energy_nodes(h))) return rc;
+        if ((rc = op_calc_stresses(h))) return rc;
     }
     if ((rc = op_loop_nodes(h))) return rc;
     return op_min_length_scale_sync(h);

@@ -605,9 +605,10 @@ __device__ __forceinline__ void element_update_tet(const Fields& F, const Config
 // same geometry and velocities): one geometry evaluation, one stress
 // read-modify-write.  Used when no energy hook sits between the two.
 template <int PLUGIN, bool ONE>
-__device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
+__device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb,
+                                                  bool count_step = true) {
     TetSlot s = tet_slot(m, lb);
-    if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
+    if (count_step && lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
         F.sc->time_step += 1;
         F.sc->current_time += F.sc->dt;
     }
@@ -624,6 +625,15 @@ __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F
 template <int PLUGIN, bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
     k_fused_step_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
+}
+
+// Temperature runs: the element update of step n is deferred past the heat
+// flux and temperature update of step n+1 (neither reads the stress) into
+// the stress kernel of step n+1, which recomputes the same geometry anyway;
+// the step counters were advanced by the heat-flux kernel.
+template <int PLUGIN, bool ONE>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_stress(Mesh m, Fields F, Config cfg) {
+    k_fused_step_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x, false);
 }
 
 // ======================================================================================
@@ -996,8 +1006,10 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
         h[4 * R] = M.heat_capacity * ((rho)*g.V) / 8.0f;
         if (cfg.thermal_stress) h[5 * R] = tsr;
-        if (s.t == 0) {
-            // Heat.c:127-135, once per element
+        // Heat.c:127-135, once per element; with one phase every element
+        // gives the same value, so only element 0 (the first the reference
+        // checks) evaluates it
+        if (s.t == 0 && (!ONE || s.e == 0)) {
             double dt_thermal_to_mech = sqrt((M.lambda + 2.0f * M.mu) / M.density) * F.sc->min_length_scale /
                                         (M.thermal_conduct / (M.heat_capacity * M.density));
             if (!(dt_thermal_to_mech > 1.0)) report(F.sc, SNAC_GPU_EPHYSICS, s.e);
@@ -1017,7 +1029,12 @@ __device__ __forceinline__ void k_heat_flux_body(const Mesh& m, const Fields& F,
 }
 
 template <bool ONE>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg) {
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg,
+                                                                           int count_step) {
+    if (count_step && blockIdx.x == 0 && threadIdx.x == 0) {  // the step's first kernel: timeStep++, currentTime += dt
+        F.sc->time_step += 1;
+        F.sc->current_time += F.sc->dt;
+    }
     k_heat_flux_body<ONE>(m, F, cfg, blockIdx.x);
 }
 
