@@ -1233,10 +1233,13 @@ int record_batch_step(snac_gpu_batch* b, bool fused, int parity) {
             return rc;
     }
     if ((rc = blaunch_nodes<BOP_HEAT_NODES>(b, D, b->node_temp, b->tune.node_threads))) return rc;
-    if (by_class)
-        rc = blaunch_elem_classes<BOP_STRESS>(b, D, fused);
+    // temperature models: after the energy hooks, the pending element update
+    // fused with the stress update (fused step) or the stress update alone
+    if (fused)
+        rc = by_class ? blaunch_elem_classes<BOP_FUSED_STRESS>(b, D, true)
+                      : blaunch_elem<BOP_FUSED_STRESS>(b, D, b->elem_temp);
     else
-        rc = blaunch_elem<BOP_STRESS>(b, D, fused ? b->elem_temp : b->elem_all);
+        rc = by_class ? blaunch_elem_classes<BOP_STRESS>(b, D, false) : blaunch_elem<BOP_STRESS>(b, D, b->elem_all);
     if (rc) return rc;
     if ((rc = blaunch_nodes<BOP_LOOP_NODES>(b, D, b->node_all, b->tune.node_threads))) return rc;
     // the node loop wrote the new coordinates into the other buffer

@@ -32,7 +32,18 @@ struct ModelStatus {
     long long time_step;
 };
 
-enum { BOP_FUSED = 0, BOP_HEAT_FLUX = 1, BOP_STRESS = 2, BOP_LOOP_NODES = 3, BOP_HEAT_NODES = 4, BOP_MINLS = 5 };
+// BOP_FUSED: the step's first element launch (models without temperature:
+// pending element update + stress update; with temperature: the heat flux,
+// the element update waiting for BOP_FUSED_STRESS after the energy hooks)
+enum {
+    BOP_FUSED = 0,
+    BOP_HEAT_FLUX = 1,
+    BOP_STRESS = 2,
+    BOP_LOOP_NODES = 3,
+    BOP_HEAT_NODES = 4,
+    BOP_MINLS = 5,
+    BOP_FUSED_STRESS = 6
+};
 
 __device__ __forceinline__ void load_desc(ModelDesc& dst, const ModelDesc* __restrict__ src) {
     constexpr int W = sizeof(ModelDesc) / 8;
@@ -44,11 +55,11 @@ __device__ __forceinline__ void load_desc(ModelDesc& dst, const ModelDesc* __res
 // the element bodies for a tile's model: phase 0 from the descriptor (in
 // shared memory) when the model has one phase, else the model's phase table
 template <int P>
-__device__ __forceinline__ void fused_step_any(const ModelDesc& md, int lb) {
+__device__ __forceinline__ void fused_step_any(const ModelDesc& md, int lb, bool count_step = true) {
     if (md.F.mat)
-        k_fused_step_body<P, false>(md.m, md.F, md.cfg, lb);
+        k_fused_step_body<P, false>(md.m, md.F, md.cfg, lb, count_step);
     else
-        k_fused_step_body<P, true>(md.m, md.F, md.cfg, lb);
+        k_fused_step_body<P, true>(md.m, md.F, md.cfg, lb, count_step);
 }
 template <int P>
 __device__ __forceinline__ void calc_stresses_any(const ModelDesc& md, int lb) {
@@ -58,18 +69,20 @@ __device__ __forceinline__ void calc_stresses_any(const ModelDesc& md, int lb) {
         k_calc_stresses_body<P, true>(md.m, md.F, md.cfg, lb);
 }
 
-template <int P>
-__device__ __forceinline__ void fused_heat_any(const ModelDesc& md, int lb) {
-    if (md.F.mat)
-        k_fused_heat_body<P, false>(md.m, md.F, md.cfg, lb);
-    else
-        k_fused_heat_body<P, true>(md.m, md.F, md.cfg, lb);
-}
 __device__ __forceinline__ void heat_flux_any(const ModelDesc& md, int lb) {
     if (md.F.mat)
         k_heat_flux_body<false>(md.m, md.F, md.cfg, lb);
     else
         k_heat_flux_body<true>(md.m, md.F, md.cfg, lb);
+}
+// a temperature model's first launch of a fused step: timeStep++,
+// currentTime += dt (once per model), then the heat flux
+__device__ __forceinline__ void heat_flux_opening_any(const ModelDesc& md, int lb) {
+    if (lb == 0 && threadIdx.x == 0) {
+        md.F.sc->time_step += 1;
+        md.F.sc->current_time += md.F.sc->dt;
+    }
+    heat_flux_any(md, lb);
 }
 
 // Element-tile kernels: the fused end-of-step/next-stress kernel (or its
@@ -86,10 +99,7 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
         const int P = md.cfg.constitutive;
         if (OP == BOP_FUSED) {
             if (md.cfg.temperature) {
-                if (P == SNAC_RHEOLOGY_MAXWELL)
-                    fused_heat_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y);
-                else
-                    fused_heat_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y);
+                heat_flux_opening_any(md, t.y);
             } else {
                 switch (P) {
                     case SNAC_RHEOLOGY_ELASTIC: fused_step_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y); break;
@@ -99,6 +109,15 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
                         break;
                     default: fused_step_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y); break;
                 }
+            }
+        } else if (OP == BOP_FUSED_STRESS) {
+            switch (P) {
+                case SNAC_RHEOLOGY_ELASTIC: fused_step_any<SNAC_RHEOLOGY_ELASTIC>(md, t.y, false); break;
+                case SNAC_RHEOLOGY_PLASTIC: fused_step_any<SNAC_RHEOLOGY_PLASTIC>(md, t.y, false); break;
+                case SNAC_RHEOLOGY_VISCOPLASTIC:
+                    fused_step_any<SNAC_RHEOLOGY_VISCOPLASTIC>(md, t.y, false);
+                    break;
+                default: fused_step_any<SNAC_RHEOLOGY_MAXWELL>(md, t.y, false); break;
             }
         } else if (OP == BOP_STRESS) {
             switch (P) {
@@ -129,9 +148,11 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB)
         __syncthreads();
         if (OP == BOP_FUSED) {
             if (TEMP)
-                fused_heat_any<P == SNAC_RHEOLOGY_MAXWELL ? SNAC_RHEOLOGY_MAXWELL : SNAC_RHEOLOGY_ELASTIC>(md, t.y);
+                heat_flux_opening_any(md, t.y);
             else
                 fused_step_any<P>(md, t.y);
+        } else if (OP == BOP_FUSED_STRESS) {
+            fused_step_any<P>(md, t.y, false);
         } else if (OP == BOP_STRESS) {
             calc_stresses_any<P>(md, t.y);
         } else {

@@ -8,8 +8,9 @@
 //   k_update_elements Snac_EP_LoopElementsMomentum UpdateElement.c
 //   k_sync           AbstractContext_EP_Sync     Context.c:1208-1268
 // In a steady step the element update of step n runs fused with the stress
-// update of step n+1 (k_fused_step, or k_fused_heat + k_calc_stresses), and
-// the minimum length scale of the element update runs fused with Sync
+// update of step n+1 (k_fused_step; with temperature k_heat_flux, k_heat_nodes,
+// then k_fused_stress, since neither energy hook reads the stress), and the
+// minimum length scale of the element update runs fused with Sync
 // (k_min_length_scale_sync).
 //
 // Element kernels run one thread per tetrahedron: a warp holds three
@@ -1038,32 +1039,6 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(M
     k_heat_flux_body<ONE>(m, F, cfg, blockIdx.x);
 }
 
-// End of step n (element update) fused with the heat flux of step n+1: both
-// need the geometry of the same coordinates.
-template <int PLUGIN, bool ONE>
-__device__ __forceinline__ void k_fused_heat_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
-    TetSlot s = tet_slot(m, lb);
-    if (lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
-        F.sc->time_step += 1;
-        F.sc->current_time += F.sc->dt;
-    }
-    V3 c[4], v[4];
-    double T[4], T0[4];
-    load_tet(m, F, s, c, v, T, T0);
-    TetGeom g;
-    tet_geometry(c, g);
-    double st[6];
-    element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
-    if (s.active) {
-        store_stress(F, s.q, st);
-    }
-    heat_flux_tet<ONE>(m, F, cfg, s, T, T0, g);
-}
-
-template <int PLUGIN, bool ONE>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_heat(Mesh m, Fields F, Config cfg) {
-    k_fused_heat_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
-}
 
 // ======================================================================================
 // Snac_EP_LoopNodesEnergy: Snac_Heat for every node (temperature/Heat.c:64-140),
