@@ -43,6 +43,17 @@ NODES_PER_HEX = {"c1": 2601 / 2048, "c2": 139425 / 131072, "c3": 1081665 / 10485
 # ncu capture of that kernel on the same workload
 # (profiles/k_fused_step_plastic_64x32x64.md); None where none was taken.
 NCU_TRAFFIC = {("c2", "k_fused_step"): 83.648000e6 + 167.135744e6}
+# what bounds the dominant kernel instead of HBM, from the same kind of ncu
+# capture (fractions of peak; profiles/k_fused_step_plastic_64x32x64.md,
+# profiles/k_fused_stress_viscoplastic_128x64x128.md)
+NCU_PIPES = {("c2", "k_fused_step"): {"fp64_pipe": 0.383, "issue_active": 0.455, "dram_throughput": 0.179},
+             ("c3", "k_fused_stress"): {"fp64_pipe": 0.374, "dram_throughput": 0.188}}
+ARITHMETIC = {
+    "c1": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
+    "c2": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
+    "c3": "reference operation order without FMA contraction; the Arrhenius viscosity's device log/exp differ "
+          "from the reference's libm pow*exp in the last bits (checked against the CPU oracle at 1e-6)",
+}
 
 
 def algorithmic_bytes(workload: str) -> float:
@@ -337,10 +348,10 @@ def run_ours(args, ws, rank, local):
             "config": {"workload": workload_name(args.workload), "hex": ne, "tets": ne * 10, "nodes": cfg.n_nodes,
                        "l2": "512 MiB flush written between timed steps",
                        "parallelism": "replicas" if ws > 1 else "single model",
-                       "arithmetic": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle"},
+                       "arithmetic": ARITHMETIC[args.workload]},
             "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
                          "frac": achieved_kernel / peak, "traffic": NCU_TRAFFIC.get((args.workload, top)),
-                         "kernel": top,
+                         "kernel": top, "ncu_pipes": NCU_PIPES.get((args.workload, top)),
                          "kernel_ms": kern_ms[top], "algorithmic_bytes_per_hex": kb,
                          "peak_source": peak_kind,
                          "step": {"achieved": achieved_step, "frac": achieved_step / peak,
