@@ -172,6 +172,11 @@ def replica_throughput(ws: int, units_per_rank: float, seconds_this_rank: float)
 
 
 # ---------------------------------------------------------------------------------------------
+# steps of the one-core CPU sample: about 15 s of the reference's sources on
+# one host core (measured rates: C1 0.71 M, C2 0.16 M, C3 0.117 M hex-steps/s)
+CPU_STEPS = {"c1": 5000, "c2": 20, "c3": 2}
+
+
 def cpu_sample(workload: str, steps: int, kind: str):
     """Time the CPU checker on `steps` SNAC steps of the full workload (one core)."""
     from oracle.pyoracle import Checker, available
@@ -334,9 +339,10 @@ def run_ours(args, ws, rank, local):
     if rank == 0 and not args.no_cpu:
         from oracle.pyoracle import available
         kind = "reference" if available("reference") else "port"
-        v, kind, dt = cpu_sample(args.workload, args.cpu_steps, kind)
+        nsteps = args.cpu_steps or CPU_STEPS[args.workload]
+        v, kind, dt = cpu_sample(args.workload, nsteps, kind)
         cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": f"{args.cpu_steps} SNAC steps of the full {args.workload} mesh ({ne} hex) on one host core, "
+               "sample": f"{nsteps} SNAC steps of the full {args.workload} mesh ({ne} hex) on one host core, "
                          f"{dt:.1f} s"}
 
     if rank == 0:
@@ -466,11 +472,11 @@ def run_ensemble(args, ws, rank, local):
             ck = Checker(c, kind)
             ck.time_step_zero()
             t0 = time.perf_counter()
-            ck.step(2)
+            ck.step(16)
             t += time.perf_counter() - t0
-            hexsteps += 2 * c.n_elements
+            hexsteps += 16 * c.n_elements
         cpu = {"value": hexsteps / t, "unit": UNIT, "cores": 1, "kind": kind,
-               "sample": f"2 SNAC steps of each of the first 8 ensemble models ({hexsteps // 2} hex) on one host core, "
+               "sample": f"16 SNAC steps of each of the first 8 ensemble models ({hexsteps // 16} hex) on one host core, "
                          f"{t:.1f} s"}
     b.close()
     if rank == 0:
@@ -623,7 +629,7 @@ def main():
     ap.add_argument("--adj-fd", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=10)
+    ap.add_argument("--cpu-steps", type=int, default=0, help="0: a sample of 10-20 s of one host core per workload")
     ap.add_argument("--cpu-procs", type=int, default=32)
     args = ap.parse_args()
     if args.warmup < 3:
