@@ -108,6 +108,7 @@ struct DevScalars {
     int status;                      // first error (SNAC_GPU_E*), 0 if none
     long long err_index;
     long long launches;
+    double inertial_density0;        // (lambda + 2 mu) / c^2 of phase 0 at the current speed of sound c (dynamic dt)
     unsigned blocks_done;            // blocks of k_min_length_scale_sync finished (0 between launches)
     unsigned pad;
 };

@@ -531,7 +531,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
             const double sos = F.sc->speed_of_sound;
-            const double inertialDensity = dv(M.lambda + 2.0f * M.mu, sos * sos);
+            const double inertialDensity = ONE ? F.sc->inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
             F.fmass[qt] = factor4 * inertialDensity * gf.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
@@ -1099,6 +1099,8 @@ __device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, doub
     if (cfg.dt_type == SNAC_DT_DYNAMIC) {
         sc->dt = minLS * 0.45f * cfg.strain_inert / vmax;
         sc->speed_of_sound = minLS * 0.5f / sc->dt;
+        // Force.c:112-114 for phase 0, once per step instead of once per tet
+        sc->inertial_density0 = dv(cfg.m0.lambda + 2.0f * cfg.m0.mu, sc->speed_of_sound * sc->speed_of_sound);
     } else if (cfg.dt_type == SNAC_DT_WAVE) {
         sc->speed_of_sound = wave_speed;
         sc->dt = 0.5f * minLS / sc->speed_of_sound;
