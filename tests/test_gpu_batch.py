@@ -89,6 +89,20 @@ def test_launch_shape_does_not_change_results(tuning):
             assert_same(m.state(), ref[i][0], f"model {i} {tuning}")
 
 
+def test_batch_with_per_element_phases_bitwise():
+    """A two-phase model (per-element phase table, density coupling) batched
+    with one-phase models: the phase-table path of the batch kernels gives
+    the single-model bits."""
+    from tests import scenarios as S
+    cfgs = [S.CASES["density"][0](), S.CASES["plastic"][0](), S.CASES["viscoplastic"][0]()]
+    ref = singles(cfgs, 6)
+    with SnacBatch(cfgs) as b:
+        b.time_step_zero()
+        b.step(6)
+        for i, m in enumerate(b.models):
+            assert_same(m.state(), ref[i][0], f"model {i}")
+
+
 def test_step_each_equals_batched():
     cfgs = small_ensemble(5, seed=8)
     with SnacBatch(cfgs) as a, SnacBatch(cfgs) as b:
