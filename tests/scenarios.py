@@ -87,6 +87,16 @@ def two_phase_density(nx=6, ny=4, nz=6):
     return cfg
 
 
+def plastic_two_phase(nx=8, ny=4, nz=8):
+    """The yielding plastic case with two Mohr-Coulomb phases (different
+    cohesion and softening) assigned per element: the phase-table path."""
+    cfg = plastic_small(nx, ny, nz)
+    cfg.materials = [W.mc_phase(c0=2.0e5, c1=2.0e4, eps1=0.001), W.mc_phase(c0=4.0e5, c1=1.0e5, eps1=0.002)]
+    rng = np.random.default_rng(13)
+    cfg.element_material = rng.integers(0, 2, cfg.n_elements).astype(np.int32)
+    return cfg
+
+
 def constant_dt(cfg: SnacConfig, dt: float) -> SnacConfig:
     cfg.dtType = "constant"
     cfg.timeStep = dt
@@ -126,4 +136,5 @@ CASES = {
     "traction": (traction_small, 60),
     "topo": (topo_small, 60),
     "density": (two_phase_density, 40),
+    "plastic_phases": (plastic_two_phase, 120),
 }

@@ -49,7 +49,7 @@ def assert_bitwise(g, c):
     assert a.time_step == b.time_step
 
 
-@pytest.mark.parametrize("case", ["elastic", "plastic", "lithostatic", "winkler", "traction", "topo"])
+@pytest.mark.parametrize("case", ["elastic", "plastic", "plastic_phases", "lithostatic", "winkler", "traction", "topo"])
 def test_bitwise_equal_to_oracle(case):
     make, steps = S.CASES[case]
     g, c = run_both(make(), steps, chunks=2)
