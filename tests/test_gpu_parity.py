@@ -264,14 +264,16 @@ def test_step_before_step_zero_is_refused():
 # ---- full-size configurations: bounded CPU comparisons and size-free properties ------------
 
 def test_c2_full_size_first_steps_bitwise():
-    """The Mohr-Coulomb plastic workload at full size (64 x 32 x 64): three steps against the oracle."""
-    g, c = run_both(W.c2_plastic(), 3)
+    """The Mohr-Coulomb plastic workload at full size (64 x 32 x 64): twelve steps
+    (step one unfused, then the graph-captured fused steps) against the oracle."""
+    g, c = run_both(W.c2_plastic(), 12)
     assert_bitwise(g, c)
 
 
-def test_c3_full_size_first_step_within_tolerance():
-    """The Maxwell visco-plastic workload at full size (128 x 64 x 128, ~1M hex): one step against the oracle."""
-    g, c = run_both(W.c3_viscoplastic(), 1)
+def test_c3_full_size_first_steps_within_tolerance():
+    """The Maxwell visco-plastic workload at full size (128 x 64 x 128, ~1M hex): three
+    steps (the unfused first step, then the fused temperature step) against the oracle."""
+    g, c = run_both(W.c3_viscoplastic(), 3)
     sg, sc = g.state(), c.state()
     for f in ("velocity", "stress", "viscosity", "temperature"):
         assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, f
