@@ -86,6 +86,28 @@ def test_elastic_c1_full_1000_steps():
     assert np.array_equal(sg.velocity, sc.velocity) and np.array_equal(sg.stress, sc.stress)
 
 
+def test_plastic_1000_steps_bitwise():
+    """The yielding Mohr-Coulomb case over 1000 steps (tension and shear
+    return maps, softening to the residual cohesion): bitwise."""
+    g, c = run_both(S.plastic_small(), 1000, chunks=4)
+    assert np.count_nonzero(c.state().plastic_strain) > 100
+    assert_bitwise(g, c)
+
+
+def test_viscoplastic_1000_steps_within_tolerance():
+    """The visco-plastic physics away from yielding over 1000 steps: the
+    device viscosity's last-bit differences from the host libm stay below
+    1e-9 (measured: 7e-11 in velocity, 6e-14 in stress).  Where tets yield
+    and soften, the return map's branch decisions amplify such differences
+    (measured on the yielding case: 2e-7 after 300 steps, ~1e-3 after 400,
+    with pow*exp or exp of logs alike), which is why the target states its
+    plastic tolerance away from bifurcation."""
+    g, c = run_both(S.viscoplastic_small(active=False), 1000, chunks=4)
+    sg, sc = g.state(), c.state()
+    for f in ("velocity", "stress"):
+        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, (f, relerr(getattr(sg, f), getattr(sc, f)))
+
+
 @pytest.mark.parametrize("dt_type", ["constant", "wave"])
 def test_other_dt_types_bitwise(dt_type):
     cfg = S.elastic_small(6, 4, 6)
