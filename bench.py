@@ -172,6 +172,20 @@ def replica_throughput(ws: int, units_per_rank: float, seconds_this_rank: float)
 
 
 # ---------------------------------------------------------------------------------------------
+def host_info() -> dict:
+    """The host the CPU figures were taken on: logical CPUs and the model name."""
+    model = None
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"nproc": os.cpu_count(), "cpu_model": model}
+
+
 # steps of the one-core CPU sample: about 15 s of the reference's sources on
 # one host core (measured rates: C1 0.71 M, C2 0.16 M, C3 0.117 M hex-steps/s)
 CPU_STEPS = {"c1": 5000, "c2": 20, "c3": 2}
@@ -227,7 +241,7 @@ def run_reference(args, ws, rank):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded, snac_b200/workloads.py)",
         "config": {"workload": workload_name(args.workload), "hex": ne, "cpu_processes": procs},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind,
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "host": host_info(),
                          "sample": f"each step: {procs} processes x 1 SNAC step of the full {args.workload} mesh "
                                    f"(includes per-process model construction)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -341,7 +355,7 @@ def run_ours(args, ws, rank, local):
         kind = "reference" if available("reference") else "port"
         nsteps = args.cpu_steps or CPU_STEPS[args.workload]
         v, kind, dt = cpu_sample(args.workload, nsteps, kind)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": kind,
+        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": kind, "host": host_info(),
                "sample": f"{nsteps} SNAC steps of the full {args.workload} mesh ({ne} hex) on one host core, "
                          f"{dt:.1f} s"}
 
@@ -475,7 +489,7 @@ def run_ensemble(args, ws, rank, local):
             ck.step(16)
             t += time.perf_counter() - t0
             hexsteps += 16 * c.n_elements
-        cpu = {"value": hexsteps / t, "unit": UNIT, "cores": 1, "kind": kind,
+        cpu = {"value": hexsteps / t, "unit": UNIT, "cores": 1, "kind": kind, "host": host_info(),
                "sample": f"16 SNAC steps of each of the first 8 ensemble models ({hexsteps // 16} hex) on one host core, "
                          f"{t:.1f} s"}
     b.close()
