@@ -390,7 +390,6 @@ def run_ours(args, ws, rank, local):
 # Algorithmic bytes per hex of one launch of each kernel (state it must read / write once).
 KERNEL_BYTES = {
     "k_fused_step": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0),
-    "k_fused_heat": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + 8.0 * NODES_PER_HEX[w],
     "k_calc_stresses": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
                                  + (8.0 * NODES_PER_HEX[w] if w == "c3" else 0.0),
     "k_fused_stress": lambda w: 960.0 + 48.0 * NODES_PER_HEX[w] + (160.0 + 8.0 if w != "c1" else 0.0)
