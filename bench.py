@@ -350,7 +350,7 @@ def run_ours(args, ws, rank, local):
                        "snac_gpu_download of the state"}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
         from oracle.pyoracle import available
         kind = "reference" if available("reference") else "port"
         nsteps = args.cpu_steps or CPU_STEPS[args.workload]
@@ -475,7 +475,7 @@ def run_ensemble(args, ws, rank, local):
                        "snac_gpu_batch_step(1), snac_gpu_download of every model's state"}
 
     cpu = None
-    if rank == 0 and not args.no_cpu:
+    if rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
         from oracle.pyoracle import Checker, available
         kind = "reference" if available("reference") else "port"
         sample = cfgs[:8]
