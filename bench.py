@@ -1,6 +1,6 @@
 """Benchmark of the SNAC explicit step on B200 (one JSON line on stdout).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c1|c3|ensemble|adjoint]
     python bench.py --impl reference ...      # the reference's CPU code on the host cores
 
 A "step" is one _AbstractContext_Step of the model (Solve + Sync) over the
@@ -14,6 +14,15 @@ recorded on the library's own stream; barrier + synchronize around the timed
 region; the max over ranks is taken.  With --gpus N (torchrun) every rank
 advances its own replica of the model (the single-model path is not
 sharded): value = all ranks' element-steps / slowest rank's time.
+
+At N = 1 the default line also carries the metric's other forms under
+"forms": the largest plain model (c3, 128 x 64(y) x 128 hex), the batched
+ensemble of 256 models against the same models one launch each, and the
+adjoint's cost in forward runs with its finite-difference agreement.
+
+--impl reference times the reference's own hot-path C sources
+(oracle/_ref/libsnacref_mt.so: element and node loops on every host CPU,
+bitwise equal to the serial build) on the same model in this process.
 """
 from __future__ import annotations
 
@@ -186,67 +195,101 @@ def host_info() -> dict:
     return {"nproc": os.cpu_count(), "cpu_model": model}
 
 
-# steps of the one-core CPU sample: about 15 s of the reference's sources on
-# one host core (measured rates: C1 0.71 M, C2 0.16 M, C3 0.117 M hex-steps/s)
-CPU_STEPS = {"c1": 5000, "c2": 20, "c3": 2}
+def host_threads() -> int:
+    """Host CPUs this process may run on."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
 
 
-def cpu_sample(workload: str, steps: int, kind: str):
-    """Time the CPU checker on `steps` SNAC steps of the full workload (one core)."""
-    from oracle.pyoracle import Checker, available
-    if kind == "reference" and not available("reference"):
-        kind = "port"
+def cpu_checker_kind(threads: int) -> str:
+    """The reference's own sources when they were compiled here (threaded
+    build for more than one thread), else the restatement."""
+    from oracle.pyoracle import available
+    if threads > 1 and available("reference_mt"):
+        return "reference_mt"
+    return "reference" if available("reference") else "port"
+
+
+def cpu_sample(workload: str, threads: int, seconds: float, max_steps: int = 100000):
+    """Time the CPU checker on whole SNAC steps of the full workload: the model
+    is built and taken through step zero once, then stepped one step at a
+    time until `seconds` have passed.  Returns (element-steps/s, kind,
+    threads used, steps, seconds)."""
+    from oracle.pyoracle import Checker
+    kind = cpu_checker_kind(threads)
     cfg = make_workload(workload)
-    ck = Checker(cfg, kind)
+    ck = Checker(cfg, kind, threads=threads)
     ck.time_step_zero()
-    t = time.perf_counter()
-    ck.step(steps)
-    dt = time.perf_counter() - t
-    return cfg.n_elements * steps / dt, kind, dt
-
-
-def _cpu_worker(args):
-    workload, steps, kind = args
-    return cpu_sample(workload, steps, kind)
+    ck.step(1)  # first step outside the sample (page-in of the state)
+    n, t = 0, 0.0
+    while n < max_steps and t < seconds:
+        t0 = time.perf_counter()
+        rc = ck.step(1)
+        t += time.perf_counter() - t0
+        n += 1
+        if rc != 0:
+            raise RuntimeError(f"CPU checker step failed: {ck.last_error()}")
+    used = ck.threads
+    ck.close()
+    return cfg.n_elements * n / t, ("reference" if kind.startswith("reference") else "port"), used, n, t
 
 
 def run_reference(args, ws, rank):
-    """--impl reference: the reference's own hot-path C code (oracle/_ref, or
-    the port when the reference could not be compiled) on the host cores, one
-    independent model copy per process (the reference is single-threaded and
-    not thread-safe)."""
+    """--impl reference: the reference's own hot-path C sources (oracle/_ref,
+    the threaded build libsnacref_mt.so: the element and node loops of the
+    driver on every host CPU, bitwise equal to the serial build; the
+    restatement when the reference could not be compiled) on the same
+    workload, in this process.  The model is built and taken through step
+    zero once; W warm-up steps, then K steps each timed alone.  Only rank 0
+    runs; the other ranks exit without work."""
     if rank != 0:
         return
-    import multiprocessing as mp
-    from oracle.pyoracle import available
-    kind = "reference" if available("reference") else "port"
-    cfg = make_workload(args.workload)
-    ne = cfg.n_elements
-    ncpu = os.cpu_count() or 1
-    procs = max(1, min(ncpu, args.cpu_procs))
-    ctx = mp.get_context("spawn")
-    per_step = []
-    with ctx.Pool(procs) as pool:
-        for s in range(args.warmup + args.steps):
-            t = time.perf_counter()
-            res = pool.map(_cpu_worker, [(args.workload, 1, kind)] * procs)
-            dt = time.perf_counter() - t
-            if s >= args.warmup:
-                per_step.append(dt)
+    try:
+        from oracle.pyoracle import Checker
+        threads = host_threads()
+        kind = cpu_checker_kind(threads)
+        w = args.workload if args.workload in ("c1", "c2", "c3") else "c2"
+        cfg = make_workload(w)
+        ne = cfg.n_elements
+        ck = Checker(cfg, kind, threads=threads)
+        if ck.time_step_zero() != 0:
+            raise RuntimeError(f"step zero failed: {ck.last_error()}")
+        if ck.step(args.warmup) != 0:
+            raise RuntimeError(f"warm-up failed: {ck.last_error()}")
+        per_step = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            rc = ck.step(1)
+            per_step.append(time.perf_counter() - t0)
+            if rc != 0:
+                raise RuntimeError(f"step failed: {ck.last_error()}")
+        used = ck.threads
+        ck.close()
+    except Exception as exc:  # one line either way, never a hang
+        print(json.dumps({"impl": "reference", "unavailable": f"CPU reference run failed: {exc}"}), flush=True)
+        return
     total = sum(per_step)
-    value = procs * ne * args.steps / total
+    value = ne * args.steps / total
+    kind_out = "reference" if kind.startswith("reference") else "port"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic (seeded, snac_b200/workloads.py)",
-        "config": {"workload": workload_name(args.workload), "hex": ne, "cpu_processes": procs},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": procs, "kind": kind, "host": host_info(),
-                         "sample": f"each step: {procs} processes x 1 SNAC step of the full {args.workload} mesh "
-                                   f"(includes per-process model construction)"},
+        "config": {"workload": workload_name(w), "hex": ne, "tets": ne * 10, "nodes": cfg.n_nodes,
+                   "parallelism": f"one model, element and node loops on {used} host threads"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": used, "kind": kind_out, "host": host_info(),
+                         "sample": f"{args.steps} SNAC steps of the full {w} mesh ({ne} hex) after {args.warmup} "
+                                   f"warm-up steps, each timed alone; {os.path.basename(PATHS_CPU[kind])}"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+PATHS_CPU = {"reference_mt": "oracle/_ref/libsnacref_mt.so", "reference": "oracle/_ref/libsnacref.so",
+             "port": "oracle/liboracle.so"}
 
 
 def workload_name(w):
@@ -256,14 +299,16 @@ def workload_name(w):
 
 
 # ---------------------------------------------------------------------------------------------
-def run_ours(args, ws, rank, local):
-    import numpy as np
+def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
+    """One plain model (c1 / c2 / c3): device-timed steps, the per-kernel
+    breakdown and roofline, e2e through the C ABI, the CPU sample.  Returns
+    the JSON line (rank 0) or None."""
     import torch
     from snac_b200.context import SnacContext
 
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
-    cfg = make_workload(args.workload)
+    cfg = make_workload(workload)
     ne = cfg.n_elements
     ctx = SnacContext(cfg)
     ctx.time_step_zero()
@@ -306,15 +351,15 @@ def run_ours(args, ws, rank, local):
     kern_ms = {k: statistics.mean(v) for k, v in kern.items()}
     top = max(kern_ms, key=kern_ms.get)
     peak, peak_kind = load_peaks()
-    alg = algorithmic_bytes(args.workload)
+    alg = algorithmic_bytes(workload)
     step_ms_mean = 1e3 * t_dev / args.steps
     achieved_step = alg * ne / (step_ms_mean / 1e3) / 1e9
-    kb = KERNEL_BYTES.get(top, lambda w: alg)(args.workload)
+    kb = KERNEL_BYTES.get(top, lambda w: alg)(workload)
     achieved_kernel = kb * ne / (kern_ms[top] / 1e3) / 1e9
 
     # ---- end to end through the C ABI with host buffers --------------------------------
     e2e = None
-    if not args.no_e2e:
+    if with_e2e and not args.no_e2e:
         from snac_b200.abi import State
         st = ctx.state()
         fields = ["coord", "velocity", "stress", "plastic_strain"]
@@ -349,15 +394,10 @@ def run_ours(args, ws, rank, local):
                "note": "per step: snac_gpu_upload of the state from pinned host buffers, snac_gpu_step(1), "
                        "snac_gpu_download of the state"}
 
+    ctx.close()
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
-        from oracle.pyoracle import available
-        kind = "reference" if available("reference") else "port"
-        nsteps = args.cpu_steps or CPU_STEPS[args.workload]
-        v, kind, dt = cpu_sample(args.workload, nsteps, kind)
-        cpu = {"value": v, "unit": UNIT, "cores": 1, "kind": kind, "host": host_info(),
-               "sample": f"{nsteps} SNAC steps of the full {args.workload} mesh ({ne} hex) on one host core, "
-                         f"{dt:.1f} s"}
+    if with_cpu and rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
+        cpu = cpu_baseline(workload, ne, args)
 
     if rank == 0:
         line = {
@@ -365,13 +405,13 @@ def run_ours(args, ws, rank, local):
             "warmup": args.warmup, "ms_per_step": step_ms_mean, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded, snac_b200/workloads.py)",
-            "config": {"workload": workload_name(args.workload), "hex": ne, "tets": ne * 10, "nodes": cfg.n_nodes,
+            "config": {"workload": workload_name(workload), "hex": ne, "tets": ne * 10, "nodes": cfg.n_nodes,
                        "l2": "512 MiB flush written between timed steps",
                        "parallelism": "replicas" if ws > 1 else "single model",
-                       "arithmetic": ARITHMETIC[args.workload]},
+                       "arithmetic": ARITHMETIC[workload]},
             "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
-                         "frac": achieved_kernel / peak, "traffic": NCU_TRAFFIC.get((args.workload, top)),
-                         "kernel": top, "ncu_pipes": NCU_PIPES.get((args.workload, top)),
+                         "frac": achieved_kernel / peak, "traffic": NCU_TRAFFIC.get((workload, top)),
+                         "kernel": top, "ncu_pipes": NCU_PIPES.get((workload, top)),
                          "kernel_ms": kern_ms[top], "algorithmic_bytes_per_hex": kb,
                          "peak_source": peak_kind,
                          "step": {"achieved": achieved_step, "frac": achieved_step / peak,
@@ -383,8 +423,20 @@ def run_ours(args, ws, rank, local):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
-    ctx.close()
+        return line
+    return None
+
+
+def cpu_baseline(workload: str, ne: int, args) -> dict:
+    """The reference's own sources on the host: all host threads (the
+    headline CPU figure) and one core, each a time-boxed sample of whole
+    steps of the full mesh."""
+    v, kind, used, n, t = cpu_sample(workload, host_threads(), args.cpu_seconds)
+    v1, _, _, n1, t1 = cpu_sample(workload, 1, args.cpu_seconds_one)
+    return {"value": v, "unit": UNIT, "cores": used, "kind": kind, "host": host_info(),
+            "sample": f"{n} SNAC steps of the full {workload} mesh ({ne} hex) on {used} host threads "
+                      f"(element and node loops split across them), {t:.1f} s",
+            "one_core": {"value": v1, "unit": UNIT, "steps": n1, "seconds": round(t1, 2)}}
 
 
 # Algorithmic bytes per hex of one launch of each kernel (state it must read / write once).
@@ -400,7 +452,7 @@ KERNEL_BYTES = {
 
 
 # ---------------------------------------------------------------------------------------------
-def run_ensemble(args, ws, rank, local):
+def run_ensemble(args, ws, rank, local, with_e2e=True, with_cpu=True):
     """--workload ensemble: 256 independent plastic / visco-plastic models of
     uneven size advanced together (one launch per kernel type per step),
     against the same models stepped one launch each (each model's own
@@ -447,7 +499,7 @@ def run_ensemble(args, ws, rank, local):
     # end to end: every model's state up from pinned host memory, one batched
     # step, every model's state down, per step
     e2e = None
-    if not args.no_e2e:
+    if with_e2e and not args.no_e2e:
         fields = ["coord", "velocity", "stress", "plastic_strain", "viscosity", "temperature"]
         hosts = []
         for m in b.models:
@@ -475,22 +527,28 @@ def run_ensemble(args, ws, rank, local):
                        "snac_gpu_batch_step(1), snac_gpu_download of every model's state"}
 
     cpu = None
-    if rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
-        from oracle.pyoracle import Checker, available
-        kind = "reference" if available("reference") else "port"
-        sample = cfgs[:8]
+    if with_cpu and rank == 0 and ws == 1 and not args.no_cpu:  # the CPU sample is taken at N = 1 only
+        # the first 8 models one after another, each on all host threads
+        from oracle.pyoracle import Checker
+        threads = host_threads()
+        kind = cpu_checker_kind(threads)
         t = 0.0
         hexsteps = 0
-        for c in sample:
-            ck = Checker(c, kind)
+        used = 1
+        for c in cfgs[:8]:
+            ck = Checker(c, kind, threads=threads)
             ck.time_step_zero()
+            ck.step(1)
             t0 = time.perf_counter()
             ck.step(16)
             t += time.perf_counter() - t0
             hexsteps += 16 * c.n_elements
-        cpu = {"value": hexsteps / t, "unit": UNIT, "cores": 1, "kind": kind, "host": host_info(),
-               "sample": f"16 SNAC steps of each of the first 8 ensemble models ({hexsteps // 16} hex) on one host core, "
-                         f"{t:.1f} s"}
+            used = ck.threads
+            ck.close()
+        cpu = {"value": hexsteps / t, "unit": UNIT, "cores": used,
+               "kind": "reference" if kind.startswith("reference") else "port", "host": host_info(),
+               "sample": f"16 SNAC steps of each of the first 8 ensemble models ({hexsteps // 16} hex), one model "
+                         f"after another on {used} host threads, {t:.1f} s"}
     b.close()
     if rank == 0:
         line = {
@@ -513,7 +571,8 @@ def run_ensemble(args, ws, rank, local):
             "e2e": e2e,
             "cpu_baseline": cpu,
         }
-        print(json.dumps(line), flush=True)
+        return line
+    return None
 
 
 # ---------------------------------------------------------------------------------------------
@@ -628,7 +687,50 @@ def run_adjoint(args, ws, rank, local):
                                                "max": max(fd_short) if fd_short else None}},
             "gpu_launches": int(launches), "wall_s": wall, "clocks": clocks, "e2e": None, "cpu_baseline": None,
         }
-        print(json.dumps(line), flush=True)
+        return line
+    return None
+
+
+def run_forms(args, ws, rank, local) -> dict:
+    """The metric's other forms beside the headline plain model, each on the
+    same GPU in the same run: the largest plain model (c3), the batched
+    ensemble against the same models one launch each, and the adjoint's cost
+    in forward runs with its finite-difference agreement.  A form that fails
+    reports its error instead of ending the run."""
+    import torch
+    forms = {}
+
+    def guarded(name, fn):
+        try:
+            forms[name] = fn()
+        except Exception as exc:  # the headline line is printed either way
+            forms[name] = {"error": f"{type(exc).__name__}: {exc}"}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+
+    def plain_c3():
+        ln = run_plain(args, ws, rank, local, "c3", with_e2e=True, with_cpu=False)
+        return {k: ln[k] for k in ("value", "unit", "ms_per_step", "config", "roofline", "kernels_ms", "gpu_launches",
+                                   "clocks", "e2e")}
+
+    def batched():
+        ln = run_ensemble(args, ws, rank, local, with_e2e=False, with_cpu=False)
+        out = {k: ln[k] for k in ("value", "unit", "ms_per_step", "config", "one_launch_each", "roofline",
+                                  "gpu_launches", "clocks")}
+        out["speedup_of_batched"] = ln["one_launch_each"]["speedup_of_batched"]
+        return out
+
+    def adjoint_form():
+        ln = run_adjoint(args, ws, rank, local)
+        out = {k: ln[k] for k in ("value", "unit", "steps", "ms_per_step", "config", "adjoint", "gpu_launches",
+                                  "clocks")}
+        out["cost_in_forward_runs"] = ln["adjoint"]["cost_in_forward_runs"]
+        return out
+
+    guarded("plain_c3", plain_c3)
+    guarded("batched", batched)
+    guarded("adjoint", adjoint_form)
+    return forms
 
 
 def main():
@@ -638,12 +740,16 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="c2", choices=["c1", "c2", "c3", "ensemble", "adjoint"])
+    ap.add_argument("--no-forms", action="store_true",
+                    help="c2 at N = 1 only: skip the c3, batched and adjoint forms added to the line")
     ap.add_argument("--adj-steps", type=int, default=2000)
     ap.add_argument("--adj-fd", type=int, default=4)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--cpu-steps", type=int, default=0, help="0: a sample of 10-20 s of one host core per workload")
-    ap.add_argument("--cpu-procs", type=int, default=32)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0,
+                    help="time box of the all-threads CPU sample (whole steps)")
+    ap.add_argument("--cpu-seconds-one", type=float, default=5.0,
+                    help="time box of the one-core CPU sample (whole steps)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -654,7 +760,18 @@ def main():
         return
     ws, rank, local = dist_setup()
     try:
-        {"ensemble": run_ensemble, "adjoint": run_adjoint}.get(args.workload, run_ours)(args, ws, rank, local)
+        if args.workload == "ensemble":
+            line = run_ensemble(args, ws, rank, local)
+        elif args.workload == "adjoint":
+            line = run_adjoint(args, ws, rank, local)
+        else:
+            line = run_plain(args, ws, rank, local, args.workload)
+            # the batched and adjoint forms of the metric ride on the default
+            # line; under torchrun every rank skips them alike
+            if args.workload == "c2" and ws == 1 and not args.no_forms:
+                line["forms"] = run_forms(args, ws, rank, local)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
     finally:
         if ws > 1:
             import torch.distributed as dist

@@ -278,8 +278,12 @@ int  snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max);
  *   - Nothing in the staging has to start at zero: each call writes every
  *     staged value before copying it out.
  *   - The first call on each device looks up the staging address
- *     (cudaGetSymbolAddress) with that device current; make that first call
- *     before any stream capture begins.  The handle's device must be current.
+ *     (cudaGetSymbolAddress) with that device current and keeps it for the
+ *     life of the process; make that first call before any stream capture
+ *     begins.  The handle's device must be current.  A cudaDeviceReset
+ *     invalidates that address together with every handle on the device:
+ *     after one, this library must not be used again in the process.
+ *   - snac_gpu_device_bytes of the handle does not change across the call.
  *   - One staging array per device: overlapping calls would race on it, so
  *     the call holds a process-wide lock until its copies have finished
  *     (calls from several threads run one after another).
@@ -292,6 +296,10 @@ long long   snac_gpu_error_index(const snac_gpu* h);   /* element/node id, -1 if
 int  snac_gpu_sizes(const snac_gpu* h, long long* n_elements, long long* n_nodes);
 /* Number of kernels this library launched on the handle since creation. */
 long long snac_gpu_launch_count(const snac_gpu* h);
+/* Device memory the library has allocated for this handle since creation,
+ * in bytes (model state, lazily allocated staging, output and adjoint
+ * buffers); it never decreases before snac_gpu_destroy. */
+int  snac_gpu_device_bytes(const snac_gpu* h, long long* bytes);
 /* The handle's cudaStream_t, as a void* (for event timing by callers). */
 void* snac_gpu_stream(snac_gpu* h);
 int  snac_gpu_device_count(void);

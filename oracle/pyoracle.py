@@ -6,6 +6,11 @@ bench.py's CPU-baseline leg, never by the snac_b200 package.
   Checker("port")       oracle/liboracle.so, the plain-C restatement
   Checker("reference")  oracle/_ref/libsnacref.so, the reference's own
                         hot-path sources compiled against oracle/refshim
+  Checker("reference_mt", threads=n)
+                        oracle/_ref/libsnacref_mt.so, the same sources with
+                        the driver's element and node loops on n threads
+                        (bitwise equal to "reference"): the all-cores CPU
+                        baseline
 Both take the product's descriptor (snac_b200.abi.SnacConfig) and expose the
 same calls, so a test can run the GPU path and either checker side by side.
 """
@@ -22,15 +27,26 @@ from snac_b200.abi import NT, Desc, Scalars, SnacConfig, State, StateView
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 PATHS = {"port": os.path.join(HERE, "liboracle.so"),
-         "reference": os.path.join(HERE, "_ref", "libsnacref.so")}
-PREFIX = {"port": "so_", "reference": "ref_"}
+         "reference": os.path.join(HERE, "_ref", "libsnacref.so"),
+         "reference_mt": os.path.join(HERE, "_ref", "libsnacref_mt.so")}
+PREFIX = {"port": "so_", "reference": "ref_", "reference_mt": "ref_"}
+
+
+def snac_tree() -> str:
+    """The SNAC source tree the reference checkers compile from: $SNAC_REF when
+    set, else reference/Snac beside this repository's directory."""
+    env = os.environ.get("SNAC_REF")
+    if env:
+        return env
+    return os.path.normpath(os.path.join(HERE, "..", "..", "reference", "Snac"))
 
 
 def build(kind: str = "port") -> str:
     """Compile the checker with oracle/Makefile if it is missing."""
     path = PATHS[kind]
     if not os.path.exists(path):
-        subprocess.run(["make", "-s", "-C", HERE, "ref" if kind == "reference" else "all"], check=True)
+        subprocess.run(["make", "-s", "-C", HERE, "all" if kind == "port" else "ref", f"SNAC_REF={snac_tree()}"],
+                       check=True)
     return path
 
 
@@ -57,6 +73,9 @@ def _lib(kind: str):
         if kind == "port":
             lib_fn("node_forces").argtypes = [vp]
             lib_fn("node_forces").restype = C.c_int
+        else:
+            lib_fn("set_threads").argtypes = [C.c_int]
+            lib_fn("threads").restype = C.c_int
         lib_fn("step").argtypes = [vp, C.c_int]
         lib_fn("step").restype = C.c_int
         lib_fn("get_state").argtypes = [vp, C.POINTER(StateView)]
@@ -81,11 +100,14 @@ def _p(a: Optional[np.ndarray]):
 class Checker:
     """One CPU model run (a Snac_Context)."""
 
-    def __init__(self, cfg: SnacConfig, kind: str = "port"):
+    def __init__(self, cfg: SnacConfig, kind: str = "port", threads: int = 1):
         self.kind = kind
         self.cfg = cfg
         self.lib = _lib(kind)
         self._f = lambda n: getattr(self.lib, PREFIX[kind] + n)  # noqa: E731
+        if kind != "port":
+            self._f("set_threads")(int(threads))
+        self.threads = self._f("threads")() if kind != "port" else 1
         self._desc = cfg.desc()
         st = C.c_int(0)
         self.h = self._f("create")(C.byref(self._desc), C.byref(st))

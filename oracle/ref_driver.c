@@ -15,6 +15,9 @@
  * and _SnacHydroStaticIC_IC.
  */
 #include <stdarg.h>
+#ifdef REF_THREADS
+#include <pthread.h>
+#endif
 
 #include "common/snac_shim_core.h"
 #include "common/snac_shim_plastic.h"
@@ -91,6 +94,64 @@ typedef struct ref_ctx {
 } ref_ctx;
 
 static ref_ctx* g_current; /* the constitutive trampoline needs the hook */
+
+/* Threads of the element and node loops.  Built with REF_THREADS
+ * (_ref/libsnacref_mt.so) the loops whose iterations are independent in the
+ * reference (every element or node writes only its own record; the minimum
+ * length scale is a min, which does not round) run on this many threads,
+ * each on one contiguous range, and give the serial build's bits; built
+ * without it the loops are the serial ones. */
+static int g_threads = 1;
+void ref_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+int ref_threads(void) {
+#ifdef REF_THREADS
+    return g_threads;
+#else
+    return 1;
+#endif
+}
+
+typedef void (*range_fn)(ref_ctx* r, unsigned lo, unsigned hi, double* acc);
+typedef struct { range_fn fn; ref_ctx* r; unsigned lo, hi; double acc; } range_job;
+#ifdef REF_THREADS
+static void* range_main(void* p) {
+    range_job* j = (range_job*)p;
+    j->fn(j->r, j->lo, j->hi, &j->acc);
+    return NULL;
+}
+#endif
+/* fn over [lo, hi) split into contiguous ranges, one per thread (a range
+ * whose thread could not be started runs on the caller); returns the min of
+ * the ranges' accumulators, each started at acc0 */
+static double parallel_range(range_fn fn, ref_ctx* r, unsigned lo, unsigned hi, int threads, double acc0) {
+    double acc = acc0;
+#ifdef REF_THREADS
+    if (threads > 1 && hi - lo >= (unsigned)threads) {
+        range_job job[256];
+        pthread_t tid[256];
+        int started[256];
+        const unsigned long long n = hi - lo;
+        for (int t = 0; t < threads; t++) {
+            job[t] = (range_job){fn, r, lo + (unsigned)(n * t / threads), lo + (unsigned)(n * (t + 1) / threads), acc0};
+            started[t] = t > 0 && pthread_create(&tid[t], NULL, range_main, &job[t]) == 0;
+        }
+        fn(r, job[0].lo, job[0].hi, &job[0].acc);
+        for (int t = 1; t < threads; t++) {
+            if (started[t])
+                pthread_join(tid[t], NULL);
+            else
+                fn(r, job[t].lo, job[t].hi, &job[t].acc);
+        }
+        for (int t = 0; t < threads; t++)
+            if (job[t].acc < acc) acc = job[t].acc;
+        return acc;
+    }
+#else
+    (void)threads;
+#endif
+    fn(r, lo, hi, &acc);
+    return acc;
+}
 
 static void run_constitutive(void* ep, void* ctx, Element_LocalIndex e) {
     (void)ep;
@@ -465,33 +526,40 @@ void ref_destroy(ref_ctx* r) {
 static int status_of(void) { return shim_firewall_count ? SNAC_GPU_ENAN : 0; }
 
 /* _Snac_Context_LoopElements, Context.c:1156-1184 */
+static void elements_momentum_range(ref_ctx* r, unsigned lo, unsigned hi, double* mn) {
+    for (unsigned e = lo; e < hi; e++) {
+        double ls;
+        Snac_UpdateElementMomentum(&r->ctx, e, &ls);
+        if (ls < *mn) *mn = ls;
+    }
+}
 int ref_loop_elements_momentum(ref_ctx* r) {
     Snac_Context* c = &r->ctx;
     g_current = r;
     Snac_UpdateElementMomentum(c, 0, &c->minLengthScale);
-    for (unsigned e = 1; e < r->ne; e++) {
-        double ls;
-        Snac_UpdateElementMomentum(c, e, &ls);
-        if (ls < c->minLengthScale) c->minLengthScale = ls;
-    }
+    c->minLengthScale = parallel_range(elements_momentum_range, r, 1, r->ne, g_threads, c->minLengthScale);
     return status_of();
 }
 
 /* _Snac_Context_CalcStresses, Context.c:1102-1117 */
-int ref_calc_stresses(ref_ctx* r) {
-    g_current = r;
-    for (unsigned e = 0; e < r->ne; e++) {
+static void calc_stresses_range(ref_ctx* r, unsigned lo, unsigned hi, double* unused) {
+    (void)unused;
+    for (unsigned e = lo; e < hi; e++) {
         Snac_StrainRate(&r->ctx, e);
         Snac_Stress(&r->ctx, e);
     }
+}
+int ref_calc_stresses(ref_ctx* r) {
+    g_current = r;
+    parallel_range(calc_stresses_range, r, 0, r->ne, g_threads, 0.0);
     return status_of();
 }
 
 /* _Snac_Context_LoopNodes, Context.c:1120-1154, with the hook order of Context.c:568-593 */
-int ref_loop_nodes_momentum(ref_ctx* r) {
+static void node_forces_range(ref_ctx* r, unsigned lo, unsigned hi, double* unused) {
     Snac_Context* c = &r->ctx;
-    g_current = r;
-    for (unsigned n = 0; n < r->nn; n++) {
+    (void)unused;
+    for (unsigned n = lo; n < hi; n++) {
         Snac_Node* node = &r->mesh.node[n];
         Snac_Force(c, n, c->speedOfSound, &r->mass_store[n], &node->inertialMass, &node->force, &r->balance_store[n]);
         if (r->winkler)  /* appended to Snac_EP_Force, winkler/Register.c:140-145 */
@@ -501,7 +569,11 @@ int ref_loop_nodes_momentum(ref_ctx* r) {
             _SnacTractionBC_Force_Apply(c, n, c->speedOfSound, &r->mass_store[n], &node->inertialMass, &node->force,
                                         &r->balance_store[n]);
     }
-    for (unsigned n = 0; n < r->nn; n++) {
+}
+static void node_update_range(ref_ctx* r, unsigned lo, unsigned hi, double* unused) {
+    Snac_Context* c = &r->ctx;
+    (void)unused;
+    for (unsigned n = lo; n < hi; n++) {
         Snac_Node* node = &r->mesh.node[n];
         Snac_UpdateNodeMomentum_PreProcess(c, n, node->inertialMass, node->force);
         Snac_UpdateNodeMomentum(c, n, node->inertialMass, node->force);
@@ -509,6 +581,15 @@ int ref_loop_nodes_momentum(ref_ctx* r) {
         Snac_UpdateNodeMomentum_UpdateInteriorTopo(c, n, node->inertialMass, node->force);
         Snac_UpdateNodeMomentum_AdjustEdgeTopo(c, n, node->inertialMass, node->force);
     }
+}
+int ref_loop_nodes_momentum(ref_ctx* r) {
+    Snac_Context* c = &r->ctx;
+    g_current = r;
+    parallel_range(node_forces_range, r, 0, r->nn, g_threads, 0.0);
+    /* the topography hooks walk the top surface in node order (UpdateNode.c:161-857):
+     * the update loop stays serial unless they are certain to do nothing */
+    const int topo_idle = c->topo_kappa == 0 && c->topoGradMax < c->topoGradCriterion;
+    parallel_range(node_update_range, r, 0, r->nn, topo_idle ? g_threads : 1, 0.0);
     return status_of();
 }
 

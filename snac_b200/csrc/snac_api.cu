@@ -62,6 +62,7 @@ struct snac_gpu {
     double wave_speed = 0.0;
     cudaStream_t stream = nullptr;
     bool own_stream = true;  // false for the models of a batch, which share the batch's stream
+    long long alloc_bytes = 0;  // device bytes allocated for this handle since creation (snac_gpu_device_bytes)
     // device buffers
     double4* pos[2] = {nullptr, nullptr};
     double4* vel = nullptr;
@@ -129,6 +130,7 @@ int dalloc(snac_gpu* h, T** p, size_t n) {
     if (n == 0) n = 1;
     cudaError_t e = cudaMalloc((void**)p, n * sizeof(T));
     if (e != cudaSuccess) return set_err(h, SNAC_GPU_ENOMEM, -1, "cudaMalloc(%zu bytes): %s", n * sizeof(T), cudaGetErrorString(e));
+    h->alloc_bytes += (long long)(n * sizeof(T));
     e = cudaMemsetAsync(*p, 0, n * sizeof(T), h->stream);
     if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "cudaMemset: %s", cudaGetErrorString(e));
     return 0;
@@ -1004,6 +1006,12 @@ int snac_gpu_sizes(const snac_gpu* h, long long* ne, long long* nn) {
 }
 long long snac_gpu_launch_count(const snac_gpu* h) { return h ? h->launches : 0; }
 
+int snac_gpu_device_bytes(const snac_gpu* h, long long* bytes) {
+    if (!h || !bytes) return SNAC_GPU_EINVAL;
+    *bytes = h->alloc_bytes;
+    return 0;
+}
+
 int snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max) {
     if (!h || !out || max < 1) return SNAC_GPU_EINVAL;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
@@ -1527,11 +1535,17 @@ extern "C" int snac_gpu_download_nodes_noalloc(snac_gpu* h, double* coord, doubl
     }
     double* stage = static_cast<double*>(g_noalloc_addr[dev]);
     int rc;
-    if ((rc = flush_pending(h))) return rc;
-    if (coord && (rc = noalloc_node_out(h, stage, h->pos[h->parity], coord, 0))) return rc;
-    if (velocity && (rc = noalloc_node_out(h, stage, h->vel, velocity, 0))) return rc;
-    if (temperature && (rc = noalloc_node_out(h, stage, h->pos[h->parity], temperature, 1))) return rc;
-    CK(cudaStreamSynchronize(h->stream));  // the staging is free again, and the host arrays are filled
+    if ((rc = flush_pending(h))) return rc;  // does not touch the staging
+    if (coord) rc = noalloc_node_out(h, stage, h->pos[h->parity], coord, 0);
+    if (!rc && velocity) rc = noalloc_node_out(h, stage, h->vel, velocity, 0);
+    if (!rc && temperature) rc = noalloc_node_out(h, stage, h->pos[h->parity], temperature, 1);
+    // Whatever happened above, this call's packs and copies are finished
+    // before the lock is released, so the next caller finds the staging free
+    // (and, on success, the host arrays are filled).
+    const cudaError_t se = cudaStreamSynchronize(h->stream);
+    if (rc) return rc;
+    if (se != cudaSuccess)
+        return set_err(h, SNAC_GPU_ECUDA, -1, "cudaStreamSynchronize: %s", cudaGetErrorString(se));
     return 0;
 }
 
@@ -1908,10 +1922,12 @@ int snac_gpu_output_open(snac_gpu* h, const char* output_path, unsigned rank, un
     const size_t need = (size_t)(ne * (4 + 1 + 6 + 1 + 1) + nn * (3 * 3 + 1) + ne * (1 + 60 + 10 + 10) + nn * (3 * 2 + 1)) * 4 +
                         sizeof(DevScalars) + 256 * 24;
     cudaError_t e = cudaMalloc((void**)&o->dstage, need);
+    if (e == cudaSuccess) h->alloc_bytes += (long long)need;
     if (e == cudaSuccess) e = cudaMallocHost((void**)&o->pinned, need);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&o->ready, cudaEventDisableTiming);
     if (e == cudaSuccess && !h->escal) {
         e = cudaMalloc((void**)&h->escal, ne * 4 * sizeof(double));
+        if (e == cudaSuccess) h->alloc_bytes += ne * 4 * (long long)sizeof(double);
         if (e == cudaSuccess) e = cudaMemsetAsync(h->escal, 0, ne * 4 * sizeof(double), h->stream);
     }
     o->cap = need;

@@ -103,4 +103,8 @@ def main(root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the checkout that holds Snac/: the first argument, else the parent of $SNAC_REF,
+    # else reference/ beside this repository
+    default = os.path.dirname(os.environ["SNAC_REF"].rstrip("/")) if os.environ.get("SNAC_REF") else \
+        os.path.normpath(os.path.join(HERE, "..", "..", "..", "reference"))
+    main(sys.argv[1] if len(sys.argv) > 1 else default)

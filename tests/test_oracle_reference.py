@@ -9,7 +9,7 @@ import pytest
 from oracle import pyoracle
 from tests import scenarios as S
 
-REF_TREE = "/root/reference/Snac"
+REF_TREE = pyoracle.snac_tree()
 
 
 def _reference_available():
@@ -68,3 +68,24 @@ def test_pull_test_bitwise():
     S.pull_test_10(a)
     S.pull_test_10(b)
     assert np.array_equal(a.state().velocity, b.state().velocity)
+
+
+@pytest.mark.parametrize("case", ["plastic", "viscoplastic", "winkler", "traction", "topo", "elastic"])
+def test_threaded_reference_is_bitwise_equal_to_serial(case):
+    """The all-cores CPU baseline (libsnacref_mt.so: the same reference
+    sources, element and node loops split over threads) gives the serial
+    build's bits; the topography case keeps its node update in node order."""
+    if not pyoracle.available("reference_mt"):
+        pytest.skip("threaded reference checker not built")
+    make, steps = S.CASES[case]
+    cfg = make()
+    a = pyoracle.Checker(cfg, "reference")
+    b = pyoracle.Checker(cfg, "reference_mt", threads=3)
+    assert b.threads == 3
+    assert a.time_step_zero() == 0 and b.time_step_zero() == 0
+    a.step(steps)
+    b.step(steps)
+    sa, sb = a.state(), b.state()
+    for f in FIELDS:
+        assert np.array_equal(getattr(sa, f), getattr(sb, f)), (case, f)
+    assert a.scalars().dt == b.scalars().dt

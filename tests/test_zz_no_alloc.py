@@ -55,6 +55,32 @@ def test_same_as_download_twice_in_a_row(make, steps):
         assert np.array_equal(third[0], ref.coord) and np.array_equal(third[1], ref.velocity)
 
 
+def device_bytes(ctx) -> int:
+    lib = load_library()
+    lib.snac_gpu_device_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_longlong)]
+    lib.snac_gpu_device_bytes.restype = C.c_int
+    b = C.c_longlong(-1)
+    ctx._check(lib.snac_gpu_device_bytes(ctx.h, C.byref(b)))
+    return b.value
+
+
+def test_allocates_nothing_on_a_fresh_handle():
+    """Called before any allocating download, the call leaves the handle's
+    device allocations where they were; the allocating download then shows
+    the check can see its lazily allocated staging."""
+    with SnacContext(W.c1_elastic()) as ctx:
+        ctx.time_step_zero()
+        ctx.step(3)
+        before = device_bytes(ctx)
+        first = call(ctx)
+        second = call(ctx)
+        assert device_bytes(ctx) == before
+        ref = ctx.state()  # snac_gpu_download: allocates its node staging on first use
+        assert device_bytes(ctx) > before
+        for got in (first, second):
+            assert np.array_equal(got[0], ref.coord) and np.array_equal(got[1], ref.velocity)
+
+
 def test_null_fields_are_skipped():
     with SnacContext(W.c1_elastic()) as ctx:
         ctx.time_step_zero()
