@@ -31,7 +31,7 @@
 extern "C" {
 #endif
 
-#define SNAC_GPU_ABI_VERSION 1
+#define SNAC_GPU_ABI_VERSION 2  /* snac_gpu_create also takes version-1 descriptors (up to topo_grad_criterion) */
 
 /* ---- status codes ------------------------------------------------------ */
 #define SNAC_GPU_OK          0
@@ -155,6 +155,24 @@ typedef struct snac_gpu_desc {
      * default is 5e-6) and "topoGradCriterion" (default 1e-16). */
     double topo_kappa;
     double topo_grad_criterion;
+
+    /* ---- ABI version 2 ----
+     * For a caller that ran the initial conditions itself (a Snac_Context
+     * after its plugin ICs, as the SnacCuda plugin passes it): the isostatic
+     * pressure and reference bottom depth SnacWinklerForce reads
+     * (context->pisos, element->rzbo), used when hydrostatic_ic == 0. */
+    double pisos, rzbo;
+    /* Velocity and temperature conditions resolved per node, in place of
+     * velocity_bcs / temperature_bcs when the mask is non-NULL: bit d of
+     * node_velocity_bc_mask[n] fixes component d of node n to
+     * node_velocity_bc_value[n*3+d]; node_temperature_bc_mask[n] != 0 fixes
+     * the temperature to node_temperature_bc_value[n].  At most 254 distinct
+     * values per velocity component and 254 temperatures (SNAC_GPU_ENOTSUP
+     * beyond).  The CPU checkers under oracle/ take the wall form only. */
+    const unsigned char* node_velocity_bc_mask;
+    const double* node_velocity_bc_value;
+    const unsigned char* node_temperature_bc_mask;
+    const double* node_temperature_bc_value;
 } snac_gpu_desc;
 
 /* Host-side view of the state for upload / download.  NULL members are

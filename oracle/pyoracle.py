@@ -28,8 +28,9 @@ from snac_b200.abi import NT, Desc, Scalars, SnacConfig, State, StateView
 HERE = os.path.dirname(os.path.abspath(__file__))
 PATHS = {"port": os.path.join(HERE, "liboracle.so"),
          "reference": os.path.join(HERE, "_ref", "libsnacref.so"),
-         "reference_mt": os.path.join(HERE, "_ref", "libsnacref_mt.so")}
-PREFIX = {"port": "so_", "reference": "ref_", "reference_mt": "ref_"}
+         "reference_mt": os.path.join(HERE, "_ref", "libsnacref_mt.so"),
+         "plugin_host": os.path.join(HERE, "_ref", "libsnaccuda_host.so")}
+PREFIX = {"port": "so_", "reference": "ref_", "reference_mt": "ref_", "plugin_host": "ref_"}
 
 
 def snac_tree() -> str:
@@ -45,8 +46,8 @@ def build(kind: str = "port") -> str:
     """Compile the checker with oracle/Makefile if it is missing."""
     path = PATHS[kind]
     if not os.path.exists(path):
-        subprocess.run(["make", "-s", "-C", HERE, "all" if kind == "port" else "ref", f"SNAC_REF={snac_tree()}"],
-                       check=True)
+        target = {"port": "all", "plugin_host": "plugin"}.get(kind, "ref")
+        subprocess.run(["make", "-s", "-C", HERE, target, f"SNAC_REF={snac_tree()}"], check=True)
     return path
 
 
@@ -207,3 +208,54 @@ class Checker:
         bal = np.zeros((self.nn, 3))
         self._f("get_node_fields")(self.h, _p(mass), _p(bal))
         return {"mass": mass, "balance": bal}
+
+
+class PluginHost(Checker):
+    """A Snac_Context of the reference sources (as Checker("reference")) into
+    which the SnacCuda plugin (snac_b200/plugin) is loaded the way
+    StGermain's PluginLoader loads it, then driven the way AbstractContext
+    drives a context: Initialise, steps of Dt / Solve / Sync, Dump, each
+    through whatever hooks the entry points hold.  Test infrastructure for
+    the plugin; stepping needs a GPU (the plugin's hooks call libsnac_b200)."""
+
+    def __init__(self, cfg: SnacConfig):
+        super().__init__(cfg, "plugin_host")
+        f = self._f
+        vp = C.c_void_p
+        for n in ("host_load_plugin",):
+            f(n).argtypes = [vp, C.c_char_p]
+            f(n).restype = C.c_int
+        for n in ("host_initialise", "host_dump"):
+            f(n).argtypes = [vp]
+            f(n).restype = C.c_int
+        f("host_step").argtypes = [vp, C.c_int]
+        f("host_step").restype = C.c_int
+        f("host_hooks").argtypes = [vp, C.c_char_p, C.c_char_p, C.c_int]
+        f("host_hooks").restype = C.c_int
+        f("host_context").argtypes = [vp]
+        f("host_context").restype = vp
+        f("host_extension").argtypes = [vp, C.c_char_p]
+        f("host_extension").restype = vp
+
+    def load_plugin(self, name: str = "SnacCuda") -> int:
+        return self._f("host_load_plugin")(self.h, name.encode())
+
+    def initialise(self) -> int:
+        return self._f("host_initialise")(self.h)
+
+    def host_step(self, n: int = 1) -> int:
+        return self._f("host_step")(self.h, int(n))
+
+    def dump(self) -> int:
+        return self._f("host_dump")(self.h)
+
+    def hooks(self, entry_point: str):
+        buf = C.create_string_buffer(1024)
+        self._f("host_hooks")(self.h, entry_point.encode(), buf, 1024)
+        return buf.value.decode().split(",") if buf.value else []
+
+    def context_ptr(self) -> int:
+        return self._f("host_context")(self.h)
+
+    def extension_ptr(self, name: str) -> int:
+        return self._f("host_extension")(self.h, name.encode())

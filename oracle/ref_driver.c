@@ -14,7 +14,9 @@
  * the topography hooks, the four constitutive hooks, the temperature loops
  * and _SnacHydroStaticIC_IC.
  */
+#define _GNU_SOURCE
 #include <stdarg.h>
+#include <dlfcn.h>
 #ifdef REF_THREADS
 #include <pthread.h>
 #endif
@@ -42,6 +44,117 @@ const Name Snac_DtType_Constant = "constant";
 const Name Snac_DtType_Dynamic = "dynamic";
 const Name Snac_DtType_Wave = "wave";
 const Name Snac_EP_LoopElementsEnergy = "Snac_EP_LoopElementsEnergy";
+const Name Snac_EP_LoopNodesEnergy = "Snac_EP_LoopNodesEnergy";
+const Name Snac_EP_CalcStresses = "Snac_EP_CalcStresses";
+const Name Snac_EP_Constitutive = "Snac_EP_Constitutive";
+const Name Snac_EP_LoopNodesMomentum = "Snac_EP_LoopNodesMomentum";
+const Name Snac_EP_Force = "Snac_EP_Force";
+const Name Snac_EP_LoopElementsMomentum = "Snac_EP_LoopElementsMomentum";
+/* AbstractContext.c:58-69 */
+const Name AbstractContext_EP_Initialise = "Context_Initialise";
+const Name AbstractContext_EP_Dt = "Context_Dt";
+const Name AbstractContext_EP_Solve = "Context_Solve";
+const Name AbstractContext_EP_Sync = "Context_Sync";
+const Name AbstractContext_EP_Dump = "Context_Dump";
+const Type Snac_Context_Type = "Snac_Context";
+
+/* ---- entry points (EntryPoint.c:681-850 semantics on a fixed-size list) ---------- */
+void* Stg_ObjectList_Get(void* list, Name name) {
+    Stg_ObjectList* l = (Stg_ObjectList*)list;
+    for (unsigned i = 0; l && i < l->count; i++)
+        if (strcmp(l->data[i]->name, name) == 0) return l->data[i];
+    return NULL;
+}
+static Hook* hook_new(Stg_ObjectList* l, Name name, Func_Ptr f, Hook_AddedBy by) {
+    for (int k = 0; k < SHIM_MAX_HOOKS; k++) {
+        int used = 0;
+        for (unsigned i = 0; i < l->count; i++) used |= l->data[i] == &l->store[k];
+        if (!used) {
+            l->store[k] = (Hook){name, f, by};
+            return &l->store[k];
+        }
+    }
+    shim_firewall("entry point: more than %d hooks", SHIM_MAX_HOOKS);
+    return NULL;
+}
+static void list_insert(Stg_ObjectList* l, unsigned at, Hook* h) {
+    if (!h) return;
+    for (unsigned i = l->count; i > at; i--) l->data[i] = l->data[i - 1];
+    l->data[at] = h;
+    l->count++;
+}
+static int list_find(Stg_ObjectList* l, Name name) {
+    for (unsigned i = 0; i < l->count; i++)
+        if (strcmp(l->data[i]->name, name) == 0) return (int)i;
+    return -1;
+}
+void EntryPoint_Append(void* ep, Name name, Func_Ptr f, Hook_AddedBy by) {
+    EntryPoint* e = (EntryPoint*)ep;
+    list_insert(e->hooks, e->hooks->count, hook_new(e->hooks, name, f, by));
+}
+void EntryPoint_Prepend(void* ep, Name name, Func_Ptr f, Hook_AddedBy by) {
+    EntryPoint* e = (EntryPoint*)ep;
+    list_insert(e->hooks, 0, hook_new(e->hooks, name, f, by));
+}
+void EntryPoint_InsertBefore(void* ep, Name before, Name name, Func_Ptr f, Hook_AddedBy by) {
+    EntryPoint* e = (EntryPoint*)ep;
+    int i = list_find(e->hooks, before);
+    if (i < 0) {
+        shim_firewall("EntryPoint_InsertBefore: no hook \"%s\" on %s", before, e->name);
+        return;
+    }
+    list_insert(e->hooks, (unsigned)i, hook_new(e->hooks, name, f, by));
+}
+void EntryPoint_Replace(void* ep, Name old, Name name, Func_Ptr f, Hook_AddedBy by) {
+    EntryPoint* e = (EntryPoint*)ep;
+    int i = list_find(e->hooks, old);
+    if (i < 0) {
+        shim_firewall("EntryPoint_Replace: no hook \"%s\" on %s", old, e->name);
+        return;
+    }
+    e->hooks->data[i]->name = name;
+    e->hooks->data[i]->funcPtr = f;
+    e->hooks->data[i]->addedBy = by;
+}
+void EntryPoint_ReplaceAll(void* ep, Name name, Func_Ptr f, Hook_AddedBy by) {
+    EntryPoint* e = (EntryPoint*)ep;
+    e->hooks->count = 0;
+    EntryPoint_Append(ep, name, f, by);
+}
+void EntryPoint_Remove(void* ep, Name name) {
+    EntryPoint* e = (EntryPoint*)ep;
+    int i = list_find(e->hooks, name);
+    if (i < 0) return;
+    for (unsigned k = (unsigned)i; k + 1 < e->hooks->count; k++) e->hooks->data[k] = e->hooks->data[k + 1];
+    e->hooks->count--;
+}
+EntryPoint* shim_get_entry_point(void* context, Name name) {
+    Snac_Context* c = (Snac_Context*)context;
+    for (unsigned i = 0; i < c->shim_ep_count; i++)
+        if (strcmp(c->shim_eps[i].name, name) == 0) return &c->shim_eps[i];
+    return NULL;
+}
+
+/* ---- extension managers ------------------------------------------------------------ */
+ExtensionInfo_Index ExtensionManager_GetHandle(void* mgr, Name name) {
+    ExtensionManager* m = (ExtensionManager*)mgr;
+    for (unsigned k = 0; k < SHIM_MAX_EXTENSIONS; k++)
+        if (m->name[k] && strcmp(m->name[k], name) == 0) return k;
+    return (ExtensionInfo_Index)-1;
+}
+ExtensionInfo_Index ExtensionManager_Add(void* mgr, Name name, size_t size) {
+    ExtensionManager* m = (ExtensionManager*)mgr;
+    for (unsigned k = 0; k < SHIM_MAX_EXTENSIONS; k++)
+        if (!m->ext[k]) {
+            m->ext[k] = calloc(m->count ? m->count : 1, size ? size : 1);
+            m->extsize[k] = size;
+            m->name[k] = name;
+            m->owned |= 1u << k;
+            return k;
+        }
+    shim_firewall("ExtensionManager_Add: no free slot for %s", name);
+    return (ExtensionInfo_Index)-1;
+}
 
 ExtensionInfo_Index SnacPlastic_ElementHandle = 0;
 ExtensionInfo_Index SnacViscoPlastic_ElementHandle = 1;
@@ -194,6 +307,81 @@ static int wall_has(const ref_ctx* r, int wall, int i, int j, int k) {
 }
 
 void ref_destroy(ref_ctx* r);
+int ref_time_step_zero(ref_ctx* r);
+int ref_loop_elements_energy(ref_ctx* r);
+int ref_loop_nodes_energy(ref_ctx* r);
+int ref_calc_stresses(ref_ctx* r);
+int ref_loop_nodes_momentum(ref_ctx* r);
+int ref_loop_elements_momentum(ref_ctx* r);
+int ref_sync(ref_ctx* r);
+
+/* ---- the context's named entry points with the reference's default hooks -------------
+ * (Context.c:470-600, the plugins' Register.c).  The checker's own step
+ * (ref_step) calls the loops directly; these serve the plugin host below,
+ * which drives a context the way AbstractContext does, through whatever
+ * hooks the entry points hold. */
+enum { EP_INIT, EP_DT, EP_SOLVE, EP_SYNC, EP_DUMP, EP_LEE, EP_LNE, EP_CALC, EP_CONST, EP_LNM, EP_FORCE, EP_LEM, EP_N };
+typedef void (*void_hook)(void*);
+static void run_hooks(void* c, Name ep) {
+    EntryPoint* e = Context_GetEntryPoint(c, ep);
+    for (unsigned i = 0; e && i < e->hooks->count && !shim_firewall_count; i++) ((void_hook)e->hooks->data[i]->funcPtr)(c);
+}
+static void hk_time_step_zero(void* c, void* data) { (void)data; ref_time_step_zero((ref_ctx*)c); }
+static double hk_dt(void* c) { return ((Snac_Context*)c)->dt; } /* _Snac_Context_Dt */
+static void hk_loop_elements_energy(void* c) { ref_loop_elements_energy((ref_ctx*)c); }
+static void hk_loop_nodes_energy(void* c) { ref_loop_nodes_energy((ref_ctx*)c); }
+static void hk_calc_stresses(void* c) { ref_calc_stresses((ref_ctx*)c); }
+static void hk_loop_nodes_momentum(void* c) { ref_loop_nodes_momentum((ref_ctx*)c); }
+static void hk_loop_elements_momentum(void* c) { ref_loop_elements_momentum((ref_ctx*)c); }
+static void hk_sync(void* c) { ref_sync((ref_ctx*)c); }
+/* _Snac_Context_Solve, Context.c:1063-1099 (one rank: no Mesh_Sync) */
+static void hk_solve(void* c) {
+    run_hooks(c, Snac_EP_LoopElementsEnergy);
+    run_hooks(c, Snac_EP_LoopNodesEnergy);
+    run_hooks(c, Snac_EP_CalcStresses);
+    run_hooks(c, Snac_EP_LoopNodesMomentum);
+    run_hooks(c, Snac_EP_LoopElementsMomentum);
+}
+static void no_hook(void* c) { (void)c; }
+
+static void setup_entry_points(ref_ctx* r, Name constitutive_type) {
+    static const char* names[EP_N];
+    names[EP_INIT] = AbstractContext_EP_Initialise;
+    names[EP_DT] = AbstractContext_EP_Dt;
+    names[EP_SOLVE] = AbstractContext_EP_Solve;
+    names[EP_SYNC] = AbstractContext_EP_Sync;
+    names[EP_DUMP] = AbstractContext_EP_Dump;
+    names[EP_LEE] = Snac_EP_LoopElementsEnergy;
+    names[EP_LNE] = Snac_EP_LoopNodesEnergy;
+    names[EP_CALC] = Snac_EP_CalcStresses;
+    names[EP_CONST] = Snac_EP_Constitutive;
+    names[EP_LNM] = Snac_EP_LoopNodesMomentum;
+    names[EP_FORCE] = Snac_EP_Force;
+    names[EP_LEM] = Snac_EP_LoopElementsMomentum;
+    Snac_Context* c = &r->ctx;
+    c->shim_eps = calloc(EP_N, sizeof(EntryPoint));
+    c->shim_ep_count = EP_N;
+    for (int i = 0; i < EP_N; i++) {
+        c->shim_eps[i].name = names[i];
+        c->shim_eps[i].hooks = &c->shim_eps[i].list;
+    }
+    EntryPoint* e = c->shim_eps;
+    EntryPoint_Append(&e[EP_INIT], "SnacTimeStepZero", (Func_Ptr)hk_time_step_zero, "Snac");
+    EntryPoint_Append(&e[EP_DT], "SnacDt", (Func_Ptr)hk_dt, "Snac");
+    EntryPoint_Append(&e[EP_SOLVE], "SnacSolve", (Func_Ptr)hk_solve, "Snac");
+    EntryPoint_Append(&e[EP_SYNC], "SnacSync", (Func_Ptr)hk_sync, "Snac");
+    if (r->temperature) {
+        EntryPoint_Append(&e[EP_LEE], "SnacTemperature", (Func_Ptr)hk_loop_elements_energy, "SnacTemperature");
+        EntryPoint_Append(&e[EP_LNE], "SnacTemperature", (Func_Ptr)hk_loop_nodes_energy, "SnacTemperature");
+    }
+    EntryPoint_Append(&e[EP_CALC], "default", (Func_Ptr)hk_calc_stresses, "Snac");
+    EntryPoint_Append(&e[EP_CONST], constitutive_type, (Func_Ptr)no_hook, constitutive_type);
+    EntryPoint_Append(&e[EP_LNM], "default", (Func_Ptr)hk_loop_nodes_momentum, "Snac");
+    EntryPoint_Append(&e[EP_FORCE], "default", (Func_Ptr)no_hook, "Snac");
+    if (r->winkler) EntryPoint_Append(&e[EP_FORCE], "SnacWinklerForce", (Func_Ptr)no_hook, "SnacWinklerForce");
+    if (r->traction) EntryPoint_Append(&e[EP_FORCE], "SnacTractionBC", (Func_Ptr)no_hook, "SnacTractionBC");
+    EntryPoint_Append(&e[EP_LEM], "default", (Func_Ptr)hk_loop_elements_momentum, "Snac");
+}
 
 ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
     *status = SNAC_GPU_EINVAL;
@@ -340,6 +528,14 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
     r->cmgr.stride = 1;
     r->cmgr.ext[0] = (char*)&r->tctx;
     r->cmgr.extsize[0] = sizeof r->tctx;
+    r->emgr.count = r->ne;
+    r->nmgr.count = r->nn;
+    r->cmgr.count = 1;
+    /* the loaded plugins' extension keys (their Type names) */
+    if (d->constitutive == SNAC_RHEOLOGY_PLASTIC) r->emgr.name[0] = "SnacPlastic";
+    if (d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) r->emgr.name[1] = "SnacViscoPlastic";
+    if (d->constitutive == SNAC_RHEOLOGY_MAXWELL) r->emgr.name[2] = "SnacMaxwell";
+    if (d->temperature) r->emgr.name[3] = r->nmgr.name[0] = r->cmgr.name[0] = "SnacTemperature";
     m->elementExtensionMgr = &r->emgr;
     m->nodeExtensionMgr = &r->nmgr;
     /* context */
@@ -368,13 +564,15 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
     r->tctx.topTemp = d->top_temp;
     r->tctx.bottomTemp = d->bottom_temp;
     r->tctx.temperatureBCs = &r->tbc;
+    Name ctype = "SnacElastic";
     switch (d->constitutive) {
         case SNAC_RHEOLOGY_ELASTIC: r->hook = _SnacElastic_Constitutive; break;
-        case SNAC_RHEOLOGY_PLASTIC: r->hook = SnacPlastic_Constitutive; break;
-        case SNAC_RHEOLOGY_VISCOPLASTIC: r->hook = SnacViscoPlastic_Constitutive; break;
-        case SNAC_RHEOLOGY_MAXWELL: r->hook = _SnacMaxwell_Constitutive; break;
+        case SNAC_RHEOLOGY_PLASTIC: r->hook = SnacPlastic_Constitutive; ctype = "SnacPlastic"; break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC: r->hook = SnacViscoPlastic_Constitutive; ctype = "SnacViscoPlastic"; break;
+        case SNAC_RHEOLOGY_MAXWELL: r->hook = _SnacMaxwell_Constitutive; ctype = "SnacMaxwell"; break;
         default: ref_destroy(r); return NULL;
     }
+    setup_entry_points(r, ctype);
     /* materials (Context.c:826-914), per-element multipliers as one phase per element */
     int per_elem = d->element_cohesion_scale || d->element_friction_scale || d->element_visc_scale;
     if (per_elem && d->constitutive == SNAC_RHEOLOGY_MAXWELL) {
@@ -520,6 +718,11 @@ void ref_destroy(ref_ctx* r) {
     free(r->tn);
     free(r->mass_store);
     free(r->balance_store);
+    ExtensionManager* mgrs[3] = {&r->emgr, &r->nmgr, &r->cmgr};
+    for (int q = 0; q < 3; q++)
+        for (unsigned k = 0; k < SHIM_MAX_EXTENSIONS; k++)
+            if (mgrs[q]->owned & (1u << k)) free(mgrs[q]->ext[k]);
+    free(r->ctx.shim_eps);
     free(r);
 }
 
@@ -800,4 +1003,109 @@ void ref_get_node_fields(ref_ctx* r, double* mass, double* balance) {
         if (balance)
             for (int q = 0; q < 3; q++) balance[n * 3 + q] = r->balance_store[n][q];
     }
+}
+
+/* ---- plugin host: a context driven through its entry points ---------------------------
+ * What StGermain's PluginLoader and AbstractContext do for one rank
+ * (PluginLoader.c:359-370, AbstractContext.c:874-941): find the plugin's
+ * register function by name, let it submit its component, construct it
+ * against this context, then run Initialise, the steps and Dump through the
+ * hooks the entry points hold. */
+typedef struct PluginEntry { Name type; void* (*defaultNew)(Name); } PluginEntry;
+static PluginEntry g_submitted[8];
+static int g_n_submitted;
+Index PluginsManager_Submit(void* pm, Name codeletName, Name version, void* (*defaultNew)(Name)) {
+    (void)pm;
+    (void)version;
+    if (g_n_submitted >= 8) return (Index)-1;
+    g_submitted[g_n_submitted] = (PluginEntry){codeletName, defaultNew};
+    return (Index)g_n_submitted++;
+}
+void* _Codelet_New(SizeT size, Type type, void* del, void* print, void* copy, void* defaultNew, void* construct,
+                   void* build, void* init, void* execute, void* destroy, Name name) {
+    (void)del, (void)print, (void)copy, (void)defaultNew, (void)build, (void)init, (void)execute, (void)destroy;
+    Codelet* c = calloc(1, size > sizeof(Codelet) ? size : sizeof(Codelet));
+    c->type = type;
+    c->name = name;
+    c->_construct = (Stg_Component_ConstructFunction*)construct;
+    return c;
+}
+static Stg_Component* factory_construct_by_name(void* cf, Name name, Type type, Bool essential, void* data) {
+    (void)type, (void)essential, (void)data;
+    return strcmp(name, "context") == 0 ? (Stg_Component*)((Stg_ComponentFactory*)cf)->context : NULL;
+}
+
+/* loads plugin "name" (e.g. "SnacCuda") into the context: returns 0 or a negative status */
+int ref_host_load_plugin(ref_ctx* r, const char* name) {
+    char sym[128];
+    Dl_info info;
+    void* self = NULL;
+    if (dladdr((void*)ref_create, &info) && info.dli_fname) self = dlopen(info.dli_fname, RTLD_NOW | RTLD_NOLOAD);
+    if (!self) return SNAC_GPU_EINVAL;
+    snprintf(sym, sizeof sym, "%s_Register", name);
+    Index (*reg)(void*) = (Index(*)(void*))dlsym(self, sym);
+    if (!reg) {  /* leading-underscore fallback, PluginLoader.c:365-370 */
+        snprintf(sym, sizeof sym, "_%s_Register", name);
+        reg = (Index(*)(void*))dlsym(self, sym);
+    }
+    dlclose(self);
+    if (!reg) return SNAC_GPU_ENOTSUP;
+    int before = g_n_submitted;
+    reg(NULL);
+    if (g_n_submitted != before + 1) return SNAC_GPU_EINVAL;
+    Codelet* comp = (Codelet*)g_submitted[before].defaultNew((Name)name);
+    g_n_submitted = before;
+    Stg_ComponentFactory cf = {&r->ctx, factory_construct_by_name};
+    comp->_construct(comp, &cf, NULL);
+    free(comp);
+    return shim_firewall_count ? SNAC_GPU_EPHYSICS : 0;
+}
+
+/* AbstractContext_Initialise: the Initialise hooks (SnacTimeStepZero, or its replacement) */
+int ref_host_initialise(ref_ctx* r) {
+    EntryPoint* e = Context_GetEntryPoint(&r->ctx, AbstractContext_EP_Initialise);
+    for (unsigned i = 0; i < e->hooks->count && !shim_firewall_count; i++)
+        ((void (*)(void*, void*))e->hooks->data[i]->funcPtr)(&r->ctx, NULL);
+    return status_of();
+}
+
+/* nsteps x (timeStep++, dt from the Dt hook, currentTime += dt, Solve hooks, Sync hooks) */
+int ref_host_step(ref_ctx* r, int nsteps) {
+    Snac_Context* c = &r->ctx;
+    for (int i = 0; i < nsteps && !shim_firewall_count; i++) {
+        c->timeStep++;
+        EntryPoint* dt = Context_GetEntryPoint(c, AbstractContext_EP_Dt);
+        double d = c->dt;
+        for (unsigned k = 0; k < dt->hooks->count; k++) d = ((double (*)(void*))dt->hooks->data[k]->funcPtr)(c);
+        r->currentTime += d;
+        c->dt = d; /* _setDt */
+        run_hooks(c, AbstractContext_EP_Solve);
+        run_hooks(c, AbstractContext_EP_Sync);
+    }
+    return status_of();
+}
+
+/* AbstractContext_Dump: the Dump hooks */
+int ref_host_dump(ref_ctx* r) {
+    run_hooks(&r->ctx, AbstractContext_EP_Dump);
+    return status_of();
+}
+
+/* the hook names of one entry point, comma-separated (for tests) */
+int ref_host_hooks(ref_ctx* r, const char* ep, char* out, int cap) {
+    EntryPoint* e = Context_GetEntryPoint(&r->ctx, ep);
+    if (!e || cap < 1) return SNAC_GPU_EINVAL;
+    out[0] = 0;
+    for (unsigned i = 0; i < e->hooks->count; i++) {
+        if (i) strncat(out, ",", (size_t)cap - strlen(out) - 1);
+        strncat(out, e->hooks->data[i]->name, (size_t)cap - strlen(out) - 1);
+    }
+    return 0;
+}
+
+/* the context, and a context extension by key (for the plugin's tests) */
+void* ref_host_context(ref_ctx* r) { return &r->ctx; }
+void* ref_host_extension(ref_ctx* r, const char* name) {
+    ExtensionInfo_Index k = ExtensionManager_GetHandle(&r->cmgr, name);
+    return k == (ExtensionInfo_Index)-1 ? NULL : r->cmgr.ext[k];
 }

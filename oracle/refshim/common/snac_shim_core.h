@@ -73,13 +73,23 @@ typedef struct Dictionary { int dummy; } Dictionary;
 #define Dictionary_Entry_Value_AsDictionary(v) ((Dictionary*)0)
 #define Dictionary_Entry_Value_AsDouble(v) (0.0)
 
-/* extension managers: item index from the item pointer, one array per handle */
+/* extension managers: item index from the item pointer, one array per handle;
+ * name[h] is the extension's key (the plugin Type that added it, NULL while the
+ * slot is unused), count the number of items (1 for the context) */
+#define SHIM_MAX_EXTENSIONS 8
 typedef struct ExtensionManager {
     char* base;
     size_t stride;
-    char* ext[8];
-    size_t extsize[8];
+    char* ext[SHIM_MAX_EXTENSIONS];
+    size_t extsize[SHIM_MAX_EXTENSIONS];
+    const char* name[SHIM_MAX_EXTENSIONS];
+    size_t count;
+    unsigned owned;  /* slots allocated by ExtensionManager_Add (freed with the context) */
 } ExtensionManager;
+/* ExtensionManager.c:678-699 (not found: (unsigned)-1) and the
+ * ExtensionManager_Add macro of ExtensionManager.h:184 */
+ExtensionInfo_Index ExtensionManager_GetHandle(void* mgr, Name name);
+ExtensionInfo_Index ExtensionManager_Add(void* mgr, Name name, size_t size);
 #define ExtensionManager_Get(mgr, item, handle)                                                  \
     ((void*)((mgr)->ext[(handle)] +                                                              \
              (((size_t)((char*)(item) - (mgr)->base)) / (mgr)->stride) * (mgr)->extsize[(handle)]))
@@ -125,11 +135,40 @@ struct VariableCondition {
 #define VariableCondition_ApplyToIndex(vc, idx, ctx) ((vc)->applyToIndex((vc), (idx), (ctx)))
 #define VariableCondition_Apply(vc, ctx) ((vc)->apply((vc), (ctx)))
 
-/* entry points: the driver installs one constitutive hook */
-typedef struct EntryPoint { int dummy; } EntryPoint;
+/* entry points: named lists of named hooks (StGermain/Base/Extensibility/src/
+ * EntryPoint.c), looked up by name on the context; the constitutive entry
+ * point of the hot loop is called through KeyCall with the one hook the
+ * driver installs */
+typedef void* Func_Ptr;
+typedef const char* Hook_AddedBy;
+typedef unsigned long SizeT;
+typedef struct Hook {
+    Name name;
+    Func_Ptr funcPtr;
+    Hook_AddedBy addedBy;
+} Hook;
+#define SHIM_MAX_HOOKS 16
+typedef struct Stg_ObjectList {
+    unsigned count;
+    Hook* data[SHIM_MAX_HOOKS];
+    Hook store[SHIM_MAX_HOOKS];
+} Stg_ObjectList;
+typedef struct EntryPoint {
+    Name name;
+    Stg_ObjectList* hooks;
+    Stg_ObjectList list;
+} EntryPoint;
+void* Stg_ObjectList_Get(void* list, Name name);
+void EntryPoint_Append(void* ep, Name name, Func_Ptr funcPtr, Hook_AddedBy addedBy);
+void EntryPoint_Prepend(void* ep, Name name, Func_Ptr funcPtr, Hook_AddedBy addedBy);
+void EntryPoint_InsertBefore(void* ep, Name hookToInsertBefore, Name name, Func_Ptr funcPtr, Hook_AddedBy addedBy);
+void EntryPoint_Replace(void* ep, Name hookToReplace, Name name, Func_Ptr funcPtr, Hook_AddedBy addedBy);
+void EntryPoint_ReplaceAll(void* ep, Name name, Func_Ptr funcPtr, Hook_AddedBy addedBy);
+void EntryPoint_Remove(void* ep, Name name);
 #define KeyCall(ctx, key, cast) ((cast)((ctx)->shim_ep_run[(key)]))
 #define KeyHandle(ctx, key) ((void*)&(ctx)->shim_ep[(key)])
-#define Context_GetEntryPoint(ctx, name) ((EntryPoint*)&(ctx)->shim_ep[0])
+#define Context_GetEntryPoint(ctx, name) shim_get_entry_point((void*)(ctx), (name))
+EntryPoint* shim_get_entry_point(void* context, Name name);
 
 /* MPI with one rank */
 #define MPI_Barrier(comm) (0)
@@ -275,13 +314,58 @@ struct _Snac_Context {
     EntryPoint_Index constitutiveK;
     void* shim_ep_run[2];
     EntryPoint shim_ep[2];
+    EntryPoint* shim_eps;  /* the named entry points of this context */
+    unsigned shim_ep_count;
 };
+
+/* AbstractContext.c:55-72 and Context.c:70-82 entry point names */
+extern const Name AbstractContext_EP_Initialise;
+extern const Name AbstractContext_EP_Dt;
+extern const Name AbstractContext_EP_Solve;
+extern const Name AbstractContext_EP_Sync;
+extern const Name AbstractContext_EP_Dump;
+extern const Name Snac_EP_LoopNodesEnergy;
+extern const Name Snac_EP_CalcStresses;
+extern const Name Snac_EP_Constitutive;
+extern const Name Snac_EP_LoopNodesMomentum;
+extern const Name Snac_EP_Force;
+extern const Name Snac_EP_LoopElementsMomentum;
 typedef Snac_Context Context;
 
 extern const Name Snac_DtType_Constant;
 extern const Name Snac_DtType_Dynamic;
 extern const Name Snac_DtType_Wave;
 extern const Name Snac_EP_LoopElementsEnergy;
+
+/* ---- plugins: PluginsManager.h:101, Codelet.h:62, Stg_ComponentFactory.h:236 --------- */
+typedef void Stg_Component;
+typedef struct Stg_ComponentFactory Stg_ComponentFactory;
+typedef Stg_Component*(Stg_ComponentFactory_ConstructByNameFunc)(void* cf, Name name, Type type, Bool essential,
+                                                                 void* data);
+struct Stg_ComponentFactory {
+    void* context;
+    Stg_ComponentFactory_ConstructByNameFunc* constructByName;
+};
+#define Stg_ComponentFactory_ConstructByName(cf, componentName, type, isEssential, data) \
+    (type*)((Stg_ComponentFactory*)(cf))->constructByName((cf), (componentName), type##_Type, (isEssential), (data))
+typedef void(Stg_Component_ConstructFunction)(void* component, Stg_ComponentFactory* cf, void* data);
+typedef struct Codelet {
+    Type type;
+    Name name;
+    Stg_Component_ConstructFunction* _construct;
+} Codelet;
+typedef struct PluginsManager PluginsManager;
+Index PluginsManager_Submit(void* pluginsMgr, Name codeletName, Name version, void* (*defaultNew)(Name));
+void* _Codelet_New(SizeT size, Type type, void* del, void* print, void* copy, void* defaultNew, void* construct,
+                   void* build, void* init, void* execute, void* destroy, Name name);
+#define _Codelet_Delete NULL
+#define _Codelet_Print NULL
+#define _Codelet_Copy NULL
+#define _Codelet_Build NULL
+#define _Codelet_Initialise NULL
+#define _Codelet_Execute NULL
+#define _Codelet_Destroy NULL
+extern const Type Snac_Context_Type;
 
 /* ---- shortcuts.h ------------------------------------------------------------------ */
 #define Snac_Node_At(self, index) (&(self)->mesh->node[(index)])

@@ -20,7 +20,7 @@ from typing import Any, Dict, List, Optional, Sequence
 
 import numpy as np
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK = 0
 EINVAL = -1
@@ -108,6 +108,9 @@ class Desc(C.Structure):
         ("init_velocity", _DP), ("init_temperature", _DP), ("init_stress", _DP),
         ("winkler", C.c_int), ("traction_bc", C.c_int),
         ("topo_kappa", C.c_double), ("topo_grad_criterion", C.c_double),
+        ("pisos", C.c_double), ("rzbo", C.c_double),
+        ("node_velocity_bc_mask", C.POINTER(C.c_ubyte)), ("node_velocity_bc_value", _DP),
+        ("node_temperature_bc_mask", C.POINTER(C.c_ubyte)), ("node_temperature_bc_value", _DP),
     ]
 
 

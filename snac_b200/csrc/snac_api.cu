@@ -596,10 +596,15 @@ int snac_gpu_device_count(void) {
 }
 
 // Builds a model; with shared != null the model uses that stream (batches)
-static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t shared) {
+static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t shared) {
     if (!out) return SNAC_GPU_EINVAL;
     *out = nullptr;
-    if (!d || d->abi_version != SNAC_GPU_ABI_VERSION) return SNAC_GPU_EINVAL;
+    if (!d_in || (d_in->abi_version != 1 && d_in->abi_version != SNAC_GPU_ABI_VERSION)) return SNAC_GPU_EINVAL;
+    // a version-1 descriptor ends at topo_grad_criterion: the version-2 fields read as zero
+    snac_gpu_desc dv;
+    memset(&dv, 0, sizeof dv);
+    memcpy(&dv, d_in, d_in->abi_version == 1 ? offsetof(snac_gpu_desc, pisos) : sizeof dv);
+    const snac_gpu_desc* d = &dv;
     if (d->nx < 1 || d->ny < 1 || d->nz < 1 || d->n_materials < 1 || !d->materials) return SNAC_GPU_EINVAL;
     if (d->n_materials > MAX_PHASES) return SNAC_GPU_EINVAL;
     if (d->constitutive != SNAC_RHEOLOGY_ELASTIC && d->constitutive != SNAC_RHEOLOGY_PLASTIC &&
@@ -655,8 +660,8 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
     c.traction = d->traction_bc ? 1 : 0;
     c.topo_kappa = d->topo_kappa;
     c.topo_crit = d->topo_grad_criterion;
-    c.pisos = 0.0;
-    c.rzbo = 0.0;
+    c.pisos = d->pisos;  // replaced below when the hydrostatic IC runs here
+    c.rzbo = d->rzbo;
     if (shared) {
         h->stream = shared;
         h->own_stream = false;
@@ -689,6 +694,38 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
         if (h->has_density && (rc = dalloc(h, &h->tpre, nn))) return rc;
     }
 
+    // ---- conditions resolved per node (ABI 2): one table entry per distinct value ----
+    // entry b of the velocity table holds, for each component q, the b-th
+    // distinct value of that component; a node's index per component points there
+    std::vector<std::vector<double>> pn_vval(3);
+    std::vector<double> pn_tval;
+    auto slot_of = [](std::vector<double>& vals, double v) -> int {
+        for (size_t b = 0; b < vals.size(); b++)
+            if (memcmp(&vals[b], &v, sizeof v) == 0) return (int)b;
+        vals.push_back(v);
+        return (int)vals.size() - 1;
+    };
+    std::vector<uchar4> pn_idx;
+    if (d->node_velocity_bc_mask || d->node_temperature_bc_mask) {
+        pn_idx.assign(nn, make_uchar4(255, 255, 255, 255));
+        for (long long n = 0; n < nn; n++) {
+            unsigned char idx[4] = {255, 255, 255, 255};
+            for (int q = 0; q < 3; q++)
+                if (d->node_velocity_bc_mask && (d->node_velocity_bc_mask[n] & (1 << q))) {
+                    int b = slot_of(pn_vval[q], d->node_velocity_bc_value[n * 3 + q]);
+                    if (b > 253) return set_err(h, SNAC_GPU_ENOTSUP, n, "more than 254 distinct velocity-BC values");
+                    idx[q] = (unsigned char)b;
+                }
+            if (d->temperature && d->node_temperature_bc_mask && d->node_temperature_bc_mask[n]) {
+                int b = slot_of(pn_tval, d->node_temperature_bc_value[n]);
+                if (b > 253) return set_err(h, SNAC_GPU_ENOTSUP, n, "more than 254 distinct temperature-BC values");
+                idx[3] = (unsigned char)b;
+            }
+            pn_idx[n] = make_uchar4(idx[0], idx[1], idx[2], idx[3]);
+        }
+    }
+    const bool pn_vel = d->node_velocity_bc_mask != nullptr, pn_temp = d->node_temperature_bc_mask != nullptr;
+
     // ---- initial conditions on the host ----
     std::vector<double> coord(nn * 3), vel(nn * 3, 0.0), temp(nn, 0.0), temp0(nn, 0.0), stress(nq * 6, 0.0);
     std::vector<uchar4> bc(nn, make_uchar4(255, 255, 255, 255));
@@ -709,24 +746,30 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
                 temp[n] = d->init_temperature[n];
         }
         unsigned char idx[4] = {255, 255, 255, 255};
-        for (int b = 0; b < d->n_velocity_bcs; b++) {  // last VC wins, CompositeVC.c:599-611
-            const snac_wall_bc& w = d->velocity_bcs[b];
-            if (!wall_has(w.wall, i, j, k, m.nnx, m.nny, m.nnz)) continue;
-            for (int q = 0; q < 3; q++)
-                if (w.mask & (1 << q)) idx[q] = (unsigned char)b;
-        }
-        for (int b = 0; b < d->n_temperature_bcs; b++) {
-            const snac_wall_bc& w = d->temperature_bcs[b];
-            if ((w.mask & 1) && wall_has(w.wall, i, j, k, m.nnx, m.nny, m.nnz)) idx[3] = (unsigned char)b;
-        }
+        if (!pn_vel)
+            for (int b = 0; b < d->n_velocity_bcs; b++) {  // last VC wins, CompositeVC.c:599-611
+                const snac_wall_bc& w = d->velocity_bcs[b];
+                if (!wall_has(w.wall, i, j, k, m.nnx, m.nny, m.nnz)) continue;
+                for (int q = 0; q < 3; q++)
+                    if (w.mask & (1 << q)) idx[q] = (unsigned char)b;
+            }
+        else
+            for (int q = 0; q < 3; q++) idx[q] = (&pn_idx[n].x)[q];
+        if (!pn_temp)
+            for (int b = 0; b < d->n_temperature_bcs; b++) {
+                const snac_wall_bc& w = d->temperature_bcs[b];
+                if ((w.mask & 1) && wall_has(w.wall, i, j, k, m.nnx, m.nny, m.nnz)) idx[3] = (unsigned char)b;
+            }
+        else
+            idx[3] = pn_idx[n].w;
         bc[n] = make_uchar4(idx[0], idx[1], idx[2], idx[3]);
         // temperature0 = temperature before the BCs are applied
         // (_SnacTemperature_InitialConditions, temperature/VariableConditions.c:240-256)
         temp0[n] = temp[n];
         // VariableCondition_Apply(velocityBCs), Context.c:773
         for (int q = 0; q < 3; q++)
-            if (idx[q] != 255) vel[n * 3 + q] = d->velocity_bcs[idx[q]].value[q];
-        if (d->temperature && idx[3] != 255) temp[n] = d->temperature_bcs[idx[3]].value[0];
+            if (idx[q] != 255) vel[n * 3 + q] = pn_vel ? pn_vval[q][idx[q]] : d->velocity_bcs[idx[q]].value[q];
+        if (d->temperature && idx[3] != 255) temp[n] = pn_temp ? pn_tval[idx[3]] : d->temperature_bcs[idx[3]].value[0];
     }
     if (d->init_stress) std::copy(d->init_stress, d->init_stress + nq * 6, stress.begin());
     if (d->hydrostatic_ic) {
@@ -739,10 +782,14 @@ static int create_model(const snac_gpu_desc* d, snac_gpu** out, cudaStream_t sha
         pos4[n] = make_double4(coord[n * 3], coord[n * 3 + 1], coord[n * 3 + 2], temp[n]);
         vel4[n] = make_double4(vel[n * 3], vel[n * 3 + 1], vel[n * 3 + 2], temp0[n]);
     }
-    std::vector<double> vbc(std::max(1, d->n_velocity_bcs) * 3, 0.0), tbc(std::max(1, d->n_temperature_bcs), 0.0);
-    for (int b = 0; b < d->n_velocity_bcs; b++)
-        for (int q = 0; q < 3; q++) vbc[b * 3 + q] = d->velocity_bcs[b].value[q];
-    for (int b = 0; b < d->n_temperature_bcs; b++) tbc[b] = d->temperature_bcs[b].value[0];
+    const int nvb = pn_vel ? (int)std::max(pn_vval[0].size(), std::max(pn_vval[1].size(), pn_vval[2].size()))
+                           : d->n_velocity_bcs;
+    const int ntb = pn_temp ? (int)pn_tval.size() : d->n_temperature_bcs;
+    std::vector<double> vbc(std::max(1, nvb) * 3, 0.0), tbc(std::max(1, ntb), 0.0);
+    for (int b = 0; b < nvb; b++)
+        for (int q = 0; q < 3; q++)
+            vbc[b * 3 + q] = pn_vel ? (b < (int)pn_vval[q].size() ? pn_vval[q][b] : 0.0) : d->velocity_bcs[b].value[q];
+    for (int b = 0; b < ntb; b++) tbc[b] = pn_temp ? pn_tval[b] : d->temperature_bcs[b].value[0];
     if ((rc = dalloc(h, &h->vbc_val, vbc.size())) || (rc = dalloc(h, &h->tbc_val, tbc.size()))) return rc;
 
     std::vector<DevMaterial> dm(MAX_PHASES);
@@ -1896,7 +1943,8 @@ int snac_gpu_output_open(snac_gpu* h, const char* output_path, unsigned rank, un
     o->checkpoint_every = checkpoint_every;
     o->max_steps = max_time_steps;
     const bool plastic = h->constitutive == SNAC_RHEOLOGY_PLASTIC || h->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC;
-    const bool visc = h->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC;
+    // viscosity records: SnacViscoPlastic's (viscoplastic/Output.c) and SnacMaxwell's (maxwell/Output.c)
+    const bool visc = h->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC || h->constitutive == SNAC_RHEOLOGY_MAXWELL;
     for (int i = 0; i < OutputState::NF; i++) {
         if ((i == OutputState::D_PL || i == OutputState::C_PL) && !plastic) continue;
         if ((i == OutputState::D_VI || i == OutputState::C_VI) && !visc) continue;
@@ -1972,6 +2020,7 @@ int snac_gpu_write_output(snac_gpu* h) {
     using S = OutputState;
     float *co = nullptr, *ve = nullptr, *fo = nullptr, *te = nullptr, *cco = nullptr, *cve = nullptr, *cte = nullptr;
     ElemOut E{};
+    E.maxwell = h->constitutive == SNAC_RHEOLOGY_MAXWELL;
     if (dump) {
         E.strain_rate = (float*)take(S::D_SR, ne * 4);
         E.stress = (float*)take(S::D_ST, ne * 4);
@@ -1991,7 +2040,7 @@ int snac_gpu_write_output(snac_gpu* h) {
         cve = (float*)take(S::C_VE, nn * 12);
         E.phase_cp = (int*)take(S::C_PH, ne * 4);
         E.eps_cp = (float*)take(S::C_PL, ne * 40);
-        E.log_visc_cp = (float*)take(S::C_VI, ne * 40);
+        E.log_visc_cp = (float*)take(S::C_VI, ne * (h->constitutive == SNAC_RHEOLOGY_MAXWELL ? 4 : 40));
         cte = (float*)take(S::C_TE, nn * 4);
     }
     o->scal_off = off;

@@ -47,6 +47,7 @@ struct ElemOut {
     // checkpoint
     float *tensor_cp, *eps_cp, *log_visc_cp;
     int* phase_cp;
+    int maxwell;  // SnacMaxwell's viscosity records (maxwell/Output.c) instead of SnacViscoPlastic's
 };
 
 // element records: one thread per element
@@ -90,6 +91,16 @@ __global__ void k_out_elements(Mesh m, Fields F, ElemOut O) {
             for (int a = 0; a < 6; a++) O.tensor_cp[(e * NT + t) * 6 + a] = (float)S[t * 6 + a];
     if (O.eps_cp && F.eps_p)
         for (int t = 0; t < NT; t++) O.eps_cp[e * NT + t] = (float)F.eps_p[e * NT + t];
+    if (O.maxwell && F.visc && (O.log_visc || O.log_visc_cp)) {
+        // maxwell/Output.c:57-118: the tet mean accumulated in a float, its
+        // log10 when positive; dump and checkpoint both write this one value
+        float viscosity = 0.0f;
+        for (int t = 0; t < NT; t++) viscosity += F.visc[e * NT + t] / NT;
+        if (viscosity > 0.0) viscosity = (float)log10((double)viscosity);  // C: the float promotes to double
+        if (O.log_visc) O.log_visc[e] = viscosity;
+        if (O.log_visc_cp) O.log_visc_cp[e] = viscosity;
+        return;
+    }
     if (O.log_visc && F.visc) {
         // viscoplastic/Output.c: log10 of the mean tet viscosity
         double viscosity = 0.0f;

@@ -315,6 +315,49 @@ def test_c2_full_size_first_steps_bitwise():
     assert_bitwise(g, c)
 
 
+def _host_threads():
+    import os
+    try:
+        return max(1, len(os.sched_getaffinity(0)))
+    except (AttributeError, OSError):
+        return os.cpu_count() or 1
+
+
+def test_c2_full_size_200_steps_bitwise_against_the_reference():
+    """The Mohr-Coulomb workload at full size (64 x 32 x 64 hex) over 200 steps,
+    against the reference's own sources (libsnacref_mt.so: the serial build's
+    bits, its element and node loops on the host's threads): bitwise, at
+    the midpoint and the end."""
+    cfg = W.c2_plastic()
+    g = SnacContext(cfg)
+    c = Checker(cfg, "reference_mt", threads=_host_threads())
+    g.time_step_zero()
+    c.time_step_zero()
+    for _ in range(2):
+        g.step(100)
+        c.step(100)
+        assert_bitwise(g, c)
+
+
+def test_c3_full_size_20_steps_against_the_reference():
+    """The Maxwell visco-plastic workload with temperature at full size (128 x 64 x 128,
+    ~1M hex) over 20 steps against the reference's own sources: within 1e-9 in
+    velocity, stress and temperature (device Arrhenius viscosity), 1e-6 in
+    the viscosity itself and where tets yield (plastic strain)."""
+    cfg = W.c3_viscoplastic()
+    g = SnacContext(cfg)
+    c = Checker(cfg, "reference_mt", threads=_host_threads())
+    g.time_step_zero()
+    c.time_step_zero()
+    g.step(20)
+    c.step(20)
+    sg, sc = g.state(), c.state()
+    for f in ("velocity", "stress", "temperature", "coord"):
+        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, (f, relerr(getattr(sg, f), getattr(sc, f)))
+    for f in ("viscosity", "plastic_strain"):
+        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-6, (f, relerr(getattr(sg, f), getattr(sc, f)))
+
+
 def test_c3_full_size_first_steps_within_tolerance():
     """The Maxwell visco-plastic workload at full size (128 x 64 x 128, ~1M hex): three
     steps (the unfused first step, then the fused temperature step) against the oracle."""
