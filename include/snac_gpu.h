@@ -321,6 +321,13 @@ int  snac_gpu_device_bytes(const snac_gpu* h, long long* bytes);
 /* The handle's cudaStream_t, as a void* (for event timing by callers). */
 void* snac_gpu_stream(snac_gpu* h);
 int  snac_gpu_device_count(void);
+/* Measurement helper (no counterpart in the reference): the current
+ * device's FP64 throughput, in fused multiply-adds per second (one FP64
+ * instruction per thread each), from independent FMA chains over a grid of
+ * 8 blocks per SM; the best of three timed launches after a warm-up.  The
+ * FP64 roofline of a kernel is its FP64 instructions per second against
+ * this rate. */
+int  snac_gpu_fp64_rate(double* fma_per_second);
 /* Self-test of the straight-line correctly rounded division the kernels use
  * (csrc/snac_device.cuh): n random operand pairs (wide exponent range,
  * signed zeros, exact quotients and ties) compared bit for bit with the

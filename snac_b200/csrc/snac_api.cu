@@ -589,6 +589,58 @@ int snac_gpu_selftest_division(long long n, unsigned long long seed, long long* 
     return 0;
 }
 
+// FP64 throughput of this GPU: eight independent FMA chains per thread, the
+// grid a multiple of the SM count.  The result never equals the sentinel for
+// these inputs (every chain converges to c / (1 - b) = 1e3), so the chains
+// stay live and the store never happens.
+__global__ void k_fp64_rate(int iters, double b, double c, double* sink) {
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; k++) a[k] = 1.0 + 1.0e-3 * (double)(threadIdx.x + k);
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 8; k++) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; k++) s += a[k];
+    if (s == -1.0) sink[0] = s;
+}
+
+int snac_gpu_fp64_rate(double* fma_per_second) {
+    if (!fma_per_second) return SNAC_GPU_EINVAL;
+    int dev = 0, sms = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return SNAC_GPU_ENODEV;
+    double* sink = nullptr;
+    if (cudaMalloc(&sink, sizeof(double)) != cudaSuccess) return SNAC_GPU_ENOMEM;
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    const int iters = 4096, threads = 256, blocks = sms * 8;
+    double best = 0.0;
+    cudaError_t e = cudaSuccess;
+    for (int rep = 0; rep < 4 && e == cudaSuccess; rep++) {  // the first launch warms up
+        cudaEventRecord(a);
+        k_fp64_rate<<<blocks, threads>>>(iters, 0.999, 1.0, sink);
+        cudaEventRecord(b);
+        e = cudaEventSynchronize(b);
+        float ms = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+        if (rep > 0 && e == cudaSuccess && ms > 0.0f) {
+            const double rate = (double)blocks * threads * 8.0 * iters / (ms * 1.0e-3);
+            if (rate > best) best = rate;
+        }
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    cudaFree(sink);
+    if (e != cudaSuccess) return SNAC_GPU_ECUDA;
+    *fma_per_second = best;
+    return 0;
+}
+
 int snac_gpu_device_count(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
