@@ -57,6 +57,12 @@ NCU_TRAFFIC = {("c2", "k_fused_step"): 83.648000e6 + 167.135744e6}
 # profiles/k_fused_stress_viscoplastic_128x64x128.md)
 NCU_PIPES = {("c2", "k_fused_step"): {"fp64_pipe": 0.383, "issue_active": 0.455, "dram_throughput": 0.179},
              ("c3", "k_fused_stress"): {"fp64_pipe": 0.374, "dram_throughput": 0.188}}
+# FP64 instructions (thread level: DADD, DMUL, DFMA) of one launch of the
+# dominant kernel, from one ncu capture of it on the same workload
+# (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum); None
+# where none was taken.  With the device's FP64 rate, measured live by
+# snac_gpu_fp64_rate, they give the kernel's FP64 roofline.
+NCU_FP64 = {}
 ARITHMETIC = {
     "c1": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
     "c2": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
@@ -78,6 +84,36 @@ def algorithmic_bytes(workload: str) -> float:
 def make_workload(name: str):
     from snac_b200 import workloads as W
     return {"c1": W.c1_elastic, "c2": W.c2_plastic, "c3": W.c3_viscoplastic}[name]()
+
+
+def fp64_rate():
+    """FP64 instructions per second per GPU (independent FMA chains), measured
+    on the current device; None if the library cannot run the probe."""
+    import ctypes as C
+    from snac_b200.context import load_library
+    try:
+        lib = load_library()
+        lib.snac_gpu_fp64_rate.argtypes = [C.POINTER(C.c_double)]
+        lib.snac_gpu_fp64_rate.restype = C.c_int
+        r = C.c_double(0.0)
+        return r.value if lib.snac_gpu_fp64_rate(C.byref(r)) == 0 and r.value > 0 else None
+    except (OSError, AttributeError):
+        return None
+
+
+def fp64_roofline(workload: str, kernel: str, kernel_ms: float):
+    """The dominant kernel's FP64 instruction rate against the device's."""
+    counts = NCU_FP64.get((workload, kernel))
+    rate = fp64_rate()
+    out = {"peak_inst_per_s": rate, "peak_source": "snac_gpu_fp64_rate (measured in this run)",
+           "counts_per_launch": counts, "achieved_inst_per_s": None, "frac": None}
+    if counts and rate:
+        inst = counts["dadd"] + counts["dmul"] + counts["dfma"]
+        out["achieved_inst_per_s"] = inst / (kernel_ms / 1e3)
+        out["frac"] = out["achieved_inst_per_s"] / rate
+        out["achieved_tflops"] = (counts["dadd"] + counts["dmul"] + 2 * counts["dfma"]) / (kernel_ms / 1e3) / 1e12
+        out["peak_tflops"] = 2 * rate / 1e12
+    return out
 
 
 def load_peaks():
@@ -412,6 +448,7 @@ def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
             "roofline": {"bound": "hbm", "achieved": achieved_kernel, "peak": peak, "unit": "GB/s",
                          "frac": achieved_kernel / peak, "traffic": NCU_TRAFFIC.get((workload, top)),
                          "kernel": top, "ncu_pipes": NCU_PIPES.get((workload, top)),
+                         "fp64": fp64_roofline(workload, top, kern_ms[top]),
                          "kernel_ms": kern_ms[top], "algorithmic_bytes_per_hex": kb,
                          "peak_source": peak_kind,
                          "step": {"achieved": achieved_step, "frac": achieved_step / peak,

@@ -17,7 +17,9 @@ from typing import Optional
 from .abi import NT, STATUS_NAMES, BatchTuning, Desc, KernelTime, Scalars, SnacConfig, State, StateView
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libsnac_b200.so")
+# $SNAC_B200_LIB selects another build of the library (e.g. a variant built
+# with different compile-time options, for comparison)
+LIB_PATH = os.environ.get("SNAC_B200_LIB") or os.path.join(HERE, "libsnac_b200.so")
 
 
 class SnacError(RuntimeError):

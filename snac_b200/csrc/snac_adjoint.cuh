@@ -244,9 +244,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     const double VS = 2.0 * (vsum * 0.5);
     const double zVS = recip(VS);
     const double tr1 = dv3(sr[0] + sr[1] + sr[2]);
+    const double tr1V = tr1 * g.V;  // the term formed on its own lane, as the forward does
     double P1 = 0.0f;
 #pragma unroll
-    for (int u = 0; u < NT; u++) P1 += grp(tr1, s.base, u) * grp(g.V, s.base, u);
+    for (int u = 0; u < NT; u++) P1 += grp(tr1V, s.base, u);
     const double corr1 = -1.0f * tr1 + dvz(P1, VS, zVS);
     sr[0] += corr1;
     sr[1] += corr1;
@@ -413,9 +414,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     }
     // stress averaging over the hex
     const double trS = dv3(st[0] + st[1] + st[2]);
+    const double trSV = trS * g.V;
     double P2 = 0.0f;
 #pragma unroll
-    for (int u = 0; u < NT; u++) P2 += grp(trS, s.base, u) * grp(g.V, s.base, u);
+    for (int u = 0; u < NT; u++) P2 += grp(trSV, s.base, u);
     const double corr2 = -1.0f * trS + dvz(P2, VS, zVS);
     double sa[6];
 #pragma unroll

@@ -712,6 +712,11 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     c.traction = d->traction_bc ? 1 : 0;
     c.topo_kappa = d->topo_kappa;
     c.topo_crit = d->topo_grad_criterion;
+    {
+        int dev = 0, sms = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess && cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess)
+            c.prefetch_ahead = sms * SNAC_ELEM_MINB;
+    }
     c.pisos = d->pisos;  // replaced below when the hydrostatic IC runs here
     c.rzbo = d->rzbo;
     if (shared) {

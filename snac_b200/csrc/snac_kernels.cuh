@@ -80,6 +80,7 @@ struct Config {
     int traction;         // SnacTractionBC on Snac_EP_Force (after Winkler)
     double topo_kappa, topo_crit;  // surface-topography diffusion
     double pisos, rzbo;   // its isostatic pressure and reference bottom depth
+    int prefetch_ahead;   // element blocks resident at once (SMs x blocks per SM): the L2 prefetch distance
     // phase 0, the only phase of a model without a per-element phase array:
     // the element kernels of such models read it from their parameters
     // (constant-bank operands) instead of loading it from the phase table
@@ -204,6 +205,37 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
     }
 }
 
+// Everything the stress update reads from global memory besides the
+// corners and the stress, loaded at the start of the element kernels: the
+// face stash below is a compiler barrier, so a load written after it could
+// not be moved above it and would wait a full memory round trip in the
+// middle of the tet's arithmetic.
+struct TetIn {
+    double eps_p;                 // plastic strain (plastic, visco-plastic)
+    double coh, fric, visc;       // per-element parameter scales (1 without them)
+    double dt, dt_rot;            // this step's dt and the pending rotation's
+    double sos, inertial_density0;
+    int want;                     // element scalars wanted (a dump follows this step)
+};
+
+template <int PLUGIN>
+__device__ __forceinline__ TetIn load_tet_in(const Fields& F, const TetSlot& s) {
+    TetIn in;
+    in.eps_p = 0.0;
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
+        in.eps_p = s.active ? F.eps_p[s.q] : 0.0;
+    in.coh = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
+    in.fric = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
+    in.visc = (F.visc_scale && s.active) ? F.visc_scale[s.e] : 1.0;
+    const DevScalars* sc = F.sc;
+    in.dt = sc->dt;
+    in.dt_rot = sc->dt_rot;
+    in.sos = sc->speed_of_sound;
+    in.inertial_density0 = sc->inertial_density0;
+    in.want = F.escal != nullptr && sc->want_scalars;
+    return in;
+}
+
 // ======================================================================================
 // Snac_EP_CalcStresses: StrainRate.c:49-305, Stress.c:53-172 and the constitutive hook
 // ======================================================================================
@@ -245,7 +277,8 @@ __device__ __forceinline__ void unstash_faces(TetGeom& g) {
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const V3 v[4], const double T[4], const TetGeom& g, double st[6],
-                                              const double dt) {
+                                              const TetIn& in) {
+    const double dt = in.dt;
     double sr[6];
     tet_strain_rate(v, g, sr);
 
@@ -254,16 +287,19 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     double elemVolume = 2.0 * (vsum * 0.5);
     // mixed discretisation, StrainRate.c:272-289
     double trace = dv3(sr[0] + sr[1] + sr[2]);
+    // each term trace_u * V_u is formed on its own lane and gathered (the same
+    // product the sum would form from the two gathered factors)
+    const double traceV = trace * g.V;
     double partial = 0.0f;
 #pragma unroll
-    for (int u = 0; u < NT; u++) partial += grp(trace, s.base, u) * grp(g.V, s.base, u);
+    for (int u = 0; u < NT; u++) partial += grp(traceV, s.base, u);
     const double zE = recip(elemVolume);
     double corr = -1.0f * trace + dvz(partial, elemVolume, zE);
     sr[0] += corr;
     sr[1] += corr;
     sr[2] += corr;
     // scalar element outputs for the dump writers, on the steps that need them
-    const bool want = F.escal != nullptr && F.sc->want_scalars;
+    const bool want = in.want;
     if (want) {
         // StrainRate.c:284-304
         double srVolAvg = grp_sum(sr[1] * sr[2] + sr[2] * sr[0] + sr[0] * sr[1], s.base);
@@ -281,9 +317,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     stash_faces(g);
     const int ph = s.active ? phase_of(F, s.e) : 0;
     const DevMaterial& M = ONE ? cfg.m0 : F.mats[ph];  // ONE: the model has one phase
-    double eps_p = 0.0, eta = 0.0;
-    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
-        eps_p = s.active ? F.eps_p[s.q] : 0.0;
+    double eps_p = in.eps_p, eta = 0.0;
 
     double sp[3] = {0, 0, 0}, cn[3][3];
     // softening-table lookup results of this tet (for the carry-over between tets)
@@ -357,7 +391,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double avgTemp = 0.0;
             for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
             double refvisc = M.refvisc;
-            if (F.visc_scale && s.active) refvisc = M.refvisc * F.visc_scale[s.e];
+            if (F.visc_scale && s.active) refvisc = M.refvisc * in.visc;
             eta = arrhenius_viscosity(M, refvisc, srJ2, avgTemp);
             if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
             maxwell_update(st, e, stressd, straind, ts3, trace_strain, M.mu, eta, dt, bulkm);
@@ -365,8 +399,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         // piecewise-linear softening (plastic/Constitutive.c:133-159 with break and
         // clamp; viscoplastic/Constitutive.c:279-293 without either: the last
         // matching segment wins)
-        const double cs = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
-        const double fsc = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
+        const double cs = in.coh;
+        const double fsc = in.fric;
         for (int i = 0; i < M.nsegments; i++) {
             const double pl1 = M.plstrain[i];
             const double pl2 = M.plstrain[i + 1];
@@ -453,9 +487,10 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 
     // trace averaging over the 10 tets, Stress.c:87-137
     double traceS = dv3(st[0] + st[1] + st[2]);
+    const double traceSV = traceS * g.V;
     double partialS = 0.0f;
 #pragma unroll
-    for (int u = 0; u < NT; u++) partialS += grp(traceS, s.base, u) * grp(g.V, s.base, u);
+    for (int u = 0; u < NT; u++) partialS += grp(traceSV, s.base, u);
     const double avgTrace = dvz(partialS, elemVolume, zE);
     double cs2 = -1.0f * traceS + avgTrace;
     st[0] += cs2;
@@ -530,8 +565,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
-            const double sos = F.sc->speed_of_sound;
-            const double inertialDensity = ONE ? F.sc->inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
+            const double sos = in.sos;
+            const double inertialDensity = ONE ? in.inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
             F.fmass[qt] = factor4 * inertialDensity * gf.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
@@ -568,6 +603,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
+    const TetIn in = load_tet_in<PLUGIN>(F, s);
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -577,7 +613,7 @@ __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields
     if (s.active) {
         load_stress(F, s.q, st);
     }
-    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, in);
 }
 
 template <int PLUGIN, bool ONE>
@@ -609,9 +645,10 @@ template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb,
                                                   bool count_step = true) {
     TetSlot s = tet_slot(m, lb);
+    const TetIn in = load_tet_in<PLUGIN>(F, s);
     if (count_step && lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
         F.sc->time_step += 1;
-        F.sc->current_time += F.sc->dt;
+        F.sc->current_time += in.dt;
     }
     V3 c[4], v[4];
     double T[4], T0[4];
@@ -619,12 +656,45 @@ __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F
     TetGeom g;
     tet_geometry(c, g);
     double st[6] = {0, 0, 0, 0, 0, 0};
-    element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
-    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+    element_update_tet<PLUGIN>(F, cfg, s, v, g, in.dt_rot, st);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, in);
+}
+
+#ifndef SNAC_L2_PREFETCH
+#define SNAC_L2_PREFETCH 0
+#endif
+// L2 prefetch of what element block `blk` will read (the block one wave of
+// resident blocks later): the corner nodes of its hexes, one (hex, corner)
+// per thread, and its stress, plastic-strain and cohesion-scale rows as bulk
+// prefetches.  Every address lies inside its array (hexes < ne, nodes of
+// those hexes) and the bulk ranges start on 16-byte boundaries and are
+// multiples of 16 bytes (480 and 80 bytes per hex; the 8-byte scale rows are
+// rounded down).  A prefetch changes no value.
+__device__ __forceinline__ void prefetch_block(const Mesh& m, const Fields& F, long long blk) {
+    const long long e0 = blk * ELEM_PER_BLOCK;
+    if (e0 >= m.ne) return;
+    const int nh = (int)((m.ne - e0) < ELEM_PER_BLOCK ? (m.ne - e0) : ELEM_PER_BLOCK);
+    const int t = threadIdx.x;
+    if (t < nh * 8) {
+        int i, j, k;
+        elem_ijk(m, e0 + t / 8, i, j, k);
+        const long long n = corner_node(m, i, j, k, t % 8);
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.pos + n));
+        asm volatile("prefetch.global.L2 [%0];" ::"l"(F.vel + n));
+    } else if (t == ELEM_WARPS * 32 - 1) {
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F.stress + e0 * NT * 6), "r"(nh * NT * 48));
+    } else if (t == ELEM_WARPS * 32 - 2 && F.eps_p) {
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F.eps_p + e0 * NT), "r"(nh * NT * 8));
+    } else if (t == ELEM_WARPS * 32 - 3 && F.coh_scale && (nh * 8) / 16 > 0) {
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(F.coh_scale + e0), "r"((nh * 8) / 16 * 16));
+    }
 }
 
 template <int PLUGIN, bool ONE>
 __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_fused_step(Mesh m, Fields F, Config cfg) {
+#if SNAC_L2_PREFETCH
+    if (cfg.prefetch_ahead > 0) prefetch_block(m, F, (long long)blockIdx.x + cfg.prefetch_ahead);
+#endif
     k_fused_step_body<PLUGIN, ONE>(m, F, cfg, blockIdx.x);
 }
 
