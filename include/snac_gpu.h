@@ -82,7 +82,9 @@ typedef struct snac_material {
     double alpha, beta;      /* thermal expansion, compressibility */
     double lambda, mu;
     int    nsegments;        /* piecewise-linear softening     */
-    int    yield_mohr_coulomb; /* 1 (mohrcoulomb); druckerprager is SNAC_GPU_ENOTSUP */
+    int    yield_mohr_coulomb; /* 1: mohrcoulomb; 0: druckerprager, which only the visco-plastic hook
+                                  has (viscoplastic/Constitutive.c:372-518; the plastic hook always
+                                  takes Mohr-Coulomb, plastic/Constitutive.c:58-247) */
     double plstrain[SNAC_MAX_SEGMENTS + 1];
     double friction_angle[SNAC_MAX_SEGMENTS + 1];   /* degrees */
     double dilation_angle[SNAC_MAX_SEGMENTS + 1];   /* degrees */
@@ -173,10 +175,17 @@ typedef struct snac_gpu_desc {
     const double* node_velocity_bc_value;
     const unsigned char* node_temperature_bc_mask;
     const double* node_temperature_bc_value;
+    /* Drucker-Prager phases of the visco-plastic hook: per phase "maxiterations"
+     * and "constitutivetolerance" (Context.c:851-854); NULL = the reference's
+     * defaults, 1 and 1e-3. */
+    const int*    dp_max_iterations;
+    const double* dp_tolerance;
 } snac_gpu_desc;
 
 /* Host-side view of the state for upload / download.  NULL members are
- * skipped.  Sizes: nn*3, nn*3, ne*10*6, ne*10, ne*10, nn, nn*3, nn. */
+ * skipped.  Sizes: nn*3, nn*3, ne*10*6, ne*10, ne*10, nn, nn*3, nn, ne*10*6.
+ * A handle created from a version-1 descriptor reads the view without its
+ * last member. */
 typedef struct snac_state_view {
     double* coord;
     double* velocity;
@@ -186,6 +195,10 @@ typedef struct snac_state_view {
     double* temperature;
     double* force;           /* download only: damped nodal force of the last step */
     double* inertial_mass;   /* download only */
+    /* ABI version 2: the visco-plastic plugin's per-tet plastic strain tensor
+     * (plasticstrainTensor, viscoplastic/Element.h; xx, yy, zz, xy, xz, yz),
+     * [ne*10*6]; kept by models with a Drucker-Prager phase, zero otherwise. */
+    double* plastic_strain_tensor;
 } snac_state_view;
 
 typedef struct snac_scalars {

@@ -163,6 +163,13 @@ ExtensionInfo_Index SnacTemperature_ElementHandle = 3;
 ExtensionInfo_Index SnacTemperature_NodeHandle = 0;
 ExtensionInfo_Index SnacTemperature_ContextHandle = 0;
 
+/* printf of the visco-plastic hook (compiled with -Dprintf=shim_quiet_printf):
+ * its messages are dropped, nothing it computes depends on them */
+int shim_quiet_printf(const char* restrict fmt, ...) {
+    (void)fmt;
+    return 0;
+}
+
 int shim_firewall_count = 0;
 char shim_firewall_msg[512];
 void shim_firewall(const char* fmt, ...) {
@@ -598,9 +605,9 @@ ref_ctx* ref_create(const snac_gpu_desc* d, int* status) {
         mm->beta = sm->beta;
         mm->lambda = sm->lambda;
         mm->mu = sm->mu;
-        mm->yieldcriterion = mohrcoulomb;
-        mm->maxiterations = 1;
-        mm->constitutivetolerance = 1.e-3;
+        mm->yieldcriterion = sm->yield_mohr_coulomb ? mohrcoulomb : druckerprager;
+        mm->maxiterations = d->dp_max_iterations ? (unsigned)d->dp_max_iterations[src] : 1u; /* Context.c:851-854 */
+        mm->constitutivetolerance = d->dp_tolerance ? d->dp_tolerance[src] : 1.e-3;
         mm->nsegments = sm->nsegments;
         mm->plstrain = calloc(sm->nsegments + 1, sizeof(double));
         mm->frictionAngle = calloc(sm->nsegments + 1, sizeof(double));
@@ -904,6 +911,16 @@ int ref_get_state(ref_ctx* r, const snac_state_view* v) {
             if (r->constitutive == SNAC_RHEOLOGY_MAXWELL) vis = r->mx[e].viscosity[t];
             if (v->plastic_strain) v->plastic_strain[e * Tetrahedra_Count + t] = ps;
             if (v->viscosity) v->viscosity[e * Tetrahedra_Count + t] = vis;
+            if (v->plastic_strain_tensor) {
+                double* q = &v->plastic_strain_tensor[((size_t)e * Tetrahedra_Count + t) * 6];
+                const StrainTensor* p = &r->vp[e].plasticstrainTensor[t];
+                q[0] = (*p)[0][0];
+                q[1] = (*p)[1][1];
+                q[2] = (*p)[2][2];
+                q[3] = (*p)[0][1];
+                q[4] = (*p)[0][2];
+                q[5] = (*p)[1][2];
+            }
         }
     return 0;
 }
@@ -931,6 +948,16 @@ int ref_set_state(ref_ctx* r, const snac_state_view* v) {
             if (v->plastic_strain) {
                 r->pl[e].plasticStrain[t] = v->plastic_strain[e * Tetrahedra_Count + t];
                 r->vp[e].plasticStrain[t] = v->plastic_strain[e * Tetrahedra_Count + t];
+            }
+            if (v->plastic_strain_tensor) {
+                const double* q = &v->plastic_strain_tensor[((size_t)e * Tetrahedra_Count + t) * 6];
+                StrainTensor* p = &r->vp[e].plasticstrainTensor[t];
+                (*p)[0][0] = q[0];
+                (*p)[1][1] = q[1];
+                (*p)[2][2] = q[2];
+                (*p)[0][1] = q[3];
+                (*p)[0][2] = q[4];
+                (*p)[1][2] = q[5];
             }
         }
     return 0;

@@ -51,6 +51,7 @@ typedef struct {
     double stress[3][3];
     double density, avgTemp;
     double plasticStrain, viscosity;
+    double plasticstrainTensor[3][3]; /* viscoplastic/Element.h (Drucker-Prager phases) */
     double heatFlux[3], thermalStress;
 } so_tet;
 
@@ -77,6 +78,8 @@ struct so_ctx {
     int nmat;
     snac_material* mat;
     unsigned* rheology;         /* per phase */
+    int* maxiterations;         /* per phase, Context.c:851-852 */
+    double* tolerance;          /* per phase, constitutivetolerance, Context.c:853-854 */
     double (*coord)[3];
     double (*vel)[3];
     double (*force)[3];
@@ -561,6 +564,94 @@ static void plastic_constitutive(so_ctx* s, long e) {
 }
 
 /* ---- viscoplastic/Constitutive.c:61-525 (Mohr-Coulomb branch) -------------- */
+/* viscoplastic/Constitutive.c:372-518: the Drucker-Prager return map of one
+ * tetrahedron, after its viscous update.  sd holds the updated deviatoric
+ * diagonal, Stress0 the stress before the viscous update.  Up to
+ * maxiterations passes: from the shear (h > 0) or tension branch, the
+ * plastic strain increments; with more than one pass the viscous update is
+ * redone with them and the yield functions re-evaluated until both fall
+ * below tolerance times their larger first value.  The increments accumulate
+ * in the plastic strain tensor, whose second invariant becomes the plastic
+ * strain.  palam (the previous pass's multiplier, used when a pass gives a
+ * negative one) is an uninitialised variable of the reference's function on
+ * its first use; it starts at 0 here. */
+static void dp_return_map(double (*stress)[3], double sd[3], double Stress0[3][3], double (*strain)[3], double vic1,
+                          double vic2, double rmu, double bulkm, double qphi, double qpsi, double kphi, double st,
+                          double tolerance, int mite, double (*pst)[3], double* plasticStrain) {
+    double I1 = (stress[0][0] + stress[1][1] + stress[2][2]) / 3.;
+    double J2 = sqrt(0.5 * (sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]) + stress[0][1] * stress[0][1] +
+                     stress[0][2] * stress[0][2] + stress[1][2] * stress[1][2]);
+    double fs = J2 + I1 * qphi - kphi;
+    double ft = I1 - st;
+    if (!(fs > 0.0f || ft > 0.0f)) return;
+    double dep0 = 0.0, dep1 = 0.0, dep2 = 0.0, dep01 = 0.0, dep02 = 0.0, dep12 = 0.0, depm;
+    const double tolerf = fs > ft ? tolerance * fs : tolerance * ft;
+    double previousfs = fs, previousft = ft, palam = 0.0, alam;
+    for (int ite = 0; ite < mite; ite++) {
+        const double aP = sqrt(1.0f + qphi * qphi) - qphi;
+        const double sP = kphi - qphi * st;
+        const double h = J2 - sP - aP * (I1 - st);
+        if (h > 0.0f) {
+            alam = fs / (bulkm * qphi * qpsi + rmu);
+            if (alam < 0.0) alam = palam * (previousfs / (previousfs - fs));
+            dep0 = alam * (0.5 * sd[0] / J2 + qpsi / 3.);
+            dep1 = alam * (0.5 * sd[1] / J2 + qpsi / 3.);
+            dep2 = alam * (0.5 * sd[2] / J2 + qpsi / 3.);
+            dep01 = alam * 0.5 * (stress[0][1]) / J2;
+            dep02 = alam * 0.5 * (stress[0][2]) / J2;
+            dep12 = alam * 0.5 * (stress[1][2]) / J2;
+        } else {
+            alam = ft / bulkm;
+            if (alam < 0.0) alam = palam * (previousft / (previousfs - ft));
+            dep0 = alam / 3.;
+            dep1 = alam / 3.;
+            dep2 = alam / 3.;
+        }
+        if (mite == 1) break;
+        depm = (dep0 + dep1 + dep2) / 3.0f;
+        const double trace_strain = strain[0][0] + strain[1][1] + strain[2][2];
+        const double straind0 = strain[0][0] - dep0 - (trace_strain) / 3.0f + depm;
+        const double straind1 = strain[1][1] - dep1 - (trace_strain) / 3.0f + depm;
+        const double straind2 = strain[2][2] - dep2 - (trace_strain) / 3.0f + depm;
+        const double trace_stress = Stress0[0][0] + Stress0[1][1] + Stress0[2][2];
+        sd[0] = Stress0[0][0] - trace_stress / 3.;
+        sd[1] = Stress0[1][1] - trace_stress / 3.;
+        sd[2] = Stress0[2][2] - trace_stress / 3.;
+        sd[0] = (sd[0] * vic1 + 2.0f * rmu * straind0) * vic2;
+        sd[1] = (sd[1] * vic1 + 2.0f * rmu * straind1) * vic2;
+        sd[2] = (sd[2] * vic1 + 2.0f * rmu * straind2) * vic2;
+        stress[0][1] = (Stress0[0][1] * vic1 + 2.0f * rmu * (strain[0][1] - dep01)) * vic2;
+        stress[0][2] = (Stress0[0][2] * vic1 + 2.0f * rmu * (strain[0][2] - dep02)) * vic2;
+        stress[1][2] = (Stress0[1][2] * vic1 + 2.0f * rmu * (strain[1][2] - dep12)) * vic2;
+        const double VolumicStress = trace_stress / 3.0f + bulkm * (trace_strain - 3. * depm);
+        stress[0][0] = sd[0] + VolumicStress;
+        stress[1][1] = sd[1] + VolumicStress;
+        stress[2][2] = sd[2] + VolumicStress;
+        I1 = (stress[0][0] + stress[1][1] + stress[2][2]) / 3.;
+        sd[0] = stress[0][0] - I1;
+        sd[1] = stress[1][1] - I1;
+        sd[2] = stress[2][2] - I1;
+        J2 = sqrt(0.5 * (sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]) + stress[0][1] * stress[0][1] +
+                  stress[0][2] * stress[0][2] + stress[1][2] * stress[1][2]);
+        previousfs = fs;
+        previousft = ft;
+        palam = alam;
+        fs = J2 + I1 * qphi - kphi;
+        ft = I1 - st;
+        if (fs < tolerf && ft < tolerf) break;
+    }
+    pst[0][0] += dep0;
+    pst[1][1] += dep1;
+    pst[2][2] += dep2;
+    pst[0][1] += dep01;
+    pst[0][2] += dep02;
+    pst[1][2] += dep12;
+    depm = (pst[0][0] + pst[1][1] + pst[2][2]) / 3.0f;
+    *plasticStrain = sqrt(0.5f * ((pst[0][0] - depm) * (pst[0][0] - depm) + (pst[1][1] - depm) * (pst[1][1] - depm) +
+                                  (pst[2][2] - depm) * (pst[2][2] - depm)) +
+                          pst[0][1] * pst[0][1] + pst[0][2] * pst[0][2] + pst[1][2] * pst[1][2]);
+}
+
 static void vp_constitutive(so_ctx* s, long e) {
     so_element* el = &s->el[e];
     const snac_material* m = &s->mat[el->material];
@@ -588,6 +679,9 @@ static void vp_constitutive(so_ctx* s, long e) {
             stress[1][1] += tt->thermalStress;
             stress[2][2] += tt->thermalStress;
         }
+        /* the stress before the viscous update (Stress0, :165-170) */
+        double Stress0[3][3];
+        memcpy(Stress0, stress, sizeof Stress0);
         trace_stress = stress[0][0] + stress[1][1] + stress[2][2];
         trace_strain = strain[0][0] + strain[1][1] + strain[2][2];
         straind0 = strain[0][0] - (trace_strain) / 3.0f;
@@ -649,11 +743,18 @@ static void vp_constitutive(so_ctx* s, long e) {
                 if (tmp < st) st = tmp;
             }
         } /* else: assert(0), compiled out of the -DNDEBUG reference build */
-        sphi = sin(frictionAngle * degrad);
-        spsi = sin(dilationAngle * degrad);
-        anphi = (1.0f + sphi) / (1.0f - sphi);
-        anpsi = (1.0f + spsi) / (1.0f - spsi);
-        mc_return_map(sp, cn, stress, &tt->plasticStrain, cohesion, hardening, anphi, anpsi, st, a1, a2);
+        if (m->yield_mohr_coulomb) {
+            sphi = sin(frictionAngle * degrad);
+            spsi = sin(dilationAngle * degrad);
+            anphi = (1.0f + sphi) / (1.0f - sphi);
+            anpsi = (1.0f + spsi) / (1.0f - spsi);
+            mc_return_map(sp, cn, stress, &tt->plasticStrain, cohesion, hardening, anphi, anpsi, st, a1, a2);
+        } else {
+            double sd[3] = {stressd0, stressd1, stressd2};
+            dp_return_map(stress, sd, Stress0, strain, vic1, vic2, rmu, bulkm, tan(frictionAngle * degrad),
+                          tan(dilationAngle * degrad), cohesion, st, s->tolerance[el->material],
+                          s->maxiterations[el->material], tt->plasticstrainTensor, &tt->plasticStrain);
+        }
         depls += tt->plasticStrain * tt->volume;
         totalVolume += tt->volume;
     }
@@ -1362,6 +1463,14 @@ so_ctx* so_create(const snac_gpu_desc* d, int* status) {
     }
     if (!per_elem)
         for (int m = 0; m < d->n_materials; m++) s->mat[m] = d->materials[m];
+    /* Drucker-Prager iteration controls of each phase (defaults 1 and 1e-3) */
+    s->maxiterations = calloc(s->nmat, sizeof(int));
+    s->tolerance = calloc(s->nmat, sizeof(double));
+    for (int p = 0; p < s->nmat; p++) {
+        int src = per_elem ? (d->element_material ? d->element_material[p] : 0) : p;
+        s->maxiterations[p] = d->dp_max_iterations ? d->dp_max_iterations[src] : 1;
+        s->tolerance[p] = d->dp_tolerance ? d->dp_tolerance[src] : 1.e-3;
+    }
     /* rheology is hard-wired to Elastic (Context.c:834); the plugin ICs OR in
      * their bit (plastic/InitialConditions.c:57, viscoplastic/InitialConditions.c:64,
      * maxwell/InitialConditions.c:53 - phase 0 only) */
@@ -1476,6 +1585,8 @@ void so_destroy(so_ctx* s) {
     free(s->tbc_val);
     free(s->mat);
     free(s->rheology);
+    free(s->maxiterations);
+    free(s->tolerance);
     free(s);
 }
 
@@ -1505,6 +1616,15 @@ int so_get_state(so_ctx* s, const snac_state_view* v) {
             }
             if (v->plastic_strain) v->plastic_strain[e * NT + t] = tt->plasticStrain;
             if (v->viscosity) v->viscosity[e * NT + t] = tt->viscosity;
+            if (v->plastic_strain_tensor) {
+                double* q = &v->plastic_strain_tensor[(e * NT + t) * 6];
+                q[0] = tt->plasticstrainTensor[0][0];
+                q[1] = tt->plasticstrainTensor[1][1];
+                q[2] = tt->plasticstrainTensor[2][2];
+                q[3] = tt->plasticstrainTensor[0][1];
+                q[4] = tt->plasticstrainTensor[0][2];
+                q[5] = tt->plasticstrainTensor[1][2];
+            }
         }
     return 0;
 }
@@ -1531,6 +1651,15 @@ int so_set_state(so_ctx* s, const snac_state_view* v) {
             }
             if (v->plastic_strain) tt->plasticStrain = v->plastic_strain[e * NT + t];
             if (v->viscosity) tt->viscosity = v->viscosity[e * NT + t];
+            if (v->plastic_strain_tensor) {
+                const double* q = &v->plastic_strain_tensor[(e * NT + t) * 6];
+                tt->plasticstrainTensor[0][0] = q[0];
+                tt->plasticstrainTensor[1][1] = q[1];
+                tt->plasticstrainTensor[2][2] = q[2];
+                tt->plasticstrainTensor[0][1] = q[3];
+                tt->plasticstrainTensor[0][2] = q[4];
+                tt->plasticstrainTensor[1][2] = q[5];
+            }
         }
     return 0;
 }

@@ -111,12 +111,14 @@ class Desc(C.Structure):
         ("pisos", C.c_double), ("rzbo", C.c_double),
         ("node_velocity_bc_mask", C.POINTER(C.c_ubyte)), ("node_velocity_bc_value", _DP),
         ("node_temperature_bc_mask", C.POINTER(C.c_ubyte)), ("node_temperature_bc_value", _DP),
+        ("dp_max_iterations", _IP), ("dp_tolerance", _DP),
     ]
 
 
 class StateView(C.Structure):
     _fields_ = [("coord", _DP), ("velocity", _DP), ("stress", _DP), ("plastic_strain", _DP),
-                ("viscosity", _DP), ("temperature", _DP), ("force", _DP), ("inertial_mass", _DP)]
+                ("viscosity", _DP), ("temperature", _DP), ("force", _DP), ("inertial_mass", _DP),
+                ("plastic_strain_tensor", _DP)]
 
 
 class KernelTime(C.Structure):
@@ -266,6 +268,9 @@ class SnacConfig:
             return a.ctypes.data_as(_IP if dtype == np.int32 else _DP)
 
         ne, nn = self.n_elements, self.n_nodes
+        if any(m.get("yieldcriterion", "mohrcoulomb") != "mohrcoulomb" for m in self.materials):
+            d.dp_max_iterations = arr([int(m.get("maxiterations", 1)) for m in self.materials], np.int32)
+            d.dp_tolerance = arr([float(m.get("constitutivetolerance", 1.0e-3)) for m in self.materials], np.float64)
         d.element_material = arr(self.element_material, np.int32, ne)
         d.element_cohesion_scale = arr(self.element_cohesion_scale, np.float64, ne)
         d.element_friction_scale = arr(self.element_friction_scale, np.float64, ne)
@@ -308,13 +313,19 @@ class State:
     temperature: np.ndarray
     force: np.ndarray
     inertial_mass: np.ndarray
+    plastic_strain_tensor: np.ndarray = None  # [ne, 10, 6], Drucker-Prager phases
+
+    def __post_init__(self):
+        if self.plastic_strain_tensor is None:
+            self.plastic_strain_tensor = np.zeros(self.stress.shape)
 
     @classmethod
     def empty(cls, n_elements: int, n_nodes: int) -> "State":
         z = np.zeros
         return cls(coord=z((n_nodes, 3)), velocity=z((n_nodes, 3)), stress=z((n_elements, NT, 6)),
                    plastic_strain=z((n_elements, NT)), viscosity=z((n_elements, NT)),
-                   temperature=z(n_nodes), force=z((n_nodes, 3)), inertial_mass=z(n_nodes))
+                   temperature=z(n_nodes), force=z((n_nodes, 3)), inertial_mass=z(n_nodes),
+                   plastic_strain_tensor=z((n_elements, NT, 6)))
 
     def view(self, fields: Optional[Sequence[str]] = None) -> StateView:
         v = StateView()

@@ -69,6 +69,9 @@ struct snac_gpu {
     double4* force = nullptr;
     double* stress = nullptr;
     double* eps_p = nullptr;
+    double* pst = nullptr;   // plastic strain tensor [nq][6] (visco-plastic with a Drucker-Prager phase)
+    int dp = 0;              // the visco-plastic model has a Drucker-Prager phase: SNAC_VP_DP kernel instances
+    int abi = SNAC_GPU_ABI_VERSION;  // version of the descriptor it was created from (state-view size)
     double* visc = nullptr;
     double* density = nullptr;
     double* vol = nullptr;
@@ -151,7 +154,7 @@ bool wall_has(int wall, int i, int j, int k, int nnx, int nny, int nnz) {
 
 // Host copy of a phase for the device.  Angles that are constant over the
 // whole softening table get their sin/tan from the host C library.
-DevMaterial to_dev(const snac_material& s, bool fric_scaled) {
+DevMaterial to_dev(const snac_material& s, bool fric_scaled, int dp_maxit, double dp_tol) {
     DevMaterial d;
     memset(&d, 0, sizeof d);
     d.density = s.density;
@@ -194,6 +197,9 @@ DevMaterial to_dev(const snac_material& s, bool fric_scaled) {
     d.tan_fric0 = tan(d.fric0 * degrad);
     d.dil0 = s.dilation_angle[0];
     d.sin_dil0 = sin(d.dil0 * degrad);
+    d.tan_dil0 = tan(d.dil0 * degrad);
+    d.dp_maxit = dp_maxit;
+    d.dp_tol = dp_tol;
     d.anphi0 = (1.0f + d.sin_fric0) / (1.0f - d.sin_fric0);
     d.anpsi0 = (1.0f + d.sin_dil0) / (1.0f - d.sin_dil0);
     d.sq_anphi0 = sqrt(d.anphi0);
@@ -211,6 +217,7 @@ Fields fields_at(const snac_gpu* h, int parity) {
     F.force = h->force;
     F.stress = h->stress;
     F.eps_p = h->eps_p;
+    F.pst = h->pst;
     F.visc = h->visc;
     F.density = h->density;
     F.vol = h->vol;
@@ -305,7 +312,12 @@ int op_fused_stress(snac_gpu* h) {
     switch (h->constitutive) {
         case SNAC_RHEOLOGY_ELASTIC: launch_fused_stress<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
         case SNAC_RHEOLOGY_PLASTIC: launch_fused_stress<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
-        case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused_stress<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC:
+            if (h->dp)
+                launch_fused_stress<SNAC_VP_DP>(h, F, c);
+            else
+                launch_fused_stress<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c);
+            break;
         case SNAC_RHEOLOGY_MAXWELL: launch_fused_stress<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
     }
     h->launches++;
@@ -324,7 +336,12 @@ int op_calc_stresses(snac_gpu* h) {
     switch (h->constitutive) {
         case SNAC_RHEOLOGY_ELASTIC: launch_stress<SNAC_RHEOLOGY_ELASTIC>(h, F, h->cfg); break;
         case SNAC_RHEOLOGY_PLASTIC: launch_stress<SNAC_RHEOLOGY_PLASTIC>(h, F, h->cfg); break;
-        case SNAC_RHEOLOGY_VISCOPLASTIC: launch_stress<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, h->cfg); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC:
+            if (h->dp)
+                launch_stress<SNAC_VP_DP>(h, F, h->cfg);
+            else
+                launch_stress<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, h->cfg);
+            break;
         case SNAC_RHEOLOGY_MAXWELL: launch_stress<SNAC_RHEOLOGY_MAXWELL>(h, F, h->cfg); break;
     }
     h->launches++;
@@ -369,7 +386,12 @@ int op_fused(snac_gpu* h) {
     switch (h->constitutive) {
         case SNAC_RHEOLOGY_ELASTIC: launch_fused<SNAC_RHEOLOGY_ELASTIC>(h, F, c); break;
         case SNAC_RHEOLOGY_PLASTIC: launch_fused<SNAC_RHEOLOGY_PLASTIC>(h, F, c); break;
-        case SNAC_RHEOLOGY_VISCOPLASTIC: launch_fused<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC:
+            if (h->dp)
+                launch_fused<SNAC_VP_DP>(h, F, c);
+            else
+                launch_fused<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, c);
+            break;
         case SNAC_RHEOLOGY_MAXWELL: launch_fused<SNAC_RHEOLOGY_MAXWELL>(h, F, c); break;
     }
     h->launches++;
@@ -671,9 +693,7 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     if (per_elem && d->constitutive == SNAC_RHEOLOGY_MAXWELL) return SNAC_GPU_ENOTSUP;
     for (int p = 0; p < d->n_materials; p++) {
         if (d->materials[p].nsegments < 0 || d->materials[p].nsegments > SNAC_MAX_SEGMENTS) return SNAC_GPU_EINVAL;
-        if ((d->constitutive == SNAC_RHEOLOGY_PLASTIC || d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) &&
-            !d->materials[p].yield_mohr_coulomb)
-            return SNAC_GPU_ENOTSUP;  // the Drucker-Prager branch is not built
+        if (d->dp_max_iterations && d->dp_max_iterations[p] < 0) return SNAC_GPU_EINVAL;
     }
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev < 1) return SNAC_GPU_ENODEV;
@@ -696,6 +716,10 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     m.ner = (m.ne + 3) & ~3LL;
     h->constitutive = d->constitutive;
     h->temperature = d->temperature;
+    h->abi = d_in->abi_version;
+    if (d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC)  // only the visco-plastic hook has the Drucker-Prager branch
+        for (int p = 0; p < d->n_materials; p++)
+            if (!d->materials[p].yield_mohr_coulomb) h->dp = 1;
     h->n_phases = d->n_materials;
     for (int p = 0; p < d->n_materials; p++)
         if (d->materials[p].alpha != 0.0 || d->materials[p].beta != 0.0) h->has_density = 1;
@@ -738,6 +762,7 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
         if ((rc = dalloc(h, &h->eps_p, nq))) return rc;
     if (d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC || d->constitutive == SNAC_RHEOLOGY_MAXWELL)
         if ((rc = dalloc(h, &h->visc, nq))) return rc;
+    if (h->dp && (rc = dalloc(h, &h->pst, nq * 6))) return rc;
     if (d->constitutive == SNAC_RHEOLOGY_MAXWELL)
         if ((rc = dalloc(h, &h->vol, nq * 2))) return rc;
     if (h->has_density)
@@ -850,7 +875,9 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     if ((rc = dalloc(h, &h->vbc_val, vbc.size())) || (rc = dalloc(h, &h->tbc_val, tbc.size()))) return rc;
 
     std::vector<DevMaterial> dm(MAX_PHASES);
-    for (int p = 0; p < d->n_materials; p++) dm[p] = to_dev(d->materials[p], d->element_friction_scale != nullptr);
+    for (int p = 0; p < d->n_materials; p++)  // Drucker-Prager controls: Context.c:851-854 defaults 1 and 1e-3
+        dm[p] = to_dev(d->materials[p], d->element_friction_scale != nullptr,
+                       d->dp_max_iterations ? d->dp_max_iterations[p] : 1, d->dp_tolerance ? d->dp_tolerance[p] : 1.e-3);
     if (d->element_material) {
         std::vector<unsigned char> mt(ne);
         for (long long e = 0; e < ne; e++) {
@@ -928,7 +955,7 @@ void snac_gpu_destroy(snac_gpu* h) {
     for (auto& gf : h->graph)
         for (auto& g : gf)
             if (g) cudaGraphExecDestroy(g);
-    void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->visc, h->density, h->vol,
+    void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->pst, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
                     h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr, h->topo_scratch};
     for (void* b : bufs)
@@ -1053,6 +1080,8 @@ int snac_gpu_upload(snac_gpu* h, const snac_state_view* v) {
         CK(cudaMemcpyAsync(h->eps_p, v->plastic_strain, nq * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     if (v->viscosity && h->visc)
         CK(cudaMemcpyAsync(h->visc, v->viscosity, nq * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+    if (h->abi >= 2 && v->plastic_strain_tensor && h->pst)
+        CK(cudaMemcpyAsync(h->pst, v->plastic_strain_tensor, nq * 6 * sizeof(double), cudaMemcpyHostToDevice, h->stream));
     CK(cudaStreamSynchronize(h->stream));  // the caller may reuse its buffers on return
     (void)nn;
     return 0;
@@ -1073,9 +1102,13 @@ int snac_gpu_download(snac_gpu* h, const snac_state_view* v) {
         CK(cudaMemcpyAsync(v->plastic_strain, h->eps_p, nq * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     if (v->viscosity && h->visc)
         CK(cudaMemcpyAsync(v->viscosity, h->visc, nq * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    const bool want_pst = h->abi >= 2 && v->plastic_strain_tensor;
+    if (want_pst && h->pst)
+        CK(cudaMemcpyAsync(v->plastic_strain_tensor, h->pst, nq * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     if (v->plastic_strain && !h->eps_p) memset(v->plastic_strain, 0, nq * sizeof(double));
     if (v->viscosity && !h->visc) memset(v->viscosity, 0, nq * sizeof(double));
+    if (want_pst && !h->pst) memset(v->plastic_strain_tensor, 0, nq * 6 * sizeof(double));
     return 0;
 }
 
@@ -1485,6 +1518,8 @@ int snac_gpu_batch_create(const snac_gpu_desc* descs, int n_models, snac_gpu_bat
             const char* msg = b->models[i] ? b->models[i]->err : "invalid descriptor";
             return bset_err(b, rc, i, "model %d: %s", i, msg[0] ? msg : "invalid descriptor");
         }
+        if (b->models[i]->dp)  // the batched kernels have no Drucker-Prager instances
+            return bset_err(b, SNAC_GPU_ENOTSUP, i, "model %d: Drucker-Prager phases are not batched", i);
         b->any_temp = b->any_temp || b->models[i]->temperature;
         if (topo_on(b->models[i]->cfg))
             return bset_err(b, SNAC_GPU_ENOTSUP, i, "model %d: topography diffusion is not batched", i);
@@ -1723,8 +1758,8 @@ AdjState adj_state(const Snap& z) { return AdjState{z.pos, z.vel, z.force, z.str
 
 int adjoint_supported(snac_gpu* h) {
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "adjoint: time step zero must come first");
-    if (h->constitutive != SNAC_RHEOLOGY_PLASTIC && h->constitutive != SNAC_RHEOLOGY_VISCOPLASTIC)
-        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and visco-plastic hooks are differentiated");
+    if ((h->constitutive != SNAC_RHEOLOGY_PLASTIC && h->constitutive != SNAC_RHEOLOGY_VISCOPLASTIC) || h->dp)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and the Mohr-Coulomb visco-plastic hooks are differentiated");
     if (h->cfg.dt_type != SNAC_DT_CONSTANT)
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: dtType must be constant (dt may not depend on the state)");
     if (h->has_density || h->cfg.thermal_stress || h->cfg.winkler || h->cfg.traction || topo_on(h->cfg))

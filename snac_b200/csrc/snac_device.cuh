@@ -17,6 +17,11 @@
 namespace snac {
 
 constexpr int NT = 10;        // Tetrahedra_Count
+// Kernel instances of the visco-plastic hook for models with a
+// Drucker-Prager phase (the extra state and branch stay out of the
+// Mohr-Coulomb instances' registers).
+constexpr int SNAC_VP_DP = SNAC_RHEOLOGY_VISCOPLASTIC | 0x100;
+__host__ __device__ constexpr bool is_vp(int plugin) { return (plugin & SNAC_RHEOLOGY_VISCOPLASTIC) != 0; }
 constexpr int MAX_PHASES = 32;
 
 // TetrahedraTables.c:42-84 (tets 0-4 are the first five-tet set, 5-9 the second).
@@ -87,7 +92,10 @@ struct DevMaterial {
     // host-evaluated transcendentals (valid when the *_const flag is set)
     int fric_const, dil_const;
     double fric0, sin_fric0, tan_fric0;
-    double dil0, sin_dil0;
+    double dil0, sin_dil0, tan_dil0;
+    // Drucker-Prager phase (yield_mc == 0, visco-plastic hook): maxiterations, constitutivetolerance
+    int dp_maxit;
+    double dp_tol;
 };
 
 // Device-resident scalars of one model (everything a captured step reads).
@@ -543,6 +551,76 @@ __device__ __forceinline__ double tan_fric(const DevMaterial& m, double phi) {
 __device__ __forceinline__ double sin_dil(const DevMaterial& m, double psi) {
     return (m.dil_const && psi == m.dil0) ? m.sin_dil0 : sin(psi * degrad());
 }
+__device__ __forceinline__ double tan_dil(const DevMaterial& m, double psi) {
+    return (m.dil_const && psi == m.dil0) ? m.tan_dil0 : tan(psi * degrad());
+}
+
+// viscoplastic/Constitutive.c:372-518, the Drucker-Prager return map of one
+// tet after its viscous update.  s: the stress (xx, yy, zz, xy, xz, yz); sd:
+// the updated deviatoric diagonal; S0: the stress before the viscous update;
+// e: the strain increment; pst: the accumulated plastic strain tensor.  Up
+// to mite passes: shear (h > 0) or tension increments; with more than one
+// pass the viscous update is redone with them and the yield functions
+// evaluated again until both are below tol times their larger first value.
+// The increments accumulate in pst, whose second invariant becomes eps_p.
+// palam, the previous pass's multiplier for a pass whose own is negative,
+// is an uninitialised function-scope variable in the reference on its first
+// use; here it starts at 0.  IEEE division and square root throughout (a
+// rarely taken path).  Returns whether the tet yielded.
+__device__ __noinline__ bool dp_return_map(double s[6], double sd[3], const double S0[6], const double e[6],
+                                           double vic1, double vic2, double rmu, double bulkm, double qphi,
+                                           double qpsi, double kphi, double st, double tol, int mite, double pst[6],
+                                           double& eps_p) {
+    double I1 = (s[0] + s[1] + s[2]) / 3.;
+    double J2 = sqrt(0.5 * (sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+    double fs = J2 + I1 * qphi - kphi;
+    double ft = I1 - st;
+    if (!(fs > 0.0f || ft > 0.0f)) return false;
+    double dep[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0}, depm;
+    const double tolerf = fs > ft ? tol * fs : tol * ft;
+    double previousfs = fs, previousft = ft, palam = 0.0, alam;
+    for (int ite = 0; ite < mite; ite++) {
+        const double aP = sqrt(1.0f + qphi * qphi) - qphi;
+        const double sP = kphi - qphi * st;
+        const double h = J2 - sP - aP * (I1 - st);
+        if (h > 0.0f) {  // shear
+            alam = fs / (bulkm * qphi * qpsi + rmu);
+            if (alam < 0.0) alam = palam * (previousfs / (previousfs - fs));
+            for (int a = 0; a < 3; a++) dep[a] = alam * (0.5 * sd[a] / J2 + qpsi / 3.);
+            for (int a = 3; a < 6; a++) dep[a] = alam * 0.5 * (s[a]) / J2;
+        } else {  // tension (the shear increments of a previous pass stay)
+            alam = ft / bulkm;
+            if (alam < 0.0) alam = palam * (previousft / (previousfs - ft));
+            for (int a = 0; a < 3; a++) dep[a] = alam / 3.;
+        }
+        if (mite == 1) break;
+        depm = (dep[0] + dep[1] + dep[2]) / 3.0f;
+        const double trace_strain = e[0] + e[1] + e[2];
+        double strd[3];
+        for (int a = 0; a < 3; a++) strd[a] = e[a] - dep[a] - (trace_strain) / 3.0f + depm;
+        const double trace_stress = S0[0] + S0[1] + S0[2];
+        for (int a = 0; a < 3; a++) sd[a] = S0[a] - trace_stress / 3.;
+        for (int a = 0; a < 3; a++) sd[a] = (sd[a] * vic1 + 2.0f * rmu * strd[a]) * vic2;
+        for (int a = 3; a < 6; a++) s[a] = (S0[a] * vic1 + 2.0f * rmu * (e[a] - dep[a])) * vic2;
+        const double VolumicStress = trace_stress / 3.0f + bulkm * (trace_strain - 3. * depm);
+        for (int a = 0; a < 3; a++) s[a] = sd[a] + VolumicStress;
+        I1 = (s[0] + s[1] + s[2]) / 3.;
+        for (int a = 0; a < 3; a++) sd[a] = s[a] - I1;
+        J2 = sqrt(0.5 * (sd[0] * sd[0] + sd[1] * sd[1] + sd[2] * sd[2]) + s[3] * s[3] + s[4] * s[4] + s[5] * s[5]);
+        previousfs = fs;
+        previousft = ft;
+        palam = alam;
+        fs = J2 + I1 * qphi - kphi;
+        ft = I1 - st;
+        if (fs < tolerf && ft < tolerf) break;
+    }
+    for (int a = 0; a < 6; a++) pst[a] += dep[a];
+    depm = (pst[0] + pst[1] + pst[2]) / 3.0f;
+    eps_p = sqrt(0.5f * ((pst[0] - depm) * (pst[0] - depm) + (pst[1] - depm) * (pst[1] - depm) +
+                         (pst[2] - depm) * (pst[2] - depm)) +
+                 pst[3] * pst[3] + pst[4] * pst[4] + pst[5] * pst[5]);
+    return true;
+}
 
 // Mohr-Coulomb composite yield + return map in principal space, shared by
 // plastic/Constitutive.c:180-237 and viscoplastic/Constitutive.c:305-370.
@@ -615,10 +693,11 @@ __device__ __forceinline__ double arrhenius_viscosity(const DevMaterial& M, doub
 // and maxwell/Constitutive.c:146-183 (identical arithmetic).
 __device__ __forceinline__ void maxwell_update(double s[6], const double e[6], double stressd[3],
                                                const double straind[3], double trace_stress3, double trace_strain,
-                                               double rmu, double eta, double dt, double bulkm) {
+                                               double rmu, double eta, double dt, double bulkm, double& vic1,
+                                               double& vic2) {
     double temp = dv(rmu, 2.0f * (eta)) * dt;
-    double vic1 = 1.0f - temp;
-    double vic2 = recip(1.0f + temp);  // RN(1 / x), the same bits as 1.0 / x
+    vic1 = 1.0f - temp;
+    vic2 = recip(1.0f + temp);  // RN(1 / x), the same bits as 1.0 / x
     stressd[0] = (stressd[0] * vic1 + 2.0f * rmu * straind[0]) * vic2;
     stressd[1] = (stressd[1] * vic1 + 2.0f * rmu * straind[1]) * vic2;
     stressd[2] = (stressd[2] * vic1 + 2.0f * rmu * straind[2]) * vic2;
@@ -629,6 +708,12 @@ __device__ __forceinline__ void maxwell_update(double s[6], const double e[6], d
     s[0] = stressd[0] + VolumicStress;
     s[1] = stressd[1] + VolumicStress;
     s[2] = stressd[2] + VolumicStress;
+}
+__device__ __forceinline__ void maxwell_update(double s[6], const double e[6], double stressd[3],
+                                               const double straind[3], double trace_stress3, double trace_strain,
+                                               double rmu, double eta, double dt, double bulkm) {
+    double vic1, vic2;
+    maxwell_update(s, e, stressd, straind, trace_stress3, trace_strain, rmu, eta, dt, bulkm, vic1, vic2);
 }
 
 }  // namespace snac

@@ -50,6 +50,7 @@ struct Fields {
     double4* force;          // damped force (x, y, z) and inertial mass (w)
     double* stress;          // [ne*10][6]
     double* eps_p;           // [ne*10]  plastic strain (plastic, visco-plastic)
+    double* pst;             // [ne*10][6] plastic strain tensor (visco-plastic with a Drucker-Prager phase)
     double* visc;            // [ne*10]  viscosity (visco-plastic, Maxwell)
     double* density;         // [ne*10]  only when some phase has alpha or beta != 0
     double* vol;             // [ne*10][2] volume, old volume (Maxwell)
@@ -213,6 +214,7 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
 struct TetIn {
     double eps_p;                 // plastic strain (plastic, visco-plastic)
     double coh, fric, visc;       // per-element parameter scales (1 without them)
+    double pst[6];                // plastic strain tensor (Drucker-Prager instances)
     double dt, dt_rot;            // this step's dt and the pending rotation's
     double sos, inertial_density0;
     int want;                     // element scalars wanted (a dump follows this step)
@@ -222,8 +224,17 @@ template <int PLUGIN>
 __device__ __forceinline__ TetIn load_tet_in(const Fields& F, const TetSlot& s) {
     TetIn in;
     in.eps_p = 0.0;
-    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || is_vp(PLUGIN))
         in.eps_p = s.active ? F.eps_p[s.q] : 0.0;
+    for (int a = 0; a < 6; a++) in.pst[a] = 0.0;
+    if (PLUGIN == SNAC_VP_DP && s.active) {
+        const double2* p = reinterpret_cast<const double2*>(F.pst + s.q * 6);
+        for (int a = 0; a < 3; a++) {
+            const double2 w = p[a];
+            in.pst[2 * a] = w.x;
+            in.pst[2 * a + 1] = w.y;
+        }
+    }
     in.coh = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
     in.fric = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
     in.visc = (F.visc_scale && s.active) ? F.visc_scale[s.e] : 1.0;
@@ -318,6 +329,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     const int ph = s.active ? phase_of(F, s.e) : 0;
     const DevMaterial& M = ONE ? cfg.m0 : F.mats[ph];  // ONE: the model has one phase
     double eps_p = in.eps_p, eta = 0.0;
+    // what the Drucker-Prager return map needs from the viscous update
+    double dp_sd[3] = {0.0, 0.0, 0.0}, dp_S0[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    double dp_vic1 = 0.0, dp_vic2 = 0.0, dp_bulkm = 0.0;
 
     double sp[3] = {0, 0, 0}, cn[3][3];
     // softening-table lookup results of this tet (for the carry-over between tets)
@@ -375,6 +389,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
                 st[1] += ts;
                 st[2] += ts;
             }
+            if (PLUGIN == SNAC_VP_DP)  // Stress0, viscoplastic/Constitutive.c:165-170
+                for (int a = 0; a < 6; a++) dp_S0[a] = st[a];
             double trace_stress = st[0] + st[1] + st[2];
             double trace_strain = e[0] + e[1] + e[2];
             double straind[3], stressd[3];
@@ -394,7 +410,11 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             if (F.visc_scale && s.active) refvisc = M.refvisc * in.visc;
             eta = arrhenius_viscosity(M, refvisc, srJ2, avgTemp);
             if (s.active && !isfinite(eta)) report(F.sc, SNAC_GPU_ENAN, s.e);
-            maxwell_update(st, e, stressd, straind, ts3, trace_strain, M.mu, eta, dt, bulkm);
+            maxwell_update(st, e, stressd, straind, ts3, trace_strain, M.mu, eta, dt, bulkm, dp_vic1, dp_vic2);
+            if (PLUGIN == SNAC_VP_DP) {
+                for (int a = 0; a < 3; a++) dp_sd[a] = stressd[a];
+                dp_bulkm = bulkm;
+            }
         }
         // piecewise-linear softening (plastic/Constitutive.c:133-159 with break and
         // clamp; viscoplastic/Constitutive.c:279-293 without either: the last
@@ -430,7 +450,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         }
     }
 
-    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC) {
+    double pst[6];
+    for (int a = 0; a < 6; a++) pst[a] = in.pst[a];
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || is_vp(PLUGIN)) {
         // The reference keeps the table values (and the tension cutoff) in
         // variables that outlive the tet loop: a tet whose lookup matched no
         // segment reuses the previous tet's values, 0 before the first match.
@@ -470,18 +492,26 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         }
         if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && s.active && frictionAngle < 0.0f)
             report(F.sc, SNAC_GPU_EPHYSICS, s.e);  // plastic/Constitutive.c:175 abort()
-        double sphi = sin_fric(M, frictionAngle);
-        double spsi = sin_dil(M, dilationAngle);
-        double anphi = fconst ? M.anphi0 : dv(1.0f + sphi, 1.0f - sphi);
-        double anpsi = (M.dil_const && dilationAngle == M.dil0) ? M.anpsi0 : dv(1.0f + spsi, 1.0f - spsi);
-        const double a1 = M.lambda + 2.0f * M.mu;
-        const double a2 = M.lambda;
-        // The reference always computes the principal stresses; they only
-        // matter when the tet yields.  A tet that provably stays inside the
-        // yield surface keeps its trial stress without the eigen-solve.
-        if (!surely_elastic(st, cohesion, anphi, fconst ? M.sq_anphi0 : sqrt(anphi), stc)) {
-            principal_stresses(st, sp, cn);
-            mc_return_map(sp, cn, st, eps_p, cohesion, hardening, anphi, anpsi, stc, a1, a2);
+        if (PLUGIN == SNAC_VP_DP && !M.yield_mc) {
+            // viscoplastic/Constitutive.c:372-518 (the principal stresses the
+            // reference computes first are not used by this branch)
+            if (s.active)
+                dp_return_map(st, dp_sd, dp_S0, e, dp_vic1, dp_vic2, M.mu, dp_bulkm, tan_fric(M, frictionAngle),
+                              tan_dil(M, dilationAngle), cohesion, stc, M.dp_tol, M.dp_maxit, pst, eps_p);
+        } else {
+            double sphi = sin_fric(M, frictionAngle);
+            double spsi = sin_dil(M, dilationAngle);
+            double anphi = fconst ? M.anphi0 : dv(1.0f + sphi, 1.0f - sphi);
+            double anpsi = (M.dil_const && dilationAngle == M.dil0) ? M.anpsi0 : dv(1.0f + spsi, 1.0f - spsi);
+            const double a1 = M.lambda + 2.0f * M.mu;
+            const double a2 = M.lambda;
+            // The reference always computes the principal stresses; they only
+            // matter when the tet yields.  A tet that provably stays inside the
+            // yield surface keeps its trial stress without the eigen-solve.
+            if (!surely_elastic(st, cohesion, anphi, fconst ? M.sq_anphi0 : sqrt(anphi), stc)) {
+                principal_stresses(st, sp, cn);
+                mc_return_map(sp, cn, st, eps_p, cohesion, hardening, anphi, anpsi, stc, a1, a2);
+            }
         }
     }
 
@@ -508,7 +538,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         pressure = dv10(pressure);
         // plastic/Constitutive.c:239-244, viscoplastic/Constitutive.c:519-523: aps
         double aps = 0.0;
-        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC)
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || is_vp(PLUGIN))
             aps = dv(grp_sum(eps_p * g.V, s.base), vsum);
         if (s.active && s.t == 0) {
             F.escal[s.e * 4 + 1] = 0.5f * sqrt(0.5f * fabs(-1.0f * sVolAvg + sOtherAvg));
@@ -595,8 +625,12 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 #pragma unroll
         for (int a = 0; a < 6; a++) ok = ok & (bool)isfinite(st[a]);
         if (!ok) report(F.sc, SNAC_GPU_ENAN, s.e);  // Stress.c:161-166
-        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC) F.eps_p[s.q] = eps_p;
-        if (PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC || (PLUGIN == SNAC_RHEOLOGY_MAXWELL && ph == 0)) F.visc[s.q] = eta;
+        if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || is_vp(PLUGIN)) F.eps_p[s.q] = eps_p;
+        if (is_vp(PLUGIN) || (PLUGIN == SNAC_RHEOLOGY_MAXWELL && ph == 0)) F.visc[s.q] = eta;
+        if (PLUGIN == SNAC_VP_DP) {
+            double2* p = reinterpret_cast<double2*>(F.pst + s.q * 6);
+            for (int a = 0; a < 3; a++) p[a] = make_double2(pst[2 * a], pst[2 * a + 1]);
+        }
     }
 }
 

@@ -153,6 +153,8 @@ void SnacCuda_FreeDescStore(SnacCuda_DescStore* st) {
     free(st->velocityBCValue);
     free(st->temperatureBCMask);
     free(st->temperatureBCValue);
+    free(st->dpMaxIterations);
+    free(st->dpTolerance);
     memset(st, 0, sizeof *st);
 }
 
@@ -205,6 +207,8 @@ int SnacCuda_FillDesc(Snac_Context* context, SnacCuda_Context* self, snac_gpu_de
         if (Snac_Element_At(context, e)->material_I + 1 > nmat) nmat = Snac_Element_At(context, e)->material_I + 1;
     }
     st->materials = (snac_material*)calloc(nmat ? nmat : 1, sizeof(snac_material));
+    st->dpMaxIterations = (int*)calloc(nmat ? nmat : 1, sizeof(int));
+    st->dpTolerance = (double*)calloc(nmat ? nmat : 1, sizeof(double));
     for (p = 0; p < nmat; p++) {
         const Snac_Material* m = &context->materialProperty[p];
         snac_material* o = &st->materials[p];
@@ -215,6 +219,8 @@ int SnacCuda_FillDesc(Snac_Context* context, SnacCuda_Context* self, snac_gpu_de
         o->lambda = m->lambda;
         o->mu = m->mu;
         o->yield_mohr_coulomb = m->yieldcriterion == mohrcoulomb;
+        st->dpMaxIterations[p] = (int)m->maxiterations;
+        st->dpTolerance[p] = m->constitutivetolerance;
         if (d->constitutive == SNAC_RHEOLOGY_PLASTIC || d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
             if (m->nsegments > SNAC_MAX_SEGMENTS) return SNAC_GPU_ENOTSUP;
             o->nsegments = (int)m->nsegments;
@@ -238,6 +244,8 @@ int SnacCuda_FillDesc(Snac_Context* context, SnacCuda_Context* self, snac_gpu_de
     }
     d->n_materials = (int)nmat;
     d->materials = st->materials;
+    d->dp_max_iterations = st->dpMaxIterations;
+    d->dp_tolerance = st->dpTolerance;
     d->element_material = st->elementMaterial;
 
     /* the state after the ICs, as initial values */
@@ -296,6 +304,7 @@ void SnacCuda_Pack(Snac_Context* context, SnacCuda_Context* self) {
         alloc_doubles(&self->plasticStrain, ne * Tetrahedra_Count);
     if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC || self->constitutive == SNAC_RHEOLOGY_MAXWELL)
         alloc_doubles(&self->viscosity, ne * Tetrahedra_Count);
+    if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) alloc_doubles(&self->plasticStrainTensor, ne * Tetrahedra_Count * 6);
     if (self->temperature) alloc_doubles(&self->temperature_, nn);
     for (n = 0; n < nn; n++) {
         Snac_Node* node = Snac_Node_At(context, n);
@@ -319,8 +328,15 @@ void SnacCuda_Pack(Snac_Context* context, SnacCuda_Context* self) {
                 self->plasticStrain[e * Tetrahedra_Count + t] = plastic_of(context, self, element)->plasticStrain[t];
             if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
                 SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
+                double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 self->plasticStrain[e * Tetrahedra_Count + t] = vp->plasticStrain[t];
                 self->viscosity[e * Tetrahedra_Count + t] = vp->viscosity[t];
+                q[0] = vp->plasticstrainTensor[t][0][0];
+                q[1] = vp->plasticstrainTensor[t][1][1];
+                q[2] = vp->plasticstrainTensor[t][2][2];
+                q[3] = vp->plasticstrainTensor[t][0][1];
+                q[4] = vp->plasticstrainTensor[t][0][2];
+                q[5] = vp->plasticstrainTensor[t][1][2];
             }
             if (self->constitutive == SNAC_RHEOLOGY_MAXWELL)
                 self->viscosity[e * Tetrahedra_Count + t] = maxwell_of(context, self, element)->viscosity[t];
@@ -356,8 +372,15 @@ void SnacCuda_Unpack(Snac_Context* context, SnacCuda_Context* self) {
                 plastic_of(context, self, element)->plasticStrain[t] = self->plasticStrain[e * Tetrahedra_Count + t];
             if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
                 SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
+                const double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 vp->plasticStrain[t] = self->plasticStrain[e * Tetrahedra_Count + t];
                 vp->viscosity[t] = self->viscosity[e * Tetrahedra_Count + t];
+                vp->plasticstrainTensor[t][0][0] = q[0];
+                vp->plasticstrainTensor[t][1][1] = q[1];
+                vp->plasticstrainTensor[t][2][2] = q[2];
+                vp->plasticstrainTensor[t][0][1] = q[3];
+                vp->plasticstrainTensor[t][0][2] = q[4];
+                vp->plasticstrainTensor[t][1][2] = q[5];
             }
             if (self->constitutive == SNAC_RHEOLOGY_MAXWELL)
                 maxwell_of(context, self, element)->viscosity[t] = self->viscosity[e * Tetrahedra_Count + t];

@@ -80,6 +80,7 @@ void SnacCuda_TimeStepZero(void* _context, void* data) {
         snac_state_view v = {0};
         v.plastic_strain = self->plasticStrain;
         v.viscosity = self->viscosity;
+        v.plastic_strain_tensor = self->plasticStrainTensor;
         if (v.plastic_strain || v.viscosity) cuda_check(context, self, snac_gpu_upload(self->gpu, &v), "snac_gpu_upload");
     }
     cuda_check(context, self, snac_gpu_time_step_zero(self->gpu), "snac_gpu_time_step_zero");
@@ -140,6 +141,7 @@ void SnacCuda_SyncHost(void* context) {
     v.temperature = self->temperature_;
     v.force = self->force;
     v.inertial_mass = self->inertialMass;
+    v.plastic_strain_tensor = self->plasticStrainTensor;
     cuda_check(context, self, snac_gpu_download(self->gpu, &v), "snac_gpu_download");
     SnacCuda_Unpack((Snac_Context*)context, self);
 }
@@ -156,6 +158,7 @@ void SnacCuda_SyncDevice(void* context) {
     v.plastic_strain = self->plasticStrain;
     v.viscosity = self->viscosity;
     v.temperature = self->temperature_;
+    v.plastic_strain_tensor = self->plasticStrainTensor;
     cuda_check(context, self, snac_gpu_upload(self->gpu, &v), "snac_gpu_upload");
 }
 

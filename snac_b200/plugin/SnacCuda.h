@@ -50,6 +50,7 @@ typedef struct SnacCuda_Context {
     double* temperature_;
     double* force;
     double* inertialMass;
+    double* plasticStrainTensor;    /* visco-plastic: plasticstrainTensor (Drucker-Prager phases) */
 } SnacCuda_Context;
 
 /* Arrays a descriptor points into while snac_gpu_create reads it. */
@@ -63,6 +64,8 @@ typedef struct SnacCuda_DescStore {
     double* velocityBCValue;
     unsigned char* temperatureBCMask;
     double* temperatureBCValue;
+    int* dpMaxIterations;
+    double* dpTolerance;
 } SnacCuda_DescStore;
 
 Index _SnacCuda_Register(PluginsManager* pluginsMgr);

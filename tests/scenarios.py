@@ -36,6 +36,18 @@ def viscoplastic_small(nx=8, ny=4, nz=8, active=True):
     return cfg
 
 
+def drucker_prager_small(nx=8, ny=4, nz=8, maxiterations=1):
+    """The yielding visco-plastic case with the Drucker-Prager criterion
+    (viscoplastic/Constitutive.c:372-518); maxiterations > 1 takes the
+    iterated return map."""
+    cfg = viscoplastic_small(nx, ny, nz)
+    for m in cfg.materials:
+        m["yieldcriterion"] = "druckerprager"
+        m["maxiterations"] = maxiterations
+        m["constitutivetolerance"] = 1.0e-3
+    return cfg
+
+
 def maxwell_small(nx=6, ny=4, nz=6):
     cfg = W.c3_viscoplastic(nx, ny, nz, extent=(100.0e3, 20.0e3, 100.0e3), sigma=5.0e3)
     cfg.plugin = "SnacMaxwell"
@@ -137,4 +149,6 @@ CASES = {
     "topo": (topo_small, 60),
     "density": (two_phase_density, 40),
     "plastic_phases": (plastic_two_phase, 120),
+    "drucker_prager": (drucker_prager_small, 120),
+    "drucker_prager_iterated": (lambda: drucker_prager_small(maxiterations=4), 120),
 }

@@ -67,14 +67,44 @@ def test_plastic_case_yields_on_gpu():
 # the device viscosity differs from the host libm pow * exp in the last bits; through the
 # yield branch the difference stays far below the plastic bar (1e-6), and
 # without plasticity (Maxwell) below the elastic bar (1e-9).
-@pytest.mark.parametrize("case,tol", [("viscoplastic", 1e-6), ("maxwell", 1e-9), ("density", 1e-6)])
+@pytest.mark.parametrize("case,tol", [("viscoplastic", 1e-6), ("maxwell", 1e-9), ("density", 1e-6),
+                                      ("drucker_prager", 1e-6), ("drucker_prager_iterated", 1e-6)])
 def test_device_transcendentals_within_tolerance(case, tol):
     make, steps = S.CASES[case]
     g, c = run_both(make(), steps)
     sg, sc = g.state(), c.state()
-    for f in ("velocity", "stress", "plastic_strain", "viscosity", "temperature", "coord"):
+    for f in ("velocity", "stress", "plastic_strain", "viscosity", "temperature", "coord", "plastic_strain_tensor"):
         e = relerr(getattr(sg, f), getattr(sc, f))
         assert e <= tol, (case, f, e)
+    if case.startswith("drucker"):  # the Drucker-Prager branch yielded and kept its tensor
+        assert np.count_nonzero(sc.plastic_strain_tensor) > 100 and np.count_nonzero(sg.plastic_strain_tensor) > 100
+
+
+def test_drucker_prager_tensor_round_trip_and_limits():
+    """The plastic strain tensor goes up and down through the state view; the
+    batched and adjoint forms refuse Drucker-Prager models; the plastic hook,
+    which has no Drucker-Prager branch, takes Mohr-Coulomb whatever the
+    phase's yield criterion says (plastic/Constitutive.c:58-247)."""
+    from snac_b200.batch import SnacBatch
+    cfg = S.drucker_prager_small()
+    with SnacContext(cfg) as g:
+        g.time_step_zero()
+        g.step(40)
+        st = g.state()
+        assert np.count_nonzero(st.plastic_strain_tensor) > 0
+        st2 = State.empty(cfg.n_elements, cfg.n_nodes)
+        st2.plastic_strain_tensor[:] = 1.5 * st.plastic_strain_tensor
+        g.set_state(st2, ["plastic_strain_tensor"])
+        assert np.array_equal(g.state().plastic_strain_tensor, 1.5 * st.plastic_strain_tensor)
+    with pytest.raises(SnacError):
+        SnacBatch([S.drucker_prager_small(4, 2, 4)])
+    mc, dp = S.plastic_small(), S.plastic_small()
+    for m in dp.materials:
+        m["yieldcriterion"] = "druckerprager"
+    g1, c1 = run_both(mc, 60)
+    g2, _ = run_both(dp, 60)
+    assert np.array_equal(g1.state().stress, g2.state().stress)
+    assert_bitwise(g2, c1)
 
 
 def test_elastic_c1_full_1000_steps():

@@ -38,13 +38,14 @@ class CudaContext(C.Structure):
                 ("temperatureNode", C.c_uint), ("temperatureContext", C.c_uint),
                 ("ne", C.c_longlong), ("nn", C.c_longlong),
                 ("coord", _DP), ("velocity", _DP), ("stress", _DP), ("plasticStrain", _DP), ("viscosity", _DP),
-                ("temperature_", _DP), ("force", _DP), ("inertialMass", _DP)]
+                ("temperature_", _DP), ("force", _DP), ("inertialMass", _DP), ("plasticStrainTensor", _DP)]
 
 
 class DescStore(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("materials", "elementMaterial", "initStress", "initVelocity",
                                           "initTemperature", "velocityBCMask", "velocityBCValue",
-                                          "temperatureBCMask", "temperatureBCValue")]
+                                          "temperatureBCMask", "temperatureBCValue", "dpMaxIterations",
+                                          "dpTolerance")]
 
 
 def host(cfg):
