@@ -206,18 +206,59 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
     }
 }
 
-// Everything the stress update reads from global memory besides the
-// corners and the stress, loaded at the start of the element kernels: the
-// face stash below is a compiler barrier, so a load written after it could
-// not be moved above it and would wait a full memory round trip in the
-// middle of the tet's arithmetic.
+#ifndef SNAC_DEFER_VEL
+#define SNAC_DEFER_VEL 0
+#endif
+// With SNAC_DEFER_VEL the fused element kernel loads only the corners'
+// coordinates before the geometry; the velocities and the tet's stress row
+// are prefetched into L1 at the start and loaded after the geometry, so
+// they do not hold registers through it.
+__device__ __forceinline__ void load_corners(const Mesh& m, const Fields& F, const TetSlot& s, V3 c[4], double T[4]) {
+#pragma unroll
+    for (int qn = 0; qn < 4; qn++) {
+        if (s.active) {
+            const long long n = corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn));
+            const double4 p = F.pos[n];
+            c[qn] = {p.x, p.y, p.z};
+            T[qn] = p.w;
+            asm volatile("prefetch.global.L1 [%0];" ::"l"(F.vel + n));
+        } else {  // a regular dummy tet keeps inactive lanes finite
+            c[qn] = {qn == 1 ? 1.0 : 0.0, qn == 2 ? 1.0 : 0.0, qn == 3 ? 1.0 : 0.0};
+            T[qn] = 0.0;
+        }
+    }
+    if (s.active) {  // the 48-byte stress row may straddle two lines
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(F.stress + s.q * 6));
+        asm volatile("prefetch.global.L1 [%0];" ::"l"(F.stress + s.q * 6 + 5));
+    }
+}
+__device__ __forceinline__ void load_velocities(const Mesh& m, const Fields& F, const TetSlot& s, V3 v[4],
+                                                double T0[4]) {
+#pragma unroll
+    for (int qn = 0; qn < 4; qn++) {
+        if (s.active) {
+            const double4 w = F.vel[corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn))];
+            v[qn] = {w.x, w.y, w.z};
+            T0[qn] = w.w;
+        } else {
+            v[qn] = {0.0, 0.0, 0.0};
+            T0[qn] = 0.0;
+        }
+    }
+}
+
+// What the constitutive update reads from global memory besides the
+// corners and the stress.  The face stash below is a compiler barrier, so
+// these loads stay after it; so that they do not wait a full memory round
+// trip in the middle of the tet's arithmetic, the element kernels prefetch
+// their lines into L1 at the start (prefetch_tet_in), which costs no
+// registers (loading the values that early would hold them across the
+// geometry, where registers are scarcest, and made the visco-plastic
+// instances spill).
 struct TetIn {
     double eps_p;                 // plastic strain (plastic, visco-plastic)
     double coh, fric, visc;       // per-element parameter scales (1 without them)
     double pst[6];                // plastic strain tensor (Drucker-Prager instances)
-    double dt, dt_rot;            // this step's dt and the pending rotation's
-    double sos, inertial_density0;
-    int want;                     // element scalars wanted (a dump follows this step)
 };
 
 template <int PLUGIN>
@@ -238,13 +279,21 @@ __device__ __forceinline__ TetIn load_tet_in(const Fields& F, const TetSlot& s) 
     in.coh = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
     in.fric = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
     in.visc = (F.visc_scale && s.active) ? F.visc_scale[s.e] : 1.0;
-    const DevScalars* sc = F.sc;
-    in.dt = sc->dt;
-    in.dt_rot = sc->dt_rot;
-    in.sos = sc->speed_of_sound;
-    in.inertial_density0 = sc->inertial_density0;
-    in.want = F.escal != nullptr && sc->want_scalars;
     return in;
+}
+
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+template <int PLUGIN>
+__device__ __forceinline__ void prefetch_tet_in(const Fields& F, const TetSlot& s) {
+    if (!s.active) return;
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || is_vp(PLUGIN)) prefetch_l1(F.eps_p + s.q);
+    if (PLUGIN == SNAC_VP_DP) prefetch_l1(F.pst + s.q * 6);
+    if (s.t == 0) {  // one lane per hex for the per-element rows
+        if (F.coh_scale) prefetch_l1(F.coh_scale + s.e);
+        if (F.fric_scale) prefetch_l1(F.fric_scale + s.e);
+        if (F.visc_scale) prefetch_l1(F.visc_scale + s.e);
+    }
 }
 
 // ======================================================================================
@@ -288,8 +337,7 @@ __device__ __forceinline__ void unstash_faces(TetGeom& g) {
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const V3 v[4], const double T[4], const TetGeom& g, double st[6],
-                                              const TetIn& in) {
-    const double dt = in.dt;
+                                              const double dt) {
     double sr[6];
     tet_strain_rate(v, g, sr);
 
@@ -310,7 +358,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     sr[1] += corr;
     sr[2] += corr;
     // scalar element outputs for the dump writers, on the steps that need them
-    const bool want = in.want;
+    const bool want = F.escal != nullptr && F.sc->want_scalars;
     if (want) {
         // StrainRate.c:284-304
         double srVolAvg = grp_sum(sr[1] * sr[2] + sr[2] * sr[0] + sr[0] * sr[1], s.base);
@@ -326,6 +374,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     for (int a = 0; a < 6; a++) e[a] = sr[a] * dt;
 
     stash_faces(g);
+    const TetIn in = load_tet_in<PLUGIN>(F, s);
     const int ph = s.active ? phase_of(F, s.e) : 0;
     const DevMaterial& M = ONE ? cfg.m0 : F.mats[ph];  // ONE: the model has one phase
     double eps_p = in.eps_p, eta = 0.0;
@@ -595,8 +644,8 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
         if (cfg.dt_type == SNAC_DT_DYNAMIC) {
-            const double sos = in.sos;
-            const double inertialDensity = ONE ? in.inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
+            const double sos = F.sc->speed_of_sound;
+            const double inertialDensity = ONE ? F.sc->inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
             F.fmass[qt] = factor4 * inertialDensity * gf.V;
         } else if (cfg.dt_type == SNAC_DT_CONSTANT) {
             const double alpha1 = (M.lambda + 2.0f * M.mu);
@@ -637,7 +686,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     TetSlot s = tet_slot(m, lb);
-    const TetIn in = load_tet_in<PLUGIN>(F, s);
+    prefetch_tet_in<PLUGIN>(F, s);
     V3 c[4], v[4];
     double T[4], T0[4];
     load_tet(m, F, s, c, v, T, T0);
@@ -647,7 +696,7 @@ __device__ __forceinline__ void k_calc_stresses_body(const Mesh& m, const Fields
     if (s.active) {
         load_stress(F, s.q, st);
     }
-    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, in);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
 
 template <int PLUGIN, bool ONE>
@@ -679,19 +728,27 @@ template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F, const Config& cfg, int lb,
                                                   bool count_step = true) {
     TetSlot s = tet_slot(m, lb);
-    const TetIn in = load_tet_in<PLUGIN>(F, s);
+    prefetch_tet_in<PLUGIN>(F, s);
     if (count_step && lb == 0 && threadIdx.x == 0) {  // _AbstractContext_Execute_Hook: timeStep++, currentTime += dt
         F.sc->time_step += 1;
-        F.sc->current_time += in.dt;
+        F.sc->current_time += F.sc->dt;
     }
     V3 c[4], v[4];
     double T[4], T0[4];
+#if SNAC_DEFER_VEL
+    load_corners(m, F, s, c, T);
+    TetGeom g;
+    tet_geometry(c, g);
+    asm volatile("" ::: "memory");  // the velocity and stress loads stay after the geometry
+    load_velocities(m, F, s, v, T0);
+#else
     load_tet(m, F, s, c, v, T, T0);
     TetGeom g;
     tet_geometry(c, g);
+#endif
     double st[6] = {0, 0, 0, 0, 0, 0};
-    element_update_tet<PLUGIN>(F, cfg, s, v, g, in.dt_rot, st);
-    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, in);
+    element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
 }
 
 #ifndef SNAC_L2_PREFETCH
