@@ -383,6 +383,52 @@ __device__ __forceinline__ void spin_rates(const V3 v[4], const TetGeom& g, doub
     dvk_n(r, 3.0, Z3);
 }
 
+// The spin rates (UpdateElement.c:145-219) and the strain rate
+// (StrainRate.c:65-184) of one tet from the same velocities and geometry,
+// as the fused element kernel needs both: the chains
+// a0+a1+a2+a3 -/+ b0 -/+ b1 -/+ b2 -/+ b3 of a spin sum and of the matching
+// shear sum share their products and their prefix a0+..+a3, which are
+// formed once here; every result has the bits of spin_rates and
+// tet_strain_rate.
+__device__ __forceinline__ void spin_and_strain_rates(const V3 v[4], const TetGeom& g, double (&r)[3], double sr[6]) {
+    double t[6];
+    t[0] = -1.0f * (face_sum(v, 0, g, 0));
+    t[1] = -1.0f * (face_sum(v, 1, g, 1));
+    t[2] = -1.0f * (face_sum(v, 2, g, 2));
+    constexpr int PA[3] = {0, 0, 1}, PB[3] = {1, 2, 2};
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        const int a = PA[k], b = PB[k];
+        const double pre = comp(v[0], a) * comp(g.n[1], b) * g.A[1] + comp(v[1], a) * comp(g.n[2], b) * g.A[2] +
+                           comp(v[2], a) * comp(g.n[3], b) * g.A[3] + comp(v[3], a) * comp(g.n[0], b) * g.A[0];
+        const double q0 = comp(v[0], b) * comp(g.n[1], a) * g.A[1], q1 = comp(v[1], b) * comp(g.n[2], a) * g.A[2],
+                     q2 = comp(v[2], b) * comp(g.n[3], a) * g.A[3], q3 = comp(v[3], b) * comp(g.n[0], a) * g.A[0];
+        r[k] = pre - q0 - q1 - q2 - q3;
+        t[3 + k] = -0.5f * (pre + q0 + q1 + q2 + q3);
+    }
+    const double hV = exp_within<-1000, 1000>(g.V) ? 0.5 * g.zV : ieee_div(0.5, g.V);
+#pragma unroll
+    for (int k = 0; k < 3; k++) r[k] = -(hV) * (r[k]);
+    dvk_n(r, 3.0, Z3);
+    dvk_n(t, 3.0, Z3);
+    dvz_n(t, g.V, g.zV);
+#pragma unroll
+    for (int a = 0; a < 6; a++) sr[a] = t[a];
+}
+
+// Jaumann rotation of the stress with the spin rates r, UpdateElement.c:145-265
+// (the strain is zeroed first, :81, so its own rotation leaves it zero); s01
+// takes "+ r12*s02".
+__device__ __forceinline__ void rotate_stress_by(const double (&r)[3], double dt, double s[6]) {
+    const double r01 = r[0], r02 = r[1], r12 = r[2];
+    s[0] += (2.0f * r01 * s[3] + 2.0f * r02 * s[4]) * dt;
+    s[1] += (2.0f * (-1.0f * r01) * s[3] + 2.0f * r12 * s[5]) * dt;
+    s[2] += (2.0f * (-1.0f * r02) * s[4] + 2.0f * (-1.0f * r12) * s[5]) * dt;
+    s[3] += (r01 * (s[1] - s[0])) * dt + (r02 * s[5] + r12 * s[4]) * dt;
+    s[4] += (r02 * (s[2] - s[0])) * dt + (r01 * s[5] - r12 * s[3]) * dt;
+    s[5] += (r12 * (s[2] - s[1])) * dt + ((-1.0f * r01) * s[4] - r02 * s[3]) * dt;
+}
+
 // Jaumann rotation of the stress, UpdateElement.c:145-265 (the strain is
 // zeroed first, :81, so its own rotation leaves it zero); s01 takes "+ r12*s02".
 __device__ __forceinline__ void rotate_stress(const V3 v[4], const TetGeom& g, double dt, double s[6]) {

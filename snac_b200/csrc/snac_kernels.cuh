@@ -337,9 +337,14 @@ __device__ __forceinline__ void unstash_faces(TetGeom& g) {
 template <int PLUGIN, bool ONE>
 __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, const Config& cfg, const TetSlot& s,
                                               const V3 v[4], const double T[4], const TetGeom& g, double st[6],
-                                              const double dt) {
+                                              const double dt, const double* sr_given = nullptr) {
     double sr[6];
-    tet_strain_rate(v, g, sr);
+    if (sr_given) {  // the fused kernel formed it with the spin rates
+#pragma unroll
+        for (int a = 0; a < 6; a++) sr[a] = sr_given[a];
+    } else {
+        tet_strain_rate(v, g, sr);
+    }
 
     // element volume: UpdateElement.c:141,267 then 2*volume (StrainRate.c:62)
     double vsum = grp_sum(g.V, s.base);
@@ -706,6 +711,25 @@ __global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stress
 
 // UpdateElement.c:84-91 volume bookkeeping (Maxwell reads V/V_old) and the
 // Jaumann rotation of the stress (:145-265) of one tet; returns the rotated stress.
+#ifndef SNAC_SHARED_SUMS
+#define SNAC_SHARED_SUMS 0
+#endif
+// UpdateElement.c:84-91 volume bookkeeping and the Jaumann rotation with
+// given spin rates
+template <int PLUGIN>
+__device__ __forceinline__ void element_update_tet_by(const Fields& F, const Config& cfg, const TetSlot& s,
+                                                      const TetGeom& g, const double (&r)[3], double dt, double st[6]) {
+    if (PLUGIN == SNAC_RHEOLOGY_MAXWELL && s.active) {
+        double vc = F.vol[s.q * 2 + 0];
+        F.vol[s.q * 2 + 1] = cfg.time_step_zero ? g.V : vc;
+        F.vol[s.q * 2 + 0] = g.V;
+    }
+    if (s.active) {
+        load_stress(F, s.q, st);
+        rotate_stress_by(r, dt, st);
+    }
+}
+
 template <int PLUGIN>
 __device__ __forceinline__ void element_update_tet(const Fields& F, const Config& cfg, const TetSlot& s, const V3 v[4],
                                                    const TetGeom& g, double dt, double st[6]) {
@@ -747,8 +771,15 @@ __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F
     tet_geometry(c, g);
 #endif
     double st[6] = {0, 0, 0, 0, 0, 0};
+#if SNAC_SHARED_SUMS
+    double r[3], sr[6];
+    spin_and_strain_rates(v, g, r, sr);
+    element_update_tet_by<PLUGIN>(F, cfg, s, g, r, F.sc->dt_rot, st);
+    stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt, sr);
+#else
     element_update_tet<PLUGIN>(F, cfg, s, v, g, F.sc->dt_rot, st);
     stress_update<PLUGIN, ONE>(m, F, cfg, s, v, T, g, st, F.sc->dt);
+#endif
 }
 
 #ifndef SNAC_L2_PREFETCH
