@@ -407,6 +407,8 @@ def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
             setattr(host, f, t.numpy())
         h2d = sum(pinned[f].numel() * 8 for f in fields)
         out = State.empty(ctx.ne, ctx.nn)       # the step's result, into pinned host buffers
+        if not ctx.keeps_plastic_strain_tensor:
+            out.plastic_strain_tensor = None    # the model has none
         keep = []
         for f, _ in out.view()._fields_:
             a = getattr(out, f, None)

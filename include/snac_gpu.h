@@ -73,6 +73,7 @@ extern "C" {
 #define SNAC_WALL_ALL    6   /* every node (AllNodesVC)                          */
 
 #define SNAC_MAX_SEGMENTS 8  /* softening table: nsegments <= 8, 9 break points */
+#define SNAC_MAX_PHASES   32 /* n_materials <= 32; finer variation goes in the per-element scales */
 
 /* One phase, Snac/libSnac/src/Material.h:54-112 and the dictionary keys of
  * Context.c:826-914.  Every value is taken as given (no float-literal

@@ -128,7 +128,7 @@ class SnacBatch:
 
 # candidate values per knob, searched one knob at a time from the default
 SEARCH_SPACE: Dict[str, List[int]] = {
-    "steps_per_graph": [1, 4, 16, 64],
+    "steps_per_graph": [1, 4, 16, 64, 256],  # 256: the largest graph the library captures
     "elem_blocks_per_sm": [0, 4, 8, 16],
     "node_threads": [64, 128, 256],
     "node_blocks_per_sm": [0, 8, 16],

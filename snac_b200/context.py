@@ -219,10 +219,19 @@ class SnacContext:
         self.sync()
 
     # -- state --------------------------------------------------------------------------
+    @property
+    def keeps_plastic_strain_tensor(self) -> bool:
+        """The visco-plastic hook with a Drucker-Prager phase keeps a per-tet
+        plastic strain tensor; other models have none (it reads as zero)."""
+        return self.cfg.plugin == "SnacViscoPlastic" and any(
+            m.get("yieldcriterion", "mohrcoulomb") != "mohrcoulomb" for m in self.cfg.materials)
+
     def state(self, out: Optional[State] = None) -> State:
         """The state at the end of the last step (into `out` if given, e.g. pinned buffers)."""
         s = out if out is not None else State.empty(self.ne, self.nn)
         v = s.view()
+        if not self.keeps_plastic_strain_tensor:
+            v.plastic_strain_tensor = None  # nothing to copy: the State's tensor stays as it is (zero)
         self._check(self.lib.snac_gpu_download(self.h, C.byref(v)))
         return s
 

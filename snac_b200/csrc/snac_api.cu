@@ -878,6 +878,8 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     for (int p = 0; p < d->n_materials; p++)  // Drucker-Prager controls: Context.c:851-854 defaults 1 and 1e-3
         dm[p] = to_dev(d->materials[p], d->element_friction_scale != nullptr,
                        d->dp_max_iterations ? d->dp_max_iterations[p] : 1, d->dp_tolerance ? d->dp_tolerance[p] : 1.e-3);
+    // the volume alone stands for the gravity and inertial-mass terms (Config::vonly)
+    h->cfg.vonly = !d->element_material && !h->has_density && d->dt_type != SNAC_DT_CONSTANT;
     if (d->element_material) {
         std::vector<unsigned char> mt(ne);
         for (long long e = 0; e < ne; e++) {

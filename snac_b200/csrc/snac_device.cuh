@@ -22,7 +22,7 @@ constexpr int NT = 10;        // Tetrahedra_Count
 // Mohr-Coulomb instances' registers).
 constexpr int SNAC_VP_DP = SNAC_RHEOLOGY_VISCOPLASTIC | 0x100;
 __host__ __device__ constexpr bool is_vp(int plugin) { return (plugin & SNAC_RHEOLOGY_VISCOPLASTIC) != 0; }
-constexpr int MAX_PHASES = 32;
+constexpr int MAX_PHASES = SNAC_MAX_PHASES;
 
 // TetrahedraTables.c:42-84 (tets 0-4 are the first five-tet set, 5-9 the second).
 // Face f of a tet is the triangle opposite its local node (3,0,1,2)[f].

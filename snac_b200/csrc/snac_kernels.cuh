@@ -82,6 +82,11 @@ struct Config {
     double topo_kappa, topo_crit;  // surface-topography diffusion
     double pisos, rzbo;   // its isostatic pressure and reference bottom depth
     int prefetch_ahead;   // element blocks resident at once (SMs x blocks per SM): the L2 prefetch distance
+    // one phase, no density coupling, dynamic or wave dt: a tet's gravity and
+    // inertial-mass terms are the same multiples of its volume for every tet,
+    // so the element kernels store the volume alone (in the fgrav row) and
+    // the node gather forms both terms from it with the same operations
+    int vonly;
     // phase 0, the only phase of a model without a per-element phase array:
     // the element kernels of such models read it from their parameters
     // (constant-bank operands) instead of loading it from the phase table
@@ -202,47 +207,6 @@ __device__ __forceinline__ void load_tet(const Mesh& m, const Fields& F, const T
             c[qn] = {qn == 1 ? 1.0 : 0.0, qn == 2 ? 1.0 : 0.0, qn == 3 ? 1.0 : 0.0};
             v[qn] = {0.0, 0.0, 0.0};
             T[qn] = T0[qn] = 0.0;
-        }
-    }
-}
-
-#ifndef SNAC_DEFER_VEL
-#define SNAC_DEFER_VEL 0
-#endif
-// With SNAC_DEFER_VEL the fused element kernel loads only the corners'
-// coordinates before the geometry; the velocities and the tet's stress row
-// are prefetched into L1 at the start and loaded after the geometry, so
-// they do not hold registers through it.
-__device__ __forceinline__ void load_corners(const Mesh& m, const Fields& F, const TetSlot& s, V3 c[4], double T[4]) {
-#pragma unroll
-    for (int qn = 0; qn < 4; qn++) {
-        if (s.active) {
-            const long long n = corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn));
-            const double4 p = F.pos[n];
-            c[qn] = {p.x, p.y, p.z};
-            T[qn] = p.w;
-            asm volatile("prefetch.global.L1 [%0];" ::"l"(F.vel + n));
-        } else {  // a regular dummy tet keeps inactive lanes finite
-            c[qn] = {qn == 1 ? 1.0 : 0.0, qn == 2 ? 1.0 : 0.0, qn == 3 ? 1.0 : 0.0};
-            T[qn] = 0.0;
-        }
-    }
-    if (s.active) {  // the 48-byte stress row may straddle two lines
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(F.stress + s.q * 6));
-        asm volatile("prefetch.global.L1 [%0];" ::"l"(F.stress + s.q * 6 + 5));
-    }
-}
-__device__ __forceinline__ void load_velocities(const Mesh& m, const Fields& F, const TetSlot& s, V3 v[4],
-                                                double T0[4]) {
-#pragma unroll
-    for (int qn = 0; qn < 4; qn++) {
-        if (s.active) {
-            const double4 w = F.vel[corner_node(m, s.i, s.j, s.k, tet_node_rt(s.t, qn))];
-            v[qn] = {w.x, w.y, w.z};
-            T0[qn] = w.w;
-        } else {
-            v[qn] = {0.0, 0.0, 0.0};
-            T0[qn] = 0.0;
         }
     }
 }
@@ -646,9 +610,15 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             o[(f * 3 + 2) * R] = t[2];
         }
         const long long qt = (long long)s.t * R + s.e;  // row t
-        F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
         const double factor4 = 1.0f / 4.0f;
-        if (cfg.dt_type == SNAC_DT_DYNAMIC) {
+        if (ONE && cfg.vonly) {
+            F.fgrav[qt] = gf.V;
+        } else {
+            F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
+        }
+        if (ONE && cfg.vonly) {
+            // both terms formed by the node gather
+        } else if (cfg.dt_type == SNAC_DT_DYNAMIC) {
             const double sos = F.sc->speed_of_sound;
             const double inertialDensity = ONE ? F.sc->inertial_density0 : dv(M.lambda + 2.0f * M.mu, sos * sos);
             F.fmass[qt] = factor4 * inertialDensity * gf.V;
@@ -759,17 +729,9 @@ __device__ __forceinline__ void k_fused_step_body(const Mesh& m, const Fields& F
     }
     V3 c[4], v[4];
     double T[4], T0[4];
-#if SNAC_DEFER_VEL
-    load_corners(m, F, s, c, T);
-    TetGeom g;
-    tet_geometry(c, g);
-    asm volatile("" ::: "memory");  // the velocity and stress loads stay after the geometry
-    load_velocities(m, F, s, v, T0);
-#else
     load_tet(m, F, s, c, v, T, T0);
     TetGeom g;
     tet_geometry(c, g);
-#endif
     double st[6] = {0, 0, 0, 0, 0, 0};
 #if SNAC_SHARED_SUMS
     double r[3], sr[6];
@@ -1046,6 +1008,10 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
         int i, j, k;
         split3(n, m.nnx, m.nny, i, j, k);
         double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
+        // with cfg.vonly the fgrav row holds the tet volume: (g rho) V / 8 and
+        // (1/4 rho_i) V are formed here exactly as the element kernel forms them
+        const double gr = cfg.gravity * cfg.m0.density;
+        const double f4r = (1.0f / 4.0f) * (DTTYPE == SNAC_DT_DYNAMIC ? F.sc->inertial_density0 : cfg.m0.density);
         // Snac_Force: the 8 incident hexes in HexaEL.c:529-573 order, 5 tets each
         // (NodeToTetra/NodeToSurface); absent hexes are skipped (Force.c:92)
 #pragma unroll
@@ -1058,12 +1024,21 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 const int t = node_tet(ne, idx);
                 const int f = node_face(ne, idx);
                 const long long R = m.ner;
-                imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[(t * 4 + f) * R + e] : F.fmass[t * R + e];
                 const double* o = F.fterm + (t * 12 + f * 3) * R + e;
-                fx += o[0];
-                fy += o[R];
-                fz += o[2 * R];
-                fy -= F.fgrav[t * R + e];
+                if (DTTYPE != SNAC_DT_CONSTANT && cfg.vonly) {
+                    const double V = F.fgrav[t * R + e];
+                    imass += f4r * V;
+                    fx += o[0];
+                    fy += o[R];
+                    fz += o[2 * R];
+                    fy -= gr * V / 8.0f;
+                } else {
+                    imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[(t * 4 + f) * R + e] : F.fmass[t * R + e];
+                    fx += o[0];
+                    fy += o[R];
+                    fz += o[2 * R];
+                    fy -= F.fgrav[t * R + e];
+                }
             }
         }
         if (cfg.winkler && cfg.gravity > 0.0 && j == 0) {

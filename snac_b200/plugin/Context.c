@@ -21,6 +21,7 @@
 #include "Snac/Maxwell/Maxwell.h"
 #include "Snac/Temperature/Temperature.h"
 #include "SnacCuda.h"
+#include <math.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -65,6 +66,14 @@ int SnacCuda_Inspect(Snac_Context* context, SnacCuda_Context* self) {
     if (self->constitutive == SNAC_RHEOLOGY_MAXWELL && self->maxwellElement == NO_HANDLE) return SNAC_GPU_EINVAL;
     self->ne = context->mesh->elementLocalCount;
     self->nn = context->mesh->nodeLocalCount;
+    /* the visco-plastic hook's Drucker-Prager branch keeps a per-tet plastic strain tensor */
+    self->druckerPrager = 0;
+    if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
+        long long e;
+        for (e = 0; e < self->ne && !self->druckerPrager; e++)
+            if (context->materialProperty[Snac_Element_At(context, e)->material_I].yieldcriterion == druckerprager)
+                self->druckerPrager = 1;
+    }
     return 0;
 }
 
@@ -143,6 +152,135 @@ static void probe_temperature_bcs(Snac_Context* context, SnacCuda_Context* self,
     }
 }
 
+/* A scale c with RN(base[i] * c) == want[i] for every i (bit for bit), the
+ * factor the device applies to a base phase's table; 1 when the tables are
+ * equal.  Candidates: the quotient of the first non-zero pair and its
+ * neighbours a few ulps away.  Returns 0 when there is none. */
+static int find_scale(const double* base, const double* want, int n, double* scale) {
+    int i, k, first = -1, same = 1;
+    for (i = 0; i < n; i++) {
+        if (memcmp(&base[i], &want[i], sizeof(double)) != 0) same = 0;
+        if (first < 0 && base[i] != 0.0) first = i;
+    }
+    if (same) {
+        *scale = 1.0;
+        return 1;
+    }
+    if (first < 0) return 0;
+    {
+        double c = want[first] / base[first], lo = c, hi = c;
+        for (k = 0; k < 9; k++) {
+            const double cand = k == 0 ? c : (k % 2 ? (lo = nextafter(lo, -INFINITY)) : (hi = nextafter(hi, INFINITY)));
+            int ok = 1;
+            for (i = 0; i < n && ok; i++) {
+                const double got = base[i] * cand;
+                ok = memcmp(&got, &want[i], sizeof(double)) == 0;
+            }
+            if (ok) {
+                *scale = cand;
+                return 1;
+            }
+        }
+    }
+    return 0;
+}
+
+/* Everything but the cohesion and friction tables and the reference
+ * viscosity: what phases sharing a base must have in common. */
+static int same_shape(const snac_material* a, const snac_material* b, int dp_a, int dp_b, double tol_a, double tol_b) {
+    snac_material x = *a, y = *b;
+    memset(x.cohesion, 0, sizeof x.cohesion);
+    memset(y.cohesion, 0, sizeof y.cohesion);
+    memset(x.friction_angle, 0, sizeof x.friction_angle);
+    memset(y.friction_angle, 0, sizeof y.friction_angle);
+    x.refvisc = y.refvisc = 0.0;
+    return memcmp(&x, &y, sizeof x) == 0 && dp_a == dp_b && memcmp(&tol_a, &tol_b, sizeof tol_a) == 0;
+}
+
+/* More phases than the device's table holds (SNAC_MAX_PHASES): the
+ * reference expresses spatially varying strength or viscosity as one phase
+ * per element (or per region).  Group the phases into base phases that
+ * differ only by a factor on the cohesion table, the friction table and the
+ * reference viscosity, and give every element its factors as per-element
+ * scales, which the device applies to the base's values (the product
+ * reproduces each phase's own value bit for bit, checked here).  A friction
+ * scale makes the device evaluate sin and tan of the scaled angles itself
+ * instead of taking the host's values. */
+static int group_phases(snac_gpu_desc* d, SnacCuda_DescStore* st, long long ne) {
+    const int nmat = d->n_materials;
+    const int nseg1 = SNAC_MAX_SEGMENTS + 1;
+    int* base_of = (int*)malloc(sizeof(int) * (size_t)nmat);
+    double* cs = (double*)malloc(sizeof(double) * (size_t)nmat);
+    double* fs = (double*)malloc(sizeof(double) * (size_t)nmat);
+    double* vs = (double*)malloc(sizeof(double) * (size_t)nmat);
+    int bases[SNAC_MAX_PHASES], nb = 0, p, b, need_c = 0, need_f = 0, need_v = 0, rc = 0;
+    long long e;
+    for (p = 0; p < nmat && !rc; p++) {
+        const snac_material* m = &st->materials[p];
+        base_of[p] = -1;
+        for (b = 0; b < nb && base_of[p] < 0; b++) {
+            const snac_material* r = &st->materials[bases[b]];
+            if (!same_shape(m, r, st->dpMaxIterations[p], st->dpMaxIterations[bases[b]], st->dpTolerance[p],
+                            st->dpTolerance[bases[b]]))
+                continue;
+            if (find_scale(r->cohesion, m->cohesion, nseg1, &cs[p]) &&
+                find_scale(r->friction_angle, m->friction_angle, nseg1, &fs[p]) &&
+                find_scale(&r->refvisc, &m->refvisc, 1, &vs[p]))
+                base_of[p] = b;
+        }
+        if (base_of[p] < 0) {
+            if (nb == SNAC_MAX_PHASES) {
+                rc = SNAC_GPU_ENOTSUP; /* more distinct phases than scaled copies of 32 */
+                break;
+            }
+            bases[nb] = p;
+            base_of[p] = nb++;
+            cs[p] = fs[p] = vs[p] = 1.0;
+        }
+        need_c |= cs[p] != 1.0;
+        need_f |= fs[p] != 1.0;
+        need_v |= vs[p] != 1.0;
+    }
+    if (!rc) {
+        snac_material* mats = (snac_material*)calloc((size_t)nb, sizeof(snac_material));
+        int* maxit = (int*)calloc((size_t)nb, sizeof(int));
+        double* tol = (double*)calloc((size_t)nb, sizeof(double));
+        for (b = 0; b < nb; b++) {
+            mats[b] = st->materials[bases[b]];
+            maxit[b] = st->dpMaxIterations[bases[b]];
+            tol[b] = st->dpTolerance[bases[b]];
+        }
+        if (need_c) st->cohesionScale = (double*)malloc(sizeof(double) * (size_t)(ne > 0 ? ne : 1));
+        if (need_f) st->frictionScale = (double*)malloc(sizeof(double) * (size_t)(ne > 0 ? ne : 1));
+        if (need_v) st->viscScale = (double*)malloc(sizeof(double) * (size_t)(ne > 0 ? ne : 1));
+        for (e = 0; e < ne; e++) {
+            const int q = st->elementMaterial[e];
+            if (need_c) st->cohesionScale[e] = cs[q];
+            if (need_f) st->frictionScale[e] = fs[q];
+            if (need_v) st->viscScale[e] = vs[q];
+            st->elementMaterial[e] = base_of[q];
+        }
+        free(st->materials);
+        free(st->dpMaxIterations);
+        free(st->dpTolerance);
+        st->materials = mats;
+        st->dpMaxIterations = maxit;
+        st->dpTolerance = tol;
+        d->n_materials = nb;
+        d->materials = mats;
+        d->dp_max_iterations = maxit;
+        d->dp_tolerance = tol;
+        d->element_cohesion_scale = st->cohesionScale;
+        d->element_friction_scale = st->frictionScale;
+        d->element_visc_scale = st->viscScale;
+    }
+    free(base_of);
+    free(cs);
+    free(fs);
+    free(vs);
+    return rc;
+}
+
 void SnacCuda_FreeDescStore(SnacCuda_DescStore* st) {
     free(st->materials);
     free(st->elementMaterial);
@@ -155,6 +293,9 @@ void SnacCuda_FreeDescStore(SnacCuda_DescStore* st) {
     free(st->temperatureBCValue);
     free(st->dpMaxIterations);
     free(st->dpTolerance);
+    free(st->cohesionScale);
+    free(st->frictionScale);
+    free(st->viscScale);
     memset(st, 0, sizeof *st);
 }
 
@@ -247,6 +388,10 @@ int SnacCuda_FillDesc(Snac_Context* context, SnacCuda_Context* self, snac_gpu_de
     d->dp_max_iterations = st->dpMaxIterations;
     d->dp_tolerance = st->dpTolerance;
     d->element_material = st->elementMaterial;
+    if (nmat > SNAC_MAX_PHASES) {
+        int rc = group_phases(d, st, ne);
+        if (rc) return rc;
+    }
 
     /* the state after the ICs, as initial values */
     st->initStress = (double*)malloc(sizeof(double) * (size_t)(ne * Tetrahedra_Count * 6 + 1));
@@ -304,7 +449,7 @@ void SnacCuda_Pack(Snac_Context* context, SnacCuda_Context* self) {
         alloc_doubles(&self->plasticStrain, ne * Tetrahedra_Count);
     if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC || self->constitutive == SNAC_RHEOLOGY_MAXWELL)
         alloc_doubles(&self->viscosity, ne * Tetrahedra_Count);
-    if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) alloc_doubles(&self->plasticStrainTensor, ne * Tetrahedra_Count * 6);
+    if (self->druckerPrager) alloc_doubles(&self->plasticStrainTensor, ne * Tetrahedra_Count * 6);
     if (self->temperature) alloc_doubles(&self->temperature_, nn);
     for (n = 0; n < nn; n++) {
         Snac_Node* node = Snac_Node_At(context, n);
@@ -328,9 +473,12 @@ void SnacCuda_Pack(Snac_Context* context, SnacCuda_Context* self) {
                 self->plasticStrain[e * Tetrahedra_Count + t] = plastic_of(context, self, element)->plasticStrain[t];
             if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
                 SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
-                double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 self->plasticStrain[e * Tetrahedra_Count + t] = vp->plasticStrain[t];
                 self->viscosity[e * Tetrahedra_Count + t] = vp->viscosity[t];
+            }
+            if (self->druckerPrager) {
+                SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
+                double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 q[0] = vp->plasticstrainTensor[t][0][0];
                 q[1] = vp->plasticstrainTensor[t][1][1];
                 q[2] = vp->plasticstrainTensor[t][2][2];
@@ -372,9 +520,12 @@ void SnacCuda_Unpack(Snac_Context* context, SnacCuda_Context* self) {
                 plastic_of(context, self, element)->plasticStrain[t] = self->plasticStrain[e * Tetrahedra_Count + t];
             if (self->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {
                 SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
-                const double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 vp->plasticStrain[t] = self->plasticStrain[e * Tetrahedra_Count + t];
                 vp->viscosity[t] = self->viscosity[e * Tetrahedra_Count + t];
+            }
+            if (self->druckerPrager) {
+                SnacViscoPlastic_Element* vp = viscoplastic_of(context, self, element);
+                const double* q = &self->plasticStrainTensor[(e * Tetrahedra_Count + t) * 6];
                 vp->plasticstrainTensor[t][0][0] = q[0];
                 vp->plasticstrainTensor[t][1][1] = q[1];
                 vp->plasticstrainTensor[t][2][2] = q[2];

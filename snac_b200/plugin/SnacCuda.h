@@ -39,6 +39,7 @@ typedef struct SnacCuda_Context {
     snac_gpu* gpu;
     int constitutive;               /* SNAC_RHEOLOGY_* of the one constitutive hook */
     int temperature;                /* SnacTemperature loaded */
+    int druckerPrager;              /* visco-plastic with a Drucker-Prager phase: the tensor is kept */
     ExtensionInfo_Index plasticElement, viscoPlasticElement, maxwellElement, temperatureNode, temperatureContext;
     long long ne, nn;
     /* the ABI's element-major host arrays (snac_state_view) */
@@ -66,6 +67,9 @@ typedef struct SnacCuda_DescStore {
     double* temperatureBCValue;
     int* dpMaxIterations;
     double* dpTolerance;
+    double* cohesionScale;   /* per element, when the phases were grouped into scaled bases */
+    double* frictionScale;
+    double* viscScale;
 } SnacCuda_DescStore;
 
 Index _SnacCuda_Register(PluginsManager* pluginsMgr);

@@ -33,7 +33,7 @@ _DP = C.POINTER(C.c_double)
 
 class CudaContext(C.Structure):
     """SnacCuda_Context (snac_b200/plugin/SnacCuda.h)."""
-    _fields_ = [("gpu", C.c_void_p), ("constitutive", C.c_int), ("temperature", C.c_int),
+    _fields_ = [("gpu", C.c_void_p), ("constitutive", C.c_int), ("temperature", C.c_int), ("druckerPrager", C.c_int),
                 ("plasticElement", C.c_uint), ("viscoPlasticElement", C.c_uint), ("maxwellElement", C.c_uint),
                 ("temperatureNode", C.c_uint), ("temperatureContext", C.c_uint),
                 ("ne", C.c_longlong), ("nn", C.c_longlong),
@@ -45,7 +45,7 @@ class DescStore(C.Structure):
     _fields_ = [(n, C.c_void_p) for n in ("materials", "elementMaterial", "initStress", "initVelocity",
                                           "initTemperature", "velocityBCMask", "velocityBCValue",
                                           "temperatureBCMask", "temperatureBCValue", "dpMaxIterations",
-                                          "dpTolerance")]
+                                          "dpTolerance", "cohesionScale", "frictionScale", "viscScale")]
 
 
 def host(cfg):
@@ -85,7 +85,7 @@ def test_unknown_plugin_is_refused():
     assert h.load_plugin("SnacNoSuchPlugin") != 0
 
 
-@pytest.mark.parametrize("case", ["plastic", "viscoplastic", "maxwell", "winkler"])
+@pytest.mark.parametrize("case", ["plastic", "viscoplastic", "maxwell", "winkler", "drucker_prager"])
 def test_pack_unpack_round_trip_bitwise(case):
     """State of a context stepped by the reference sources -> the library's
     arrays (pack) equal its own element-major view; wiping the context and
@@ -103,7 +103,10 @@ def test_pack_unpack_round_trip_bitwise(case):
     assert (cx.ne, cx.nn) == (ne, nn)
     packed = {"coord": (cx.coord, nn * 3), "velocity": (cx.velocity, nn * 3), "stress": (cx.stress, ne * 60),
               "plastic_strain": (cx.plasticStrain, ne * 10), "viscosity": (cx.viscosity, ne * 10),
-              "temperature": (cx.temperature_, nn)}
+              "temperature": (cx.temperature_, nn), "plastic_strain_tensor": (cx.plasticStrainTensor, ne * 60)}
+    assert bool(cx.plasticStrainTensor) == (case == "drucker_prager")
+    if case == "drucker_prager":
+        assert np.count_nonzero(want.plastic_strain_tensor) > 0
     for f, (p, n) in packed.items():
         if p:
             assert np.array_equal(np.ctypeslib.as_array(p, (n,)), getattr(want, f).reshape(-1)), f
@@ -114,7 +117,7 @@ def test_pack_unpack_round_trip_bitwise(case):
     h.set_state(zero)  # wipe what the unpack writes
     plugin_fn(h, "SnacCuda_Unpack", C.c_void_p, C.c_void_p)(ctx, ext)
     got = h.state()
-    for f in FIELDS:
+    for f in FIELDS + ("plastic_strain_tensor",):
         if f in ("plastic_strain",) and cfg.plugin not in ("SnacPlastic", "SnacViscoPlastic"):
             continue
         assert np.array_equal(getattr(got, f), getattr(want, f)), f
@@ -128,7 +131,7 @@ def _wall_mask(cfg, wall):
             "front": k == nnz - 1, "all": np.ones_like(i, bool)}[wall]
 
 
-@pytest.mark.parametrize("case", ["elastic", "lithostatic", "viscoplastic", "traction"])
+@pytest.mark.parametrize("case", ["elastic", "lithostatic", "viscoplastic", "traction", "plastic_phases"])
 def test_fill_desc_from_the_context(case):
     """The descriptor the plugin builds from the context: mesh, phases, the
     state after the ICs, and the conditions resolved per node, last VC
@@ -173,6 +176,18 @@ def test_fill_desc_from_the_context(case):
             assert np.array_equal(np.ctypeslib.as_array(d.node_temperature_bc_mask, (nn,)), tmask)
         if cfg.hydrostatic_ic:
             assert d.pisos != 0.0 and d.rzbo == cfg.min[1]
+        if cfg.element_cohesion_scale is not None:
+            # one phase per element in the context, grouped back into scaled base phases:
+            # each element's cohesion table is reproduced to the bit by base x scale
+            assert 1 <= d.n_materials <= 32 and d.element_cohesion_scale
+            cs = np.ctypeslib.as_array(d.element_cohesion_scale, (ne,))
+            em = np.ctypeslib.as_array(d.element_material, (ne,))
+            for e in range(ne):
+                base = d.materials[int(em[e])]
+                for i in range(base.nsegments + 1):
+                    src = cfg.materials[cfg.element_material[e] if cfg.element_material is not None else 0]
+                    want = src[f"cohesion{i}"] * cfg.element_cohesion_scale[e]
+                    assert base.cohesion[i] * cs[e] == want
         # the probe leaves the context's velocities as they were
         assert np.array_equal(h.state().velocity, state.velocity)
     finally:
@@ -187,7 +202,7 @@ def relerr(a, b):
 @pytest.mark.gpu
 @pytest.mark.parametrize("case, tol", [("elastic", 0.0), ("plastic", 0.0), ("plastic_phases", 0.0),
                                        ("lithostatic", 0.0), ("winkler", 0.0), ("traction", 0.0), ("topo", 0.0),
-                                       ("viscoplastic", 1e-6), ("maxwell", 1e-9)])
+                                       ("viscoplastic", 1e-6), ("maxwell", 1e-9), ("drucker_prager", 1e-6)])
 def test_context_driven_through_the_plugin(case, tol):
     """60 steps of a Snac_Context through the plugin's hooks (step zero,
     then Dt / Solve / Sync per step, then Dump) against the compiled
@@ -209,7 +224,7 @@ def test_context_driven_through_the_plugin(case, tol):
     ref_mid = ref.state()
     ref.step(steps - steps // 2)
     want = ref.state()
-    fields = [f for f in FIELDS if f not in ("force", "inertial_mass")] + ["force", "inertial_mass"]
+    fields = list(FIELDS) + ["plastic_strain_tensor"]
     for a, b in ((mid, ref_mid), (got, want)):
         for f in fields:
             x, y = getattr(a, f), getattr(b, f)
