@@ -398,24 +398,32 @@ def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
     if with_e2e and not args.no_e2e:
         from snac_b200.abi import State
         st = ctx.state()
-        fields = ["coord", "velocity", "stress", "plastic_strain"]
+        # the model's state, what one step reads and writes: coordinates, velocities,
+        # stresses, and the plugins' per-tet / per-node state (plastic strain,
+        # temperature, the Drucker-Prager tensor) where the model has them
+        fields = ["coord", "velocity", "stress"]
+        if cfg.plugin in ("SnacPlastic", "SnacViscoPlastic"):
+            fields.append("plastic_strain")
+        if cfg.temperature:
+            fields.append("temperature")
+        if ctx.keeps_plastic_strain_tensor:
+            fields.append("plastic_strain_tensor")
         host = State.empty(ctx.ne, ctx.nn)
-        pinned = {}
-        for f in fields:
-            t = torch.from_numpy(getattr(st, f)).pin_memory()
-            pinned[f] = t
-            setattr(host, f, t.numpy())
-        h2d = sum(pinned[f].numel() * 8 for f in fields)
         out = State.empty(ctx.ne, ctx.nn)       # the step's result, into pinned host buffers
-        if not ctx.keeps_plastic_strain_tensor:
-            out.plastic_strain_tensor = None    # the model has none
         keep = []
         for f, _ in out.view()._fields_:
-            a = getattr(out, f, None)
-            if a is not None:
-                t = torch.from_numpy(a).pin_memory()
+            if f in fields:
+                t = torch.from_numpy(getattr(st, f)).pin_memory()
+                keep.append(t)
+                setattr(host, f, t.numpy())
+                t = torch.from_numpy(getattr(out, f)).pin_memory()
                 keep.append(t)
                 setattr(out, f, t.numpy())
+            else:
+                setattr(host, f, None)
+                setattr(out, f, None)
+        h2d = sum(getattr(host, f).nbytes for f in fields)
+        d2h = sum(getattr(out, f).nbytes for f in fields)
         ke = max(3, min(args.steps, 10))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
@@ -425,12 +433,10 @@ def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
             ctx.state(out)                       # device -> host, the step's result
         torch.cuda.synchronize()
         te = (time.perf_counter() - t0) / ke
-        d2h = sum(getattr(out, f).nbytes for f in ("coord", "velocity", "stress", "plastic_strain", "viscosity",
-                                                    "temperature", "force", "inertial_mass"))
         e2e = {"value": ws * ne / allmax(ws, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
-               "note": "per step: snac_gpu_upload of the state from pinned host buffers, snac_gpu_step(1), "
-                       "snac_gpu_download of the state"}
+               "note": "per step: snac_gpu_upload of the state (" + ", ".join(fields) + ") from pinned host "
+                       "buffers, snac_gpu_step(1), snac_gpu_download of the same fields into pinned host buffers"}
 
     ctx.close()
     cpu = None
@@ -539,27 +545,37 @@ def run_ensemble(args, ws, rank, local, with_e2e=True, with_cpu=True):
     # step, every model's state down, per step
     e2e = None
     if with_e2e and not args.no_e2e:
-        fields = ["coord", "velocity", "stress", "plastic_strain", "viscosity", "temperature"]
-        hosts = []
+        def state_fields(m):  # a model's state: what one step reads and writes
+            f = ["coord", "velocity", "stress"]
+            if m.cfg.plugin in ("SnacPlastic", "SnacViscoPlastic"):
+                f.append("plastic_strain")
+            if m.cfg.temperature:
+                f.append("temperature")
+            return f
+
+        hosts, outs = [], []
         for m in b.models:
             st = m.state()
-            h = State.empty(m.ne, m.nn)
-            for f in fields:
-                setattr(h, f, torch.from_numpy(getattr(st, f)).pin_memory().numpy())
-            hosts.append(h)
-        h2d = sum(getattr(h, f).nbytes for h in hosts for f in fields)
+            fl = state_fields(m)
+            h, o = State.empty(m.ne, m.nn), State.empty(m.ne, m.nn)
+            for f, _ in h.view()._fields_:
+                setattr(h, f, torch.from_numpy(getattr(st, f)).pin_memory().numpy() if f in fl else None)
+                setattr(o, f, torch.from_numpy(getattr(o, f)).pin_memory().numpy() if f in fl else None)
+            hosts.append((h, fl))
+            outs.append(o)
+        h2d = sum(getattr(h, f).nbytes for h, fl in hosts for f in fl)
+        d2h = h2d
         ke = 2
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(ke):
-            for m, h in zip(b.models, hosts):
-                m.set_state(h, fields)
+            for m, (h, fl) in zip(b.models, hosts):
+                m.set_state(h, fl)
             b.step(1)
-            outs = [m.state() for m in b.models]
+            for m, o in zip(b.models, outs):
+                m.state(o)
         torch.cuda.synchronize()
         te = (time.perf_counter() - t0) / ke
-        d2h = sum(getattr(o, f).nbytes for o in outs for f in ("coord", "velocity", "stress", "plastic_strain",
-                                                               "viscosity", "temperature", "force", "inertial_mass"))
         e2e = {"value": ws * ne / allmax(ws, te), "unit": UNIT, "h2d_bytes_per_step": int(h2d),
                "d2h_bytes_per_step": int(d2h),
                "note": "per step: snac_gpu_upload of every model's state from pinned host buffers, "
