@@ -353,19 +353,19 @@ def _host_threads():
         return os.cpu_count() or 1
 
 
-def test_c2_full_size_200_steps_bitwise_against_the_reference():
-    """The Mohr-Coulomb workload at full size (64 x 32 x 64 hex) over 200 steps,
+def test_c2_full_size_1000_steps_bitwise_against_the_reference():
+    """The Mohr-Coulomb workload at full size (64 x 32 x 64 hex) over 1000 steps,
     against the reference's own sources (libsnacref_mt.so: the serial build's
-    bits, its element and node loops on the host's threads): bitwise, at
-    the midpoint and the end."""
+    bits, its element and node loops on the host's threads): bitwise after
+    200 steps and after 1000."""
     cfg = W.c2_plastic()
     g = SnacContext(cfg)
     c = Checker(cfg, "reference_mt", threads=_host_threads())
     g.time_step_zero()
     c.time_step_zero()
-    for _ in range(2):
-        g.step(100)
-        c.step(100)
+    for n in (200, 800):
+        g.step(n)
+        c.step(n)
         assert_bitwise(g, c)
 
 
