@@ -233,3 +233,24 @@ def test_context_driven_through_the_plugin(case, tol):
             else:
                 assert relerr(x, y) <= tol, (case, f, relerr(x, y))
     assert h.scalars().dt == ref.scalars().dt or tol > 0
+
+
+def test_unrelated_phases_beyond_the_table_are_refused():
+    """Forty phases that differ in their elastic moduli are not scaled copies
+    of a base phase: the descriptor cannot express them and is refused."""
+    from snac_b200 import workloads as W
+    cfg = S.plastic_small()
+    cfg.element_cohesion_scale = None
+    base = cfg.materials[0]
+    cfg.materials = [dict(base, mu=base["mu"] * (1.0 + 0.01 * p)) for p in range(40)]
+    cfg.element_material = (np.arange(cfg.n_elements) % 40).astype(np.int32)
+    h = host(cfg)
+    ctx, ext = h.context_ptr(), h.extension_ptr("SnacCuda")
+    assert plugin_fn(h, "SnacCuda_Inspect", C.c_void_p, C.c_void_p, restype=C.c_int)(ctx, ext) == 0
+    d, st = Desc(), DescStore()
+    fill = plugin_fn(h, "SnacCuda_FillDesc", C.c_void_p, C.c_void_p, C.POINTER(Desc), C.POINTER(DescStore),
+                     restype=C.c_int)
+    try:
+        assert fill(ctx, ext, C.byref(d), C.byref(st)) == -9  # SNAC_GPU_ENOTSUP
+    finally:
+        plugin_fn(h, "SnacCuda_FreeDescStore", C.POINTER(DescStore))(C.byref(st))
