@@ -34,6 +34,7 @@ import subprocess
 import sys
 import threading
 import time
+from typing import Optional
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -51,18 +52,20 @@ NODES_PER_HEX = {"c1": 2601 / 2048, "c2": 139425 / 131072, "c3": 1081665 / 10485
 # DRAM bytes (read + write) of one launch of the dominant kernel, from one
 # ncu capture of that kernel on the same workload
 # (profiles/k_fused_step_plastic_64x32x64.md); None where none was taken.
-NCU_TRAFFIC = {("c2", "k_fused_step"): 83.648000e6 + 167.135744e6}
+NCU_TRAFFIC = {("c2", "k_fused_step"): 83.627520e6 + 153.497600e6,
+               ("c3", "k_fused_stress"): 657.412352e6 + 1706.645248e6}
 # what bounds the dominant kernel instead of HBM, from the same kind of ncu
 # capture (fractions of peak; profiles/k_fused_step_plastic_64x32x64.md,
 # profiles/k_fused_stress_viscoplastic_128x64x128.md)
-NCU_PIPES = {("c2", "k_fused_step"): {"fp64_pipe": 0.383, "issue_active": 0.455, "dram_throughput": 0.179},
-             ("c3", "k_fused_stress"): {"fp64_pipe": 0.374, "dram_throughput": 0.188}}
+NCU_PIPES = {("c2", "k_fused_step"): {"fp64_pipe": 0.384, "issue_active": 0.461, "dram_throughput": 0.175},
+             ("c3", "k_fused_stress"): {"fp64_pipe": 0.389, "issue_active": 0.480, "dram_throughput": 0.195}}
 # FP64 instructions (thread level: DADD, DMUL, DFMA) of one launch of the
 # dominant kernel, from one ncu capture of it on the same workload
 # (smsp__sass_thread_inst_executed_op_{dadd,dmul,dfma}_pred_on.sum); None
 # where none was taken.  With the device's FP64 rate, measured live by
 # snac_gpu_fp64_rate, they give the kernel's FP64 roofline.
-NCU_FP64 = {}
+NCU_FP64 = {("c2", "k_fused_step"): {"dadd": 382913409, "dmul": 449323008, "dfma": 208497024},
+            ("c3", "k_fused_stress"): {"dadd": 3477029944, "dmul": 3983840824, "dfma": 2411197120}}
 ARITHMETIC = {
     "c1": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
     "c2": "reference rounding (no FMA contraction), bitwise equal to the CPU oracle",
@@ -472,6 +475,36 @@ def run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=True):
     return None
 
 
+def verbatim_bc_cost(seconds: float) -> Optional[dict]:
+    """The cost of the reference's boundary-condition lookup on the elastic
+    16x8x16 workload, one core: StGermain's VariableCondition_ApplyToIndex
+    searches the condition's index table linearly for every node and step
+    (VariableCondition.c:449-463); the checkers (and the baselines above) use
+    an O(1) per-node mask with the same results.  None without the compiled
+    reference."""
+    from oracle.pyoracle import Checker
+    if cpu_checker_kind(1) != "reference":
+        return None
+    cfg = make_workload("c1")
+    out = {}
+    for name, on in (("mask", False), ("verbatim", True)):
+        ck = Checker(cfg, "reference")
+        ck.set_verbatim_bc(on)
+        ck.time_step_zero()
+        ck.step(1)
+        n, t = 0, 0.0
+        while t < seconds / 2:
+            t0 = time.perf_counter()
+            if ck.step(1) != 0:
+                raise RuntimeError(ck.last_error())
+            t += time.perf_counter() - t0
+            n += 1
+        ck.close()
+        out[name] = cfg.n_elements * n / t
+    return {"workload": "elastic 16x8(y)x16 hex", "unit": UNIT, "mask": out["mask"], "verbatim": out["verbatim"],
+            "slowdown": out["mask"] / out["verbatim"]}
+
+
 def cpu_baseline(workload: str, ne: int, args) -> dict:
     """The reference's own sources on the host: all host threads (the
     headline CPU figure) and one core, each a time-boxed sample of whole
@@ -481,7 +514,8 @@ def cpu_baseline(workload: str, ne: int, args) -> dict:
     return {"value": v, "unit": UNIT, "cores": used, "kind": kind, "host": host_info(),
             "sample": f"{n} SNAC steps of the full {workload} mesh ({ne} hex) on {used} host threads "
                       f"(element and node loops split across them), {t:.1f} s",
-            "one_core": {"value": v1, "unit": UNIT, "steps": n1, "seconds": round(t1, 2)}}
+            "one_core": {"value": v1, "unit": UNIT, "steps": n1, "seconds": round(t1, 2)},
+            "verbatim_bc": verbatim_bc_cost(4.0)}
 
 
 # Algorithmic bytes per hex of one launch of each kernel (state it must read / write once).

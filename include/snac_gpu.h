@@ -359,10 +359,13 @@ int  snac_gpu_selftest_division(long long n, unsigned long long seed, long long*
  * and viscosity scales (element_cohesion_scale / element_friction_scale /
  * element_visc_scale; an absent array is a scale of 1).  On return the model
  * holds the forward's final state, as after snac_gpu_step(h, nsteps).
- * Differentiated physics: SnacPlastic and SnacViscoPlastic (Mohr-Coulomb
- * return map along the branch the forward took), dtType constant, no density
- * coupling or thermal stress, temperature held fixed (thermal_conduct = 0);
- * otherwise SNAC_GPU_ENOTSUP. */
+ * Differentiated physics: the SnacElastic, SnacMaxwell, SnacPlastic and
+ * SnacViscoPlastic hooks (Mohr-Coulomb return map along the branch the
+ * forward took), dtType constant, no density coupling or thermal stress,
+ * temperature held fixed (thermal_conduct = 0); otherwise SNAC_GPU_ENOTSUP.
+ * (The parameter gradients of the elastic and Maxwell hooks are zero: no
+ * scale enters them; snac_gpu_adjoint_grads also returns the gradients with
+ * respect to the initial state.) */
 typedef struct snac_adjoint_desc {
     int nsteps;
     int checkpoint_every;
@@ -380,6 +383,24 @@ typedef struct snac_adjoint_stats {
 
 int  snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, double* grad_cohesion,
                       double* grad_friction, double* grad_viscosity, snac_adjoint_stats* stats);
+/* The same sweep, returning any subset of dL/d(scale) and of the gradients
+ * with respect to the state the model held on entry: coordinates and
+ * velocities (node order, 3 per node), the tet stresses and plastic
+ * strains (element-major, as the state view lays them out).  The state
+ * gradients hold every other state entry fixed; for the Maxwell hook that
+ * includes the stored tet volumes the first step's volume ratio reads.
+ * A null pointer skips that output. */
+typedef struct snac_adjoint_grads {
+    double* cohesion;        /* [ne]        */
+    double* friction;        /* [ne]        */
+    double* viscosity;       /* [ne]        */
+    double* coordinates;     /* [nn*3]      */
+    double* velocity;        /* [nn*3]      */
+    double* stress;          /* [ne*10*6]   */
+    double* plastic_strain;  /* [ne*10]     */
+} snac_adjoint_grads;
+int  snac_gpu_adjoint_grads(snac_gpu* h, const snac_adjoint_desc* a, double* loss, const snac_adjoint_grads* g,
+                            snac_adjoint_stats* stats);
 /* L of the current state (no stepping): the forward half of the above, for
  * finite-difference checks. */
 int  snac_gpu_misfit(snac_gpu* h, const snac_adjoint_desc* a, double* loss);

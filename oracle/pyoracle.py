@@ -77,6 +77,8 @@ def _lib(kind: str):
         else:
             lib_fn("set_threads").argtypes = [C.c_int]
             lib_fn("threads").restype = C.c_int
+            if kind in ("reference", "reference_mt"):
+                lib_fn("set_verbatim_bc").argtypes = [vp, C.c_int]
         lib_fn("step").argtypes = [vp, C.c_int]
         lib_fn("step").restype = C.c_int
         lib_fn("get_state").argtypes = [vp, C.POINTER(StateView)]
@@ -164,6 +166,15 @@ class Checker:
 
     def set_dt(self, dt: float):
         self._f("set_dt")(self.h, C.c_double(dt))
+
+    def set_verbatim_bc(self, on: bool = True):
+        """Compiled reference only: the boundary conditions' ApplyToIndex
+        searches its index table linearly, as StGermain's does
+        (VariableCondition.c:449-463), instead of the O(1) per-node mask
+        (same results, the reference's cost)."""
+        if self.kind not in ("reference", "reference_mt"):
+            raise ValueError("the verbatim search is an option of the compiled reference")
+        self._f("set_verbatim_bc")(self.h, 1 if on else 0)
 
     def last_error(self) -> str:
         return self._f("last_error")(self.h).decode()

@@ -211,6 +211,7 @@ typedef struct ref_ctx {
     double (*mass_store);
     double (*balance_store)[3];
     long timeStep_total;
+    int verbatim_bc; /* VariableCondition_ApplyToIndex searches its index table as the reference does */
 } ref_ctx;
 
 static ref_ctx* g_current; /* the constitutive trampoline needs the hook */
@@ -223,6 +224,7 @@ static ref_ctx* g_current; /* the constitutive trampoline needs the hook */
  * without it the loops are the serial ones. */
 static int g_threads = 1;
 void ref_set_threads(int n) { g_threads = n < 1 ? 1 : (n > 256 ? 256 : n); }
+void ref_set_verbatim_bc(ref_ctx* r, int on) { r->verbatim_bc = on != 0; }
 int ref_threads(void) {
 #ifdef REF_THREADS
     return g_threads;
@@ -278,9 +280,22 @@ static void run_constitutive(void* ep, void* ctx, Element_LocalIndex e) {
     g_current->hook(ctx, e);
 }
 
+/* VariableCondition_ApplyToIndex (StGermain VariableCondition.c:449-463)
+ * first finds the index in the condition's index table by a linear search
+ * and returns when it is absent; the table of a CompositeVC is the union of
+ * its walls' node sets in ascending node order.  The per-node masks below
+ * give the same result in O(1); with verbatim_bc the search runs first, as
+ * in the reference, so that its cost can be timed. */
+static int vc_has_index(const VariableCondition* vc, Index n) {
+    Index q;
+    for (q = 0; q < vc->indexCount; q++)
+        if (vc->indexTbl[q] == n) break;
+    return q < vc->indexCount;
+}
 static void vbc_apply_index(VariableCondition* vc, Index n, void* context) {
     ref_ctx* r = (ref_ctx*)((char*)vc - offsetof(ref_ctx, vbc));
     (void)context;
+    if (r->verbatim_bc && !vc_has_index(vc, n)) return;
     for (int d = 0; d < 3; d++)
         if (r->vbc_mask[n] & (1u << d)) r->mesh.node[n].velocity[d] = r->vbc_val[n][d];
 }
@@ -290,6 +305,7 @@ static void vbc_apply(VariableCondition* vc, void* context) {
 static void tbc_apply_index(VariableCondition* vc, Index n, void* context) {
     ref_ctx* r = (ref_ctx*)((char*)vc - offsetof(ref_ctx, tbc));
     (void)context;
+    if (r->verbatim_bc && !vc_has_index(vc, n)) return;
     if (r->tbc_mask[n]) r->tn[n].temperature = r->tbc_val[n];
 }
 static void tbc_apply(VariableCondition* vc, void* context) {

@@ -1,6 +1,10 @@
 """FP64 adjoint of the SNAC step through the C ABI (snac_gpu_adjoint).
 
     loss, g = adjoint(ctx, nsteps, target_vy, target_y)   # g["cohesion"], g["friction"], g["viscosity"]
+    r = adjoint(ctx, nsteps, target_vy, target_y, state=True)
+    # also r.grad["coordinates"], ["velocity"] ([nn, 3]), ["stress"] ([ne*10, 6]),
+    # ["plastic_strain"] ([ne*10]): gradients with respect to the entry state
+    # (snac_gpu_adjoint_grads)
 
 `SnacMisfit` wraps the same call as a torch.autograd.Function of the three
 per-element scale fields:
@@ -32,6 +36,11 @@ class AdjointDesc(C.Structure):
                 ("w_v", C.c_double), ("w_h", C.c_double)]
 
 
+class AdjointGrads(C.Structure):
+    _fields_ = [(k, _DP) for k in ("cohesion", "friction", "viscosity", "coordinates", "velocity", "stress",
+                                   "plastic_strain")]
+
+
 class AdjointStats(C.Structure):
     _fields_ = [("ms_forward", C.c_double), ("ms_reverse", C.c_double), ("checkpoint_every", C.c_int),
                 ("checkpoints", C.c_int)]
@@ -43,6 +52,9 @@ def _bind():
         lib.snac_gpu_adjoint.argtypes = [C.c_void_p, C.POINTER(AdjointDesc), _DP, _DP, _DP, _DP,
                                          C.POINTER(AdjointStats)]
         lib.snac_gpu_adjoint.restype = C.c_int
+        lib.snac_gpu_adjoint_grads.argtypes = [C.c_void_p, C.POINTER(AdjointDesc), _DP, C.POINTER(AdjointGrads),
+                                               C.POINTER(AdjointStats)]
+        lib.snac_gpu_adjoint_grads.restype = C.c_int
         lib.snac_gpu_misfit.argtypes = [C.c_void_p, C.POINTER(AdjointDesc), _DP]
         lib.snac_gpu_misfit.restype = C.c_int
         lib._adjoint_bound = True
@@ -76,18 +88,23 @@ class AdjointResult:
 
 
 def adjoint(ctx: SnacContext, nsteps: int, target_vy, target_y, w_v: float = 1.0, w_h: float = 1.0,
-            checkpoint_every: int = 0) -> AdjointResult:
+            checkpoint_every: int = 0, state: bool = False) -> AdjointResult:
     """Loss after nsteps steps from the context's current state and its
     gradient with respect to the per-element cohesion, friction and viscosity
-    scales.  The context ends at the forward's final state."""
+    scales, and with state=True also with respect to the entry state
+    (coordinates, velocities, tet stresses and plastic strains).  The context
+    ends at the forward's final state."""
     lib = _bind()
     d, keep = _desc(nsteps, target_vy, target_y, w_v, w_h, checkpoint_every)
-    ne = ctx.ne
+    ne, nn, nq = ctx.ne, ctx.nn, ctx.ne * 10
     g = {k: np.zeros(ne) for k in ("cohesion", "friction", "viscosity")}
+    if state:
+        g.update(coordinates=np.zeros((nn, 3)), velocity=np.zeros((nn, 3)), stress=np.zeros((nq, 6)),
+                 plastic_strain=np.zeros(nq))
+    gr = AdjointGrads(**{k: v.ctypes.data_as(_DP) for k, v in g.items()})
     loss = C.c_double()
     st = AdjointStats()
-    rc = lib.snac_gpu_adjoint(ctx.h, C.byref(d), C.byref(loss), g["cohesion"].ctypes.data_as(_DP),
-                              g["friction"].ctypes.data_as(_DP), g["viscosity"].ctypes.data_as(_DP), C.byref(st))
+    rc = lib.snac_gpu_adjoint_grads(ctx.h, C.byref(d), C.byref(loss), C.byref(gr), C.byref(st))
     ctx._check(rc)
     return AdjointResult(loss.value, g, st.ms_forward, st.ms_reverse, st.checkpoint_every, st.checkpoints)
 

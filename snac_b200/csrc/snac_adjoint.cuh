@@ -2,15 +2,18 @@
 //
 // Gradients of a loss on the final top-surface vertical velocity and
 // topography with respect to the per-element cohesion, friction-angle and
-// viscosity scales (Fields::coh_scale / fric_scale / visc_scale), for the
-// Mohr-Coulomb plastic and visco-plastic constitutive hooks with a constant
-// dt.  The temperature field is held fixed (zero conductivity).
+// viscosity scales (Fields::coh_scale / fric_scale / visc_scale) and to the
+// entry state (coordinates, velocities, tet stresses, plastic strains), for
+// the elastic, Maxwell, Mohr-Coulomb plastic and visco-plastic constitutive
+// hooks with a constant dt.  The temperature field is held fixed (zero
+// conductivity).
 //
 // Forward step n (what is differentiated; the per-tet operations are those
 // of csrc/snac_kernels.cuh):
 //   sigma_pre^n = Rot(sigma_avg^{n-1}, v^n, G(x^n))       (end of step n-1)
 //   sr          = StrainRate(v^n, G(x^n)) + mixed averaging over the hex
 //   sigma_c     = Constitutive(sigma_pre^n, sr dt, eps_p^n, scales)
+//                 (Maxwell: also the volume ratio V(x^n) / V(x^{n-1}))
 //   sigma_avg^n = trace averaging of sigma_c over the hex
 //   F, m        = Force(sigma_avg^n, G(x^n))                (node gather)
 //   v^{n+1}     = v^n + dt damp(F, v^n) / m   (BC components fixed)
@@ -41,6 +44,7 @@ struct AdjState {
     const double4* force;  // damped force and inertial mass of step n-1
     const double* stress;  // sigma_avg^{n-1} (n >= 1) or sigma_pre^0 (n = 0)
     const double* eps_p;   // eps_p^n
+    const double* vol;     // [nq][2] Maxwell: tet volume and old volume as stored (else null)
 };
 
 struct AdjBufs {
@@ -51,6 +55,7 @@ struct AdjBufs {
     double* sbar;    // [nq][6] adjoint of sigma_avg^{n-1}, handed to the next (earlier) step
     double* epbar;   // [nq] adjoint of eps_p
     double* pbar;    // [nq][3] adjoint of the cohesion, friction, viscosity scales
+    double* vobar;   // [nq] Maxwell: adjoint of the volume pass n stored, handed to pass n-1
 };
 
 struct D3 {
@@ -75,6 +80,10 @@ struct ConsRec {
     // visco-plastic Maxwell step
     double trs, tre, d[3], sd[3], Q, J, eta, eta_base, vic1, vic2, tmp;
     bool J_from_sqrt, eta_free;
+    // Maxwell hook: whether the tet's phase takes the update, and the volume
+    // ratio its trace strain is formed from
+    bool mx;
+    double vcur, vold;
     // softening lookup
     double co, hd, fa, da, fa_b, co_b, dpl, tgf_b, tgc_b, tgd;
     bool clamped;
@@ -181,6 +190,8 @@ __device__ __forceinline__ void mc_reverse(const ConsRec& R, const double sb_out
 template <int PLUGIN>
 __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, const Config& cfg, const AdjState& S,
                                              const AdjBufs& B, int rotate, int first_rev, double dt, int lb) {
+    // hooks with a Mohr-Coulomb return map and a plastic strain
+    constexpr bool MC = PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_VISCOPLASTIC;
     TetSlot s = tet_slot(m, lb);
     // corners of step n
     V3 c[4], v[4];
@@ -261,14 +272,17 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     const double cs = (F.coh_scale && s.active) ? F.coh_scale[s.e] : 1.0;
     const double fsc = (F.fric_scale && s.active) ? F.fric_scale[s.e] : 1.0;
     const double vsc = (F.visc_scale && s.active) ? F.visc_scale[s.e] : 1.0;
-    double eps_p = s.active ? S.eps_p[s.q] : 0.0;
+    double eps_p = (MC && s.active) ? S.eps_p[s.q] : 0.0;
     const double eps_p0 = eps_p;
 
     ConsRec R;
     double st[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) st[a] = s_pre[a];
-    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) {
+    R.mx = false;
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_ELASTIC) {
+        // the elastic trial of the plastic hook and the elastic hook's whole update
+        // (the same arithmetic)
         double tr = e[0] + e[1] + e[2];
         st[0] += (2.0f * M.mu) * e[0] + M.lambda * (tr);
         st[1] += (2.0f * M.mu) * e[1] + M.lambda * (tr);
@@ -276,6 +290,38 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         st[3] += (2.0f * M.mu) * e[3];
         st[4] += (2.0f * M.mu) * e[4];
         st[5] += (2.0f * M.mu) * e[5];
+    } else if (PLUGIN == SNAC_RHEOLOGY_MAXWELL) {
+        // maxwell/Constitutive.c:47-184: the trace strain is the volume ratio of the
+        // tet (pass n >= 1 rotates: its own volume over the one the previous pass
+        // stored; pass 0 reads both as the state holds them), the second invariant
+        // includes the shear strains, and only phase 0 takes the update
+        R.mx = (ph == 0);
+        R.trs = st[0] + st[1] + st[2];
+        R.vcur = rotate ? g.V : (s.active ? S.vol[s.q * 2 + 0] : 1.0);
+        R.vold = s.active ? S.vol[s.q * 2 + (rotate ? 0 : 1)] : 1.0;
+        R.tre = dv(R.vcur, R.vold) - 1.0f;
+        const double tn3 = dv3(R.tre), ts3 = dv3(R.trs);
+        for (int a = 0; a < 3; a++) R.d[a] = e[a] - tn3;
+        for (int a = 0; a < 3; a++) R.sd[a] = st[a] - ts3;
+        R.Q = R.d[1] * R.d[2] + R.d[2] * R.d[0] + R.d[0] * R.d[1] - e[3] * e[3] - e[4] * e[4] - e[5] * e[5];
+        double J = sqrt(fabs(R.Q)) / dt;
+        R.J_from_sqrt = !(J == 0.0f);
+        if (J == 0.0f) J = M.refsrate;
+        R.J = J;
+        double avgTemp = 0.0;
+        for (int qn = 0; qn < 4; qn++) avgTemp += 0.25 * T[qn];
+        const double eta = arrhenius_viscosity(M, M.refvisc, J, avgTemp);
+        R.eta_free = (eta > M.vis_min && eta < M.vis_max);
+        R.eta = eta;
+        R.eta_base = 0.0;
+        R.tmp = dv(M.mu, 2.0f * (eta)) * dt;
+        R.vic1 = 1.0f - R.tmp;
+        R.vic2 = dv(1.0f, 1.0f + R.tmp);
+        if (R.mx) {
+            const double bulkm = M.lambda + dv3(2.0f * M.mu);
+            double stressd[3] = {R.sd[0], R.sd[1], R.sd[2]};
+            maxwell_update(st, e, stressd, R.d, ts3, R.tre, M.mu, eta, dt, bulkm);
+        }
     } else {
         const double bulkm = M.lambda + dv3(2.0f * M.mu);
         R.trs = st[0] + st[1] + st[2];
@@ -301,115 +347,119 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
         double stressd[3] = {R.sd[0], R.sd[1], R.sd[2]};
         maxwell_update(st, e, stressd, R.d, dv3(R.trs), R.tre, M.mu, eta, dt, bulkm);
     }
-    // softening lookup: this tet's own segment (plastic: first match, clamp past the end;
-    // visco-plastic: last match)
-    bool matched = false;
-    R.clamped = false;
-    R.co = R.hd = R.fa = R.da = R.fa_b = R.co_b = R.tgf_b = R.tgc_b = R.tgd = 0.0;
-    R.dpl = 1.0;
-    for (int i = 0; i < M.nsegments; i++) {
-        const double pl1 = M.plstrain[i];
-        const double pl2 = M.plstrain[i + 1];
-        if (eps_p >= pl1 && eps_p <= pl2) {
-            const double dpl = pl2 - pl1;
-            R.dpl = dpl;
-            double tg[3] = {M.fric[i + 1] - M.fric[i], M.coh[i + 1] - M.coh[i], M.dil[i + 1] - M.dil[i]};
-            dvz_n(tg, dpl, M.zpl[i]);
-            R.tgf_b = tg[0];
-            R.tgc_b = tg[1];
-            R.tgd = tg[2];
-            R.fa_b = M.fric[i] + R.tgf_b * (eps_p - pl1);
-            R.co_b = M.coh[i] + R.tgc_b * (eps_p - pl1);
-            R.da = M.dil[i] + R.tgd * (eps_p - pl1);
-            matched = true;
-            R.clamped = false;
-            if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) break;
-        } else if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && i == M.nsegments - 1 && eps_p > pl2) {
-            R.fa_b = M.fric[M.nsegments];
-            R.co_b = M.coh[M.nsegments];
-            R.da = M.dil[M.nsegments];
-            R.tgf_b = R.tgc_b = R.tgd = 0.0;
-            matched = true;
-            R.clamped = true;
-            break;
-        }
-    }
-    if (s.active && !matched) report(F.sc, SNAC_GPU_ENOTSUP, s.e);  // the carried-over lookup is not differentiated
-    // values as the forward forms them (scales applied to the table entries)
-    {
-        // recompute exactly as the forward does, for identical branch decisions
-        double fa = 0.0, co = 0.0, hd = 0.0;
-        for (int i = 0; i < M.nsegments; i++) {
-            const double pl1 = M.plstrain[i];
-            const double pl2 = M.plstrain[i + 1];
-            double f0 = F.fric_scale ? M.fric[i] * fsc : M.fric[i];
-            double f1 = F.fric_scale ? M.fric[i + 1] * fsc : M.fric[i + 1];
-            double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
-            double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
-            if (eps_p >= pl1 && eps_p <= pl2) {
-                double tg[2] = {f1 - f0, c1 - c0};
-                dvz_n(tg, pl2 - pl1, M.zpl[i]);
-                const double tgf = tg[0], tgc = tg[1];
-                fa = f0 + tgf * (eps_p - pl1);
-                co = c0 + tgc * (eps_p - pl1);
-                hd = tgc;
-                if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) break;
-            } else if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && i == M.nsegments - 1 && eps_p > pl2) {
-                fa = F.fric_scale ? M.fric[M.nsegments] * fsc : M.fric[M.nsegments];
-                co = F.coh_scale ? M.coh[M.nsegments] * cs : M.coh[M.nsegments];
-                hd = 0.0;
-                break;
-            }
-        }
-        R.fa = fa;
-        R.co = co;
-        R.hd = hd;
-    }
-    const bool phi_ok = (PLUGIN == SNAC_RHEOLOGY_PLASTIC) ? (R.fa >= 0.0f) : (R.fa > 0.0f);
-    if (s.active && !phi_ok) report(F.sc, SNAC_GPU_ENOTSUP, s.e);
-    R.stc = M.ten_off;
-    R.stc_from_co = false;
-    // constant-angle values as the forward takes them (host-evaluated, same bits)
-    const bool fconst = M.fric_const && R.fa == M.fric0;
-    if (R.fa > 0.0) {
-        double tmp = fconst ? dvz(R.co, M.tan_fric0, M.ztan_fric0) : dv(R.co, tan_fric(M, R.fa));
-        if (tmp < R.stc) {
-            R.stc = tmp;
-            R.stc_from_co = true;
-        }
-    }
-    R.sphi = sin_fric(M, R.fa);
-    R.spsi = sin_dil(M, R.da);
-    R.anphi = fconst ? M.anphi0 : dv(1.0f + R.sphi, 1.0f - R.sphi);
-    R.anpsi = (M.dil_const && R.da == M.dil0) ? M.anpsi0 : dv(1.0f + R.spsi, 1.0f - R.spsi);
     const double a1 = M.lambda + 2.0f * M.mu;
     const double a2 = M.lambda;
-    double st_trial[6];
-#pragma unroll
-    for (int a = 0; a < 6; a++) st_trial[a] = st[a];
     R.yield = false;
     R.tension = false;
     R.alam = 0.0;
     R.inc = 0.0;
-    if (!surely_elastic(st, R.co, R.anphi, fconst ? M.sq_anphi0 : sqrt(R.anphi), R.stc)) {
-        principal_stresses(st, R.sp, R.cn);
-        double sp[3] = {R.sp[0], R.sp[1], R.sp[2]};
-        double fs = sp[0] - sp[2] * R.anphi + 2 * R.co * sqrt(R.anphi);
-        double ft = sp[2] - R.stc;
-        double aP = sqrt(1.0f + R.anphi * R.anphi) + R.anphi;
-        double sP = R.stc * R.anphi - 2 * R.co * sqrt(R.anphi);
-        double hh = sp[2] - R.stc + aP * (sp[0] - sP);
-        R.tension = !(hh < 0.0f);
-        const double ep_before = eps_p;
-        R.yield = mc_return_map(sp, R.cn, st, eps_p, R.co, R.hd, R.anphi, R.anpsi, R.stc, a1, a2) != 0;
-        (void)fs;
-        (void)ft;
-        if (R.yield) {
-            R.alam = R.tension ? dv(ft, a1)
-                               : dv(fs, a1 - a2 * R.anpsi + a1 * R.anphi * R.anpsi - a2 * R.anphi +
-                                            2.0 * sqrt(R.anphi) * R.hd);
-            R.inc = eps_p - ep_before;
-            for (int k = 0; k < 3; k++) R.sq[k] = sp[k];
+    R.co = R.hd = R.fa = R.da = R.fa_b = R.co_b = R.tgf_b = R.tgc_b = R.tgd = 0.0;
+    R.sphi = R.spsi = R.anphi = R.anpsi = R.stc = 0.0;
+    R.dpl = 1.0;
+    R.clamped = false;
+    R.stc_from_co = false;
+    if (MC) {
+        // softening lookup: this tet's own segment (plastic: first match, clamp past the end;
+        // visco-plastic: last match)
+        bool matched = false;
+        for (int i = 0; i < M.nsegments; i++) {
+            const double pl1 = M.plstrain[i];
+            const double pl2 = M.plstrain[i + 1];
+            if (eps_p >= pl1 && eps_p <= pl2) {
+                const double dpl = pl2 - pl1;
+                R.dpl = dpl;
+                double tg[3] = {M.fric[i + 1] - M.fric[i], M.coh[i + 1] - M.coh[i], M.dil[i + 1] - M.dil[i]};
+                dvz_n(tg, dpl, M.zpl[i]);
+                R.tgf_b = tg[0];
+                R.tgc_b = tg[1];
+                R.tgd = tg[2];
+                R.fa_b = M.fric[i] + R.tgf_b * (eps_p - pl1);
+                R.co_b = M.coh[i] + R.tgc_b * (eps_p - pl1);
+                R.da = M.dil[i] + R.tgd * (eps_p - pl1);
+                matched = true;
+                R.clamped = false;
+                if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) break;
+            } else if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && i == M.nsegments - 1 && eps_p > pl2) {
+                R.fa_b = M.fric[M.nsegments];
+                R.co_b = M.coh[M.nsegments];
+                R.da = M.dil[M.nsegments];
+                R.tgf_b = R.tgc_b = R.tgd = 0.0;
+                matched = true;
+                R.clamped = true;
+                break;
+            }
+        }
+        if (s.active && !matched) report(F.sc, SNAC_GPU_ENOTSUP, s.e);  // the carried-over lookup is not differentiated
+        // values as the forward forms them (scales applied to the table entries)
+        {
+            // recompute exactly as the forward does, for identical branch decisions
+            double fa = 0.0, co = 0.0, hd = 0.0;
+            for (int i = 0; i < M.nsegments; i++) {
+                const double pl1 = M.plstrain[i];
+                const double pl2 = M.plstrain[i + 1];
+                double f0 = F.fric_scale ? M.fric[i] * fsc : M.fric[i];
+                double f1 = F.fric_scale ? M.fric[i + 1] * fsc : M.fric[i + 1];
+                double c0 = F.coh_scale ? M.coh[i] * cs : M.coh[i];
+                double c1 = F.coh_scale ? M.coh[i + 1] * cs : M.coh[i + 1];
+                if (eps_p >= pl1 && eps_p <= pl2) {
+                    double tg[2] = {f1 - f0, c1 - c0};
+                    dvz_n(tg, pl2 - pl1, M.zpl[i]);
+                    const double tgf = tg[0], tgc = tg[1];
+                    fa = f0 + tgf * (eps_p - pl1);
+                    co = c0 + tgc * (eps_p - pl1);
+                    hd = tgc;
+                    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) break;
+                } else if (PLUGIN == SNAC_RHEOLOGY_PLASTIC && i == M.nsegments - 1 && eps_p > pl2) {
+                    fa = F.fric_scale ? M.fric[M.nsegments] * fsc : M.fric[M.nsegments];
+                    co = F.coh_scale ? M.coh[M.nsegments] * cs : M.coh[M.nsegments];
+                    hd = 0.0;
+                    break;
+                }
+            }
+            R.fa = fa;
+            R.co = co;
+            R.hd = hd;
+        }
+        const bool phi_ok = (PLUGIN == SNAC_RHEOLOGY_PLASTIC) ? (R.fa >= 0.0f) : (R.fa > 0.0f);
+        if (s.active && !phi_ok) report(F.sc, SNAC_GPU_ENOTSUP, s.e);
+        R.stc = M.ten_off;
+        R.stc_from_co = false;
+        // constant-angle values as the forward takes them (host-evaluated, same bits)
+        const bool fconst = M.fric_const && R.fa == M.fric0;
+        if (R.fa > 0.0) {
+            double tmp = fconst ? dvz(R.co, M.tan_fric0, M.ztan_fric0) : dv(R.co, tan_fric(M, R.fa));
+            if (tmp < R.stc) {
+                R.stc = tmp;
+                R.stc_from_co = true;
+            }
+        }
+        R.sphi = sin_fric(M, R.fa);
+        R.spsi = sin_dil(M, R.da);
+        R.anphi = fconst ? M.anphi0 : dv(1.0f + R.sphi, 1.0f - R.sphi);
+        R.anpsi = (M.dil_const && R.da == M.dil0) ? M.anpsi0 : dv(1.0f + R.spsi, 1.0f - R.spsi);
+        double st_trial[6];
+#pragma unroll
+        for (int a = 0; a < 6; a++) st_trial[a] = st[a];
+        if (!surely_elastic(st, R.co, R.anphi, fconst ? M.sq_anphi0 : sqrt(R.anphi), R.stc)) {
+            principal_stresses(st, R.sp, R.cn);
+            double sp[3] = {R.sp[0], R.sp[1], R.sp[2]};
+            double fs = sp[0] - sp[2] * R.anphi + 2 * R.co * sqrt(R.anphi);
+            double ft = sp[2] - R.stc;
+            double aP = sqrt(1.0f + R.anphi * R.anphi) + R.anphi;
+            double sP = R.stc * R.anphi - 2 * R.co * sqrt(R.anphi);
+            double hh = sp[2] - R.stc + aP * (sp[0] - sP);
+            R.tension = !(hh < 0.0f);
+            const double ep_before = eps_p;
+            R.yield = mc_return_map(sp, R.cn, st, eps_p, R.co, R.hd, R.anphi, R.anpsi, R.stc, a1, a2) != 0;
+            (void)fs;
+            (void)ft;
+            if (R.yield) {
+                R.alam = R.tension ? dv(ft, a1)
+                                   : dv(fs, a1 - a2 * R.anpsi + a1 * R.anphi * R.anpsi - a2 * R.anphi +
+                                                2.0 * sqrt(R.anphi) * R.hd);
+                R.inc = eps_p - ep_before;
+                for (int k = 0; k < 3; k++) R.sq[k] = sp[k];
+            }
         }
     }
     // stress averaging over the hex
@@ -502,7 +552,7 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     // softening chain: anphi(sphi(fa)), anpsi(spsi(da)), stc(co, fa)
     const double deg = degrad();
     double fab = 0.0, dab = 0.0;
-    {
+    if (MC) {
         const double dan = 2.0 / ((1.0 - R.sphi) * (1.0 - R.sphi));
         fab += anphib * dan * cos(R.fa * deg) * deg;
         const double dap = 2.0 / ((1.0 - R.spsi) * (1.0 - R.spsi));
@@ -520,14 +570,64 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     epb += cob * cs * R.tgc_b + fab * fsc * R.tgf_b + dab * R.tgd;
     double vscb = 0.0;
 
-    // elastic trial (plastic) or Maxwell step (visco-plastic)
+    // elastic trial (plastic), elastic update, or Maxwell step (Maxwell, visco-plastic)
     double sprb[6], eb[6];
-    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC) {
+    double Vcb = 0.0, Vob = 0.0;  // Maxwell: adjoints of the current and the old tet volume
+    if (PLUGIN == SNAC_RHEOLOGY_PLASTIC || PLUGIN == SNAC_RHEOLOGY_ELASTIC) {
 #pragma unroll
         for (int a = 0; a < 6; a++) sprb[a] = trialb[a];
         const double lsum = trialb[0] + trialb[1] + trialb[2];
         for (int a = 0; a < 3; a++) eb[a] = 2.0 * M.mu * trialb[a] + M.lambda * lsum;
         for (int a = 3; a < 6; a++) eb[a] = 2.0 * M.mu * trialb[a];
+    } else if (PLUGIN == SNAC_RHEOLOGY_MAXWELL) {
+        if (!R.mx) {
+#pragma unroll
+            for (int a = 0; a < 6; a++) {
+                sprb[a] = trialb[a];
+                eb[a] = 0.0;
+            }
+        } else {
+            const double bulkm = M.lambda + 2.0 * M.mu * K13;
+            const double mu = M.mu;
+            double sdb[3], db[3] = {0, 0, 0};
+            double vic1b = 0.0, vic2b = 0.0;
+            const double osum = trialb[0] + trialb[1] + trialb[2];
+            double trsb = osum * K13, treb = bulkm * osum;
+            for (int a = 0; a < 3; a++) {
+                const double sdo = trialb[a];
+                sdb[a] = sdo * R.vic1 * R.vic2;
+                db[a] += sdo * 2.0 * mu * R.vic2;
+                vic1b += sdo * R.sd[a] * R.vic2;
+                vic2b += sdo * (R.sd[a] * R.vic1 + 2.0 * mu * R.d[a]);
+            }
+            for (int a = 3; a < 6; a++) {
+                sprb[a] = trialb[a] * R.vic1 * R.vic2;
+                eb[a] = trialb[a] * 2.0 * mu * R.vic2;
+                vic1b += trialb[a] * s_pre[a] * R.vic2;
+                vic2b += trialb[a] * (s_pre[a] * R.vic1 + 2.0 * mu * e[a]);
+            }
+            const double tmpb = -vic1b - vic2b * R.vic2 * R.vic2;
+            const double etab = -tmpb * R.tmp / R.eta;
+            if (R.eta_free && R.J_from_sqrt) {
+                const double p = 1.0 / M.srexponent - 1.0;
+                const double Jb = etab * R.eta * p / R.J;
+                const double Qb = Jb * sgnd(R.Q) / (2.0 * sqrt(fabs(R.Q)) * dt);
+                db[0] += Qb * (R.d[2] + R.d[1]);
+                db[1] += Qb * (R.d[2] + R.d[0]);
+                db[2] += Qb * (R.d[1] + R.d[0]);
+                for (int a = 3; a < 6; a++) eb[a] += Qb * (-2.0 * e[a]);
+            }
+            for (int a = 0; a < 3; a++) {
+                eb[a] = db[a];
+                treb -= db[a] * K13;
+                sprb[a] = sdb[a];
+                trsb -= sdb[a] * K13;
+            }
+            for (int a = 0; a < 3; a++) sprb[a] += trsb;
+            // tre = vcur / vold - 1
+            Vcb = treb / R.vold;
+            Vob = -treb * R.vcur / (R.vold * R.vold);
+        }
     } else {
         const double bulkm = M.lambda + 2.0 * M.mu * K13;
         const double mu = M.mu;
@@ -671,6 +771,11 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     // VS = sum over the hex of V; VSb already holds the hex total (both terms
     // were summed over the hex), so every tet's V receives it once
     Vb += VSb;
+    if (PLUGIN == SNAC_RHEOLOGY_MAXWELL && rotate) {
+        // a rotating pass stores its own volume, which the next pass reads as the old one
+        if (s.active && !first_rev) Vb += B.vobar[s.q];
+        Vb += Vcb;
+    }
 
     // geometry: V = |det(c1-c0, c2-c0, c3-c0)| / 6, w_f = ((c_f1 - c_f0) x (c_f2 - c_f0)) / 2
     D3 cb[4] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
@@ -709,10 +814,10 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
             o[k * 6 + 4] = vb[k].y;
             o[k * 6 + 5] = vb[k].z;
         }
-        if (rotate) {
+        // pass 0 leaves the adjoint of the stress the state held
 #pragma unroll
-            for (int a = 0; a < 6; a++) B.sbar[s.q * 6 + a] = sinb[a];
-        }
+        for (int a = 0; a < 6; a++) B.sbar[s.q * 6 + a] = sinb[a];
+        if (PLUGIN == SNAC_RHEOLOGY_MAXWELL) B.vobar[s.q] = rotate ? Vob : 0.0;
         B.epbar[s.q] = epb;
         B.pbar[s.q * 3 + 0] += csb;
         B.pbar[s.q * 3 + 1] += fscb;
@@ -813,9 +918,9 @@ __global__ void k_adj_loss(Mesh m, const double4* pos, const double4* vel, const
 
 // up to 6 array copies in one launch (checkpoint save / restore), 64-bit words
 struct CopyJob {
-    unsigned long long* dst[6];
-    const unsigned long long* src[6];
-    long long n[6];
+    unsigned long long* dst[7];
+    const unsigned long long* src[7];
+    long long n[7];
     int count;
 };
 __global__ void __launch_bounds__(256) k_copy_many(CopyJob J) {

@@ -351,10 +351,19 @@ int op_calc_stresses(snac_gpu* h) {
 int op_loop_nodes(snac_gpu* h) {
     Fields F = fields(h);
     unsigned nb = node_blocks(h->mesh);
+    const bool vo = h->cfg.vonly != 0;
     switch (h->cfg.dt_type) {
-        case SNAC_DT_CONSTANT: k_loop_nodes<SNAC_DT_CONSTANT><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg); break;
-        case SNAC_DT_DYNAMIC: k_loop_nodes<SNAC_DT_DYNAMIC><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg); break;
-        default: k_loop_nodes<SNAC_DT_WAVE><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg); break;
+        case SNAC_DT_CONSTANT:
+            k_loop_nodes<SNAC_DT_CONSTANT, false><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg);
+            break;
+        case SNAC_DT_DYNAMIC:
+            if (vo) k_loop_nodes<SNAC_DT_DYNAMIC, true><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg);
+            else k_loop_nodes<SNAC_DT_DYNAMIC, false><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg);
+            break;
+        default:
+            if (vo) k_loop_nodes<SNAC_DT_WAVE, true><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg);
+            else k_loop_nodes<SNAC_DT_WAVE, false><<<nb, 128, 0, h->stream>>>(h->mesh, F, h->cfg);
+            break;
     }
     h->launches++;
     h->parity ^= 1;  // the new coordinates are current from here on
@@ -879,7 +888,7 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
         dm[p] = to_dev(d->materials[p], d->element_friction_scale != nullptr,
                        d->dp_max_iterations ? d->dp_max_iterations[p] : 1, d->dp_tolerance ? d->dp_tolerance[p] : 1.e-3);
     // the volume alone stands for the gravity and inertial-mass terms (Config::vonly)
-    h->cfg.vonly = !d->element_material && !h->has_density && d->dt_type != SNAC_DT_CONSTANT;
+    h->cfg.vonly = SNAC_VOLUME_ONLY && !d->element_material && !h->has_density && d->dt_type != SNAC_DT_CONSTANT;
     if (d->element_material) {
         std::vector<unsigned char> mt(ne);
         for (long long e = 0; e < ne; e++) {
@@ -1704,6 +1713,7 @@ struct Snap {
     double* stress = nullptr;
     double* eps_p = nullptr;
     DevScalars* sc = nullptr;
+    double* vol = nullptr;  // Maxwell: the tet volumes and old volumes
     bool pending = false;
     long long time_step = 0;
 };
@@ -1712,32 +1722,37 @@ int snap_alloc(snac_gpu* h, Snap& z) {
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
     int rc;
     if ((rc = dalloc(h, &z.pos, nn)) || (rc = dalloc(h, &z.vel, nn)) || (rc = dalloc(h, &z.force, nn)) ||
-        (rc = dalloc(h, &z.stress, nq * 6)) || (rc = dalloc(h, &z.eps_p, nq)) || (rc = dalloc(h, &z.sc, 1)))
+        (rc = dalloc(h, &z.stress, nq * 6)) || (rc = dalloc(h, &z.sc, 1)))
         return rc;
+    // the hooks' own per-tet state: plastic strain (plastic, visco-plastic), volumes (Maxwell)
+    if (h->eps_p && (rc = dalloc(h, &z.eps_p, nq))) return rc;
+    if (h->vol && (rc = dalloc(h, &z.vol, nq * 2))) return rc;
     return 0;
 }
 
 void snap_free(Snap& z) {
-    void* b[] = {z.pos, z.vel, z.force, z.stress, z.eps_p, z.sc};
+    void* b[] = {z.pos, z.vel, z.force, z.stress, z.eps_p, z.sc, z.vol};
     for (void* p : b)
         if (p) cudaFree(p);
     z = Snap();
 }
 
-// one launch copying the six arrays of a state (sizes in 64-bit words)
+// one launch copying the arrays of a state (sizes in 64-bit words)
 int snap_copy(snac_gpu* h, bool save, Snap& z) {
     static_assert(sizeof(DevScalars) % 8 == 0, "scalars are copied as 64-bit words");
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
     using U = unsigned long long;
-    U* hp[6] = {(U*)h->pos[h->parity], (U*)h->vel, (U*)h->force, (U*)h->stress, (U*)h->eps_p, (U*)h->sc};
-    U* zp[6] = {(U*)z.pos, (U*)z.vel, (U*)z.force, (U*)z.stress, (U*)z.eps_p, (U*)z.sc};
-    const long long n[6] = {nn * 4, nn * 4, nn * 4, nq * 6, nq, (long long)(sizeof(DevScalars) / 8)};
+    U* hp[7] = {(U*)h->pos[h->parity], (U*)h->vel, (U*)h->force, (U*)h->stress, (U*)h->eps_p, (U*)h->sc, (U*)h->vol};
+    U* zp[7] = {(U*)z.pos, (U*)z.vel, (U*)z.force, (U*)z.stress, (U*)z.eps_p, (U*)z.sc, (U*)z.vol};
+    const long long n[7] = {nn * 4, nn * 4, nn * 4, nq * 6, nq, (long long)(sizeof(DevScalars) / 8), nq * 2};
     CopyJob J;
-    J.count = 6;
-    for (int a = 0; a < 6; a++) {
-        J.dst[a] = save ? zp[a] : hp[a];
-        J.src[a] = save ? hp[a] : zp[a];
-        J.n[a] = n[a];
+    J.count = 0;
+    for (int a = 0; a < 7; a++) {
+        if (!hp[a] || !zp[a]) continue;  // a per-tet array this hook does not keep
+        J.dst[J.count] = save ? zp[a] : hp[a];
+        J.src[J.count] = save ? hp[a] : zp[a];
+        J.n[J.count] = n[a];
+        J.count++;
     }
     k_copy_many<<<148 * 8, 256, 0, h->stream>>>(J);
     h->launches++;
@@ -1756,12 +1771,12 @@ int snap_copy(snac_gpu* h, bool save, Snap& z) {
 int snap_save(snac_gpu* h, Snap& z) { return snap_copy(h, true, z); }
 int snap_restore(snac_gpu* h, const Snap& z) { return snap_copy(h, false, const_cast<Snap&>(z)); }
 
-AdjState adj_state(const Snap& z) { return AdjState{z.pos, z.vel, z.force, z.stress, z.eps_p}; }
+AdjState adj_state(const Snap& z) { return AdjState{z.pos, z.vel, z.force, z.stress, z.eps_p, z.vol}; }
 
 int adjoint_supported(snac_gpu* h) {
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "adjoint: time step zero must come first");
-    if ((h->constitutive != SNAC_RHEOLOGY_PLASTIC && h->constitutive != SNAC_RHEOLOGY_VISCOPLASTIC) || h->dp)
-        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: only the plastic and the Mohr-Coulomb visco-plastic hooks are differentiated");
+    if (h->dp)
+        return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: the Drucker-Prager return map is not differentiated");
     if (h->cfg.dt_type != SNAC_DT_CONSTANT)
         return set_err(h, SNAC_GPU_ENOTSUP, -1, "adjoint: dtType must be constant (dt may not depend on the state)");
     if (h->has_density || h->cfg.thermal_stress || h->cfg.winkler || h->cfg.traction || topo_on(h->cfg))
@@ -1780,12 +1795,24 @@ int adjoint_supported(snac_gpu* h) {
 
 int adj_tet_launch(snac_gpu* h, const AdjState& S, const AdjBufs& B, int rotate, int first_rev, double dt) {
     const unsigned nb = elem_blocks(h->mesh);
-    if (h->constitutive == SNAC_RHEOLOGY_PLASTIC)
-        k_adj_tet<SNAC_RHEOLOGY_PLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg, S, B, rotate,
-                                                                              first_rev, dt);
-    else
-        k_adj_tet<SNAC_RHEOLOGY_VISCOPLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, fields(h), h->cfg, S, B,
-                                                                                   rotate, first_rev, dt);
+    const Fields F = fields(h);
+    switch (h->constitutive) {
+        case SNAC_RHEOLOGY_ELASTIC:
+            k_adj_tet<SNAC_RHEOLOGY_ELASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
+                                                                                  first_rev, dt);
+            break;
+        case SNAC_RHEOLOGY_PLASTIC:
+            k_adj_tet<SNAC_RHEOLOGY_PLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
+                                                                                  first_rev, dt);
+            break;
+        case SNAC_RHEOLOGY_MAXWELL:
+            k_adj_tet<SNAC_RHEOLOGY_MAXWELL><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
+                                                                                  first_rev, dt);
+            break;
+        default:
+            k_adj_tet<SNAC_RHEOLOGY_VISCOPLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B,
+                                                                                       rotate, first_rev, dt);
+    }
     h->launches++;
     return launch_check_named(h, "k_adj_tet");
 }
@@ -1830,7 +1857,7 @@ struct AdjWork {
     double* terms = nullptr;
     double* grads = nullptr;  // [3][ne]
     void release() {
-        void* b[] = {B.xbar, B.vbar, B.fbar, B.cbuf, B.sbar, B.epbar, B.pbar, terms, grads};
+        void* b[] = {B.xbar, B.vbar, B.fbar, B.cbuf, B.sbar, B.epbar, B.pbar, B.vobar, terms, grads};
         for (void* p : b)
             if (p) cudaFree(p);
         *this = AdjWork();
@@ -1844,6 +1871,7 @@ int adj_work_alloc(snac_gpu* h, AdjWork& w) {
         (rc = dalloc(h, &w.B.cbuf, nq * 24)) || (rc = dalloc(h, &w.B.sbar, nq * 6)) || (rc = dalloc(h, &w.B.epbar, nq)) ||
         (rc = dalloc(h, &w.B.pbar, nq * 3)) || (rc = dalloc(h, &w.terms, nt)) || (rc = dalloc(h, &w.grads, 3 * h->mesh.ne)))
         return rc;
+    if (h->constitutive == SNAC_RHEOLOGY_MAXWELL && (rc = dalloc(h, &w.B.vobar, nq))) return rc;
     return 0;
 }
 
@@ -1878,7 +1906,16 @@ int snac_gpu_misfit(snac_gpu* h, const snac_adjoint_desc* a, double* loss) {
 
 int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, double* grad_cohesion,
                      double* grad_friction, double* grad_viscosity, snac_adjoint_stats* stats) {
-    if (!h || !a || !loss || !a->target_vy || !a->target_y || a->nsteps < 1) return SNAC_GPU_EINVAL;
+    snac_adjoint_grads g{};
+    g.cohesion = grad_cohesion;
+    g.friction = grad_friction;
+    g.viscosity = grad_viscosity;
+    return snac_gpu_adjoint_grads(h, a, loss, &g, stats);
+}
+
+int snac_gpu_adjoint_grads(snac_gpu* h, const snac_adjoint_desc* a, double* loss, const snac_adjoint_grads* gr,
+                           snac_adjoint_stats* stats) {
+    if (!h || !a || !loss || !gr || !a->target_vy || !a->target_y || a->nsteps < 1) return SNAC_GPU_EINVAL;
     int rc = adjoint_supported(h);
     if (rc) return rc;
     const int N = a->nsteps;
@@ -1937,6 +1974,7 @@ int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, doub
     cudaMemsetAsync(w.B.sbar, 0, nq * 6 * sizeof(double), h->stream);
     cudaMemsetAsync(w.B.epbar, 0, nq * sizeof(double), h->stream);
     cudaMemsetAsync(w.B.pbar, 0, nq * 3 * sizeof(double), h->stream);
+    if (w.B.vobar) cudaMemsetAsync(w.B.vobar, 0, nq * sizeof(double), h->stream);
     cudaEventRecord(ev[2], h->stream);
     for (int j = ncp - 1; j >= 0; j--) {
         const int a0 = j * K, b0 = std::min(a0 + K, N);
@@ -1963,12 +2001,22 @@ int snac_gpu_adjoint(snac_gpu* h, const snac_adjoint_desc* a, double* loss, doub
     ACK(launch_check_named(h, "k_adj_reduce"));
     cudaEventRecord(ev[3], h->stream);
     ACK(adj_status(h));
-    if (grad_cohesion)
-        cudaMemcpyAsync(grad_cohesion, w.grads, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    if (grad_friction)
-        cudaMemcpyAsync(grad_friction, w.grads + ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
-    if (grad_viscosity)
-        cudaMemcpyAsync(grad_viscosity, w.grads + 2 * ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (gr->cohesion) cudaMemcpyAsync(gr->cohesion, w.grads, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (gr->friction)
+        cudaMemcpyAsync(gr->friction, w.grads + ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (gr->viscosity)
+        cudaMemcpyAsync(gr->viscosity, w.grads + 2 * ne, ne * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    // the adjoints the sweep left for the entry state (pass 0 wrote sbar and epbar,
+    // the last node gather xbar and vbar)
+    if (gr->coordinates) ACK(node_out(h, w.B.xbar, gr->coordinates, 0));
+    if (gr->velocity) ACK(node_out(h, w.B.vbar, gr->velocity, 0));
+    if (gr->stress) cudaMemcpyAsync(gr->stress, w.B.sbar, nq * 6 * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+    if (gr->plastic_strain) {
+        if (h->eps_p)
+            cudaMemcpyAsync(gr->plastic_strain, w.B.epbar, nq * sizeof(double), cudaMemcpyDeviceToHost, h->stream);
+        else
+            memset(gr->plastic_strain, 0, nq * sizeof(double));
+    }
     // leave the model at the forward's final state
     ACK(snap_restore(h, fin));
     if (cudaStreamSynchronize(h->stream) != cudaSuccess) ACK(set_err(h, SNAC_GPU_ECUDA, -1, "adjoint: sync"));

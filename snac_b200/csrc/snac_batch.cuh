@@ -180,10 +180,17 @@ __global__ void __launch_bounds__(256) kb_nodes(const ModelDesc* __restrict__ D,
         load_desc(md, D + t.x);
         __syncthreads();
         if (OP == BOP_LOOP_NODES) {
+            const bool vo = md.cfg.vonly != 0;
             switch (md.cfg.dt_type) {
-                case SNAC_DT_CONSTANT: k_loop_nodes_body<SNAC_DT_CONSTANT>(md.m, md.F, md.cfg, t.y); break;
-                case SNAC_DT_DYNAMIC: k_loop_nodes_body<SNAC_DT_DYNAMIC>(md.m, md.F, md.cfg, t.y); break;
-                default: k_loop_nodes_body<SNAC_DT_WAVE>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_DT_CONSTANT: k_loop_nodes_body<SNAC_DT_CONSTANT, false>(md.m, md.F, md.cfg, t.y); break;
+                case SNAC_DT_DYNAMIC:
+                    if (vo) k_loop_nodes_body<SNAC_DT_DYNAMIC, true>(md.m, md.F, md.cfg, t.y);
+                    else k_loop_nodes_body<SNAC_DT_DYNAMIC, false>(md.m, md.F, md.cfg, t.y);
+                    break;
+                default:
+                    if (vo) k_loop_nodes_body<SNAC_DT_WAVE, true>(md.m, md.F, md.cfg, t.y);
+                    else k_loop_nodes_body<SNAC_DT_WAVE, false>(md.m, md.F, md.cfg, t.y);
+                    break;
             }
         } else if (OP == BOP_HEAT_NODES) {
             k_heat_nodes_body(md.m, md.F, md.cfg, t.y);

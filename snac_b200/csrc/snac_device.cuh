@@ -316,7 +316,7 @@ __device__ __forceinline__ void tet_face(const V3& c1, const V3& c2, const V3& c
     double b = z2 * x3 - x2 * z3;
     double c = x2 * y3 - y2 * x3;
     double s = sqrt(a * a + b * b + c * c);
-    area = s / 2.0;
+    area = s * 0.5;  // a product with 2^-k rounds exactly as the quotient by 2^k
     double t[3] = {a, b, c};
     dvz_n(t, s, recip(s));
     n = {t[0], t[1], t[2]};

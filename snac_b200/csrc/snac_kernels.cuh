@@ -73,6 +73,9 @@ struct Fields {
     DevScalars* sc;
 };
 
+#ifndef SNAC_VOLUME_ONLY
+#define SNAC_VOLUME_ONLY 1
+#endif
 struct Config {
     int dt_type, constitutive, temperature, thermal_stress, has_density, time_step_zero;
     double gravity, demf;
@@ -86,6 +89,7 @@ struct Config {
     // inertial-mass terms are the same multiples of its volume for every tet,
     // so the element kernels store the volume alone (in the fgrav row) and
     // the node gather forms both terms from it with the same operations
+    // (SNAC_VOLUME_ONLY = 0 turns this off, for measurement)
     int vonly;
     // phase 0, the only phase of a model without a per-element phase array:
     // the element kernels of such models read it from their parameters
@@ -614,7 +618,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
         if (ONE && cfg.vonly) {
             F.fgrav[qt] = gf.V;
         } else {
-            F.fgrav[qt] = cfg.gravity * rho * gf.V / 8.0f;
+            F.fgrav[qt] = cfg.gravity * rho * gf.V * 0.125;  // x * 2^-3 rounds as x / 8
         }
         if (ONE && cfg.vonly) {
             // both terms formed by the node gather
@@ -867,7 +871,7 @@ __device__ __forceinline__ double hex_min_length_scale(const Mesh& m, const Fiel
                 double sq = a * a + b * b + cc * cc;
                 if (sq > smax) smax = sq;
             }
-            double A = sqrt(smax) / 2.0;
+            double A = sqrt(smax) * 0.5;  // rounds as / 2
             if (A) {
                 double l = fabs(dv(V, A));
                 if (ls > l) ls = l;
@@ -998,7 +1002,9 @@ __device__ __noinline__ V3 traction_force(const double4* pos, int nx, int ny, in
     return V3{fx, fy, fz};
 }
 
-template <int DTTYPE>
+// VONLY: cfg.vonly (a template argument, so that the gather loop of each
+// instance is straight-line code)
+template <int DTTYPE, bool VONLY>
 __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     long long n = (long long)lb * blockDim.x + threadIdx.x;
     bool active = n < m.nn;
@@ -1010,8 +1016,9 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
         double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
         // with cfg.vonly the fgrav row holds the tet volume: (g rho) V / 8 and
         // (1/4 rho_i) V are formed here exactly as the element kernel forms them
-        const double gr = cfg.gravity * cfg.m0.density;
-        const double f4r = (1.0f / 4.0f) * (DTTYPE == SNAC_DT_DYNAMIC ? F.sc->inertial_density0 : cfg.m0.density);
+        const double gr = VONLY ? cfg.gravity * cfg.m0.density : 0.0;
+        const double f4r =
+            VONLY ? (1.0f / 4.0f) * (DTTYPE == SNAC_DT_DYNAMIC ? F.sc->inertial_density0 : cfg.m0.density) : 0.0;
         // Snac_Force: the 8 incident hexes in HexaEL.c:529-573 order, 5 tets each
         // (NodeToTetra/NodeToSurface); absent hexes are skipped (Force.c:92)
 #pragma unroll
@@ -1025,13 +1032,13 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 const int f = node_face(ne, idx);
                 const long long R = m.ner;
                 const double* o = F.fterm + (t * 12 + f * 3) * R + e;
-                if (DTTYPE != SNAC_DT_CONSTANT && cfg.vonly) {
+                if (DTTYPE != SNAC_DT_CONSTANT && VONLY) {
                     const double V = F.fgrav[t * R + e];
                     imass += f4r * V;
                     fx += o[0];
                     fy += o[R];
                     fz += o[2 * R];
-                    fy -= gr * V / 8.0f;
+                    fy -= gr * V * 0.125;
                 } else {
                     imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[(t * 4 + f) * R + e] : F.fmass[t * R + e];
                     fx += o[0];
@@ -1086,9 +1093,12 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
         atomicMax(&F.sc->vmax_bits, (unsigned long long)__double_as_longlong(vcand));
 }
 
-template <int DTTYPE>
-__global__ void __launch_bounds__(128) k_loop_nodes(Mesh m, Fields F, Config cfg) {
-    k_loop_nodes_body<DTTYPE>(m, F, cfg, blockIdx.x);
+#ifndef SNAC_NODE_MINB
+#define SNAC_NODE_MINB 8  // resident 128-thread blocks per SM asked of the node gather (64 registers; measured best)
+#endif
+template <int DTTYPE, bool VONLY>
+__global__ void __launch_bounds__(128, SNAC_NODE_MINB) k_loop_nodes(Mesh m, Fields F, Config cfg) {
+    k_loop_nodes_body<DTTYPE, VONLY>(m, F, cfg, blockIdx.x);
 }
 
 // ======================================================================================
@@ -1172,7 +1182,7 @@ __device__ __forceinline__ void heat_flux_tet(const Mesh& m, const Fields& F, co
         // tetra density is set from TimeStepZero on, so the reference's
         // "density == 0" fallback (Heat.c:120-125) is never taken
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
-        h[4 * R] = M.heat_capacity * ((rho)*g.V) / 8.0f;
+        h[4 * R] = M.heat_capacity * ((rho)*g.V) * 0.125;  // rounds as / 8
         if (cfg.thermal_stress) h[5 * R] = tsr;
         // Heat.c:127-135, once per element; with one phase every element
         // gives the same value, so only element 0 (the first the reference

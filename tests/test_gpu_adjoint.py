@@ -179,3 +179,118 @@ def test_unsupported_physics_is_refused():
         with pytest.raises(SnacError) as e:
             adjoint(ctx, 3, tv, tv)
         assert e.value.code == -9
+
+
+# ---- gradients with respect to the entry state, all four hooks --------------------------
+#
+# FLAC damping multiplies the force by 1 - demf sgn(v) sgn(F): the loss jumps
+# wherever a perturbation moves a velocity or force component across zero at
+# some step, and central differences across a jump measure jump / 2h, not the
+# derivative (the adjoint is exact for the discretisation either way).  The
+# state gradients are therefore checked with the damping off (demf = 0),
+# where the loss is smooth away from the return map's branch switches, from
+# an entry state whose velocities got a seeded random field after time step
+# zero (no exact symmetry is left).
+
+STATE_FIELDS = {"coordinates": ("coord", 10.0, 1.0e-6), "velocity": ("velocity", 1.0e-9, 1.0e-6),
+                "stress": ("stress", 1.0e5, 1.0e-5), "plastic_strain": ("plastic_strain", 1.0e-4, 1.0e-6)}
+
+
+def state_cfg(plugin):
+    """The adjoint workload through one of the four hooks; the elastic and
+    Maxwell hooks take no per-element scales."""
+    base = "SnacPlastic" if plugin == "SnacPlastic" else "SnacViscoPlastic"
+    cfg = make_cfg(*base_params(), base)
+    cfg.demf = 0.0
+    if plugin in ("SnacElastic", "SnacMaxwell"):
+        cfg.plugin = plugin
+        cfg.element_cohesion_scale = cfg.element_friction_scale = cfg.element_visc_scale = None
+    return cfg
+
+
+WARM = 6  # steps before the entry state, so that yielded tets carry plastic strain
+FIELDS = ["coord", "velocity", "stress", "plastic_strain"]
+
+
+def enter(ctx, field=None, delta=None):
+    """Time step zero, a seeded velocity field, WARM steps, then the state
+    uploaded again (with `delta` added to one field)."""
+    ctx.time_step_zero()
+    s = ctx.state()
+    rng = np.random.default_rng(17)
+    s.velocity += 0.05 * W.CM_PER_YR * rng.standard_normal(s.velocity.shape)
+    ctx.set_state(s, ["velocity"])
+    ctx.step(WARM)
+    s = ctx.state()
+    if field is not None:
+        a = getattr(s, field)
+        a += delta.reshape(a.shape)
+    ctx.set_state(s, FIELDS)
+    return s
+
+
+def state_targets(cfg):
+    with SnacContext(cfg) as ctx:
+        enter(ctx)
+        ctx.step(NSTEPS)
+        v, y = top_surface(cfg, ctx.state())
+    rng = np.random.default_rng(11)
+    return v * (1.0 + 0.2 * rng.uniform(-1, 1, v.size)), y + 5.0 * rng.uniform(-1, 1, y.size)
+
+
+def loss_from_perturbed(cfg, field, delta, tv, ty, wv, wh):
+    with SnacContext(cfg) as ctx:
+        enter(ctx, field, delta)
+        ctx.step(NSTEPS)
+        return misfit(ctx, tv, ty, wv, wh)
+
+
+@pytest.mark.parametrize("plugin", ["SnacElastic", "SnacMaxwell", "SnacPlastic", "SnacViscoPlastic"])
+def test_state_gradients_match_finite_differences(plugin):
+    cfg = state_cfg(plugin)
+    tv, ty = state_targets(cfg)
+    wv, wh = weights(tv, ty)
+    with SnacContext(cfg) as ctx:
+        s0 = enter(ctx)
+        r = adjoint(ctx, NSTEPS, tv, ty, wv, wh, checkpoint_every=5, state=True)
+        end = ctx.state()
+    eps0 = s0.plastic_strain.reshape(-1)
+    v0 = s0.velocity.reshape(-1)
+    if plugin in ("SnacElastic", "SnacMaxwell"):
+        for k in ("cohesion", "friction", "viscosity", "plastic_strain"):
+            assert not np.any(r.grad[k]), k  # no scale or plastic strain enters these hooks
+    else:
+        assert np.count_nonzero(end.plastic_strain) > 0  # the shear branch was taken
+    if plugin in ("SnacMaxwell", "SnacViscoPlastic"):
+        assert np.any(end.viscosity > 1.0e19) and np.any(end.viscosity < 1.0e24)
+    rng = np.random.default_rng(13)
+    fields = [k for k in STATE_FIELDS if k != "plastic_strain" or plugin in ("SnacPlastic", "SnacViscoPlastic")]
+    for k in fields:
+        name, scale, h = STATE_FIELDS[k]
+        g = r.grad[k].reshape(-1)
+        assert np.all(np.isfinite(g)) and np.any(g != 0.0), k
+        d = scale * rng.standard_normal(g.size)
+        if k == "plastic_strain":
+            assert np.count_nonzero(eps0) > 0
+            d = np.where(eps0 > 0.0, d * np.minimum(1.0, eps0 / scale), 0.0)  # stays on the softening table
+        if k == "velocity":
+            d = np.where(np.abs(v0) > 1.0e3 * h * scale, d, 0.0)  # no component changes sign
+        ad = float(np.dot(g, d))
+        fd = (loss_from_perturbed(cfg, name, h * d, tv, ty, wv, wh) -
+              loss_from_perturbed(cfg, name, -h * d, tv, ty, wv, wh)) / (2.0 * h)
+        rel = abs(ad - fd) / max(abs(fd), 1e-300)
+        print(f"{plugin} {k}: adjoint {ad:.12e}  fd {fd:.12e}  rel {rel:.2e}  (h {h:g})")
+        assert rel <= 1.0e-5, (k, ad, fd)
+
+
+def test_state_gradient_checkpointing_is_exact():
+    cfg = state_cfg("SnacMaxwell")
+    tv, ty = state_targets(cfg)
+    res = []
+    for k in (1, 5, NSTEPS):
+        with SnacContext(cfg) as ctx:
+            enter(ctx)
+            res.append(adjoint(ctx, NSTEPS, tv, ty, checkpoint_every=k, state=True))
+    for r in res[1:]:
+        for k in ("coordinates", "velocity", "stress"):
+            assert np.array_equal(r.grad[k], res[0].grad[k]), k

@@ -89,3 +89,18 @@ def test_threaded_reference_is_bitwise_equal_to_serial(case):
     for f in FIELDS:
         assert np.array_equal(getattr(sa, f), getattr(sb, f)), (case, f)
     assert a.scalars().dt == b.scalars().dt
+
+
+@pytest.mark.parametrize("make", [S.elastic_small, S.viscoplastic_small])
+def test_verbatim_bc_search_gives_the_same_bits(make):
+    """The boundary conditions applied by StGermain's linear index search
+    (the reference's cost) and by the per-node mask give the same state."""
+    cfg = make(6, 4, 6)
+    a, b = pyoracle.Checker(cfg, "reference"), pyoracle.Checker(cfg, "reference")
+    b.set_verbatim_bc(True)
+    for c in (a, b):
+        assert c.time_step_zero() == 0
+        assert c.step(25) == 0
+    sa, sb = a.state(), b.state()
+    for f in ("coord", "velocity", "stress", "plastic_strain", "temperature"):
+        assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
