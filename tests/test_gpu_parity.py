@@ -67,6 +67,23 @@ def test_plastic_case_yields_on_gpu():
 # the device viscosity differs from the host libm pow * exp in the last bits; through the
 # yield branch the difference stays far below the plastic bar (1e-6), and
 # without plasticity (Maxwell) below the elastic bar (1e-9).
+@pytest.mark.parametrize("shape", [(1, 1, 1), (1, 3, 1), (2, 1, 5), (3, 2, 1), (7, 1, 1), (5, 3, 7), (13, 5, 11)])
+@pytest.mark.parametrize("make", [S.elastic_small, S.plastic_small])
+def test_ragged_meshes_bitwise_equal_to_the_reference(make, shape):
+    """Meshes one element wide in any direction and hex counts that leave the
+    last warp (three hexes) and the last block partly empty, against the
+    reference's own sources."""
+    cfg = make(*shape)
+    g = SnacContext(cfg)
+    c = Checker(cfg, "reference")
+    g.time_step_zero()
+    c.time_step_zero()
+    g.step(30)
+    c.step(30)
+    assert_bitwise(g, c)
+    g.close()
+
+
 @pytest.mark.parametrize("case,tol", [("viscoplastic", 1e-6), ("maxwell", 1e-9), ("density", 1e-6),
                                       ("drucker_prager", 1e-6), ("drucker_prager_iterated", 1e-6)])
 def test_device_transcendentals_within_tolerance(case, tol):
