@@ -179,6 +179,16 @@ def test_unsupported_physics_is_refused():
         with pytest.raises(SnacError) as e:
             adjoint(ctx, 3, tv, tv)
         assert e.value.code == -9
+    # the Drucker-Prager return map (an iteration count that switches with a
+    # tolerance test) is not differentiated
+    from tests import scenarios as S
+    dp = S.constant_dt(S.drucker_prager_small(5, 3, 4), 1.0e8)
+    tv = np.zeros((dp.nx + 1) * (dp.nz + 1))
+    with SnacContext(dp) as ctx:
+        ctx.time_step_zero()
+        with pytest.raises(SnacError) as e:
+            adjoint(ctx, 3, tv, tv)
+        assert e.value.code == -9
 
 
 # ---- gradients with respect to the entry state, all four hooks --------------------------
