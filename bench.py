@@ -16,7 +16,8 @@ advances its own replica of the model (the single-model path is not
 sharded): value = all ranks' element-steps / slowest rank's time.
 
 At N = 1 the default line also carries the metric's other forms under
-"forms": the largest plain model (c3, 128 x 64(y) x 128 hex), the batched
+"forms": the small and the largest plain models (c1, 16 x 8(y) x 16 hex;
+c3, 128 x 64(y) x 128 hex), the batched
 ensemble of 256 models against the same models one launch each, and the
 adjoint's cost in forward runs with its finite-difference agreement.
 
@@ -782,10 +783,10 @@ def run_adjoint(args, ws, rank, local):
 
 def run_forms(args, ws, rank, local) -> dict:
     """The metric's other forms beside the headline plain model, each on the
-    same GPU in the same run: the largest plain model (c3), the batched
-    ensemble against the same models one launch each, and the adjoint's cost
-    in forward runs with its finite-difference agreement.  A form that fails
-    reports its error instead of ending the run."""
+    same GPU in the same run: the small and the largest plain models (c1,
+    c3), the batched ensemble against the same models one launch each, and
+    the adjoint's cost in forward runs with its finite-difference agreement.
+    A form that fails reports its error instead of ending the run."""
     import torch
     forms = {}
 
@@ -797,8 +798,8 @@ def run_forms(args, ws, rank, local) -> dict:
         torch.cuda.synchronize()
         torch.cuda.empty_cache()
 
-    def plain_c3():
-        ln = run_plain(args, ws, rank, local, "c3", with_e2e=True, with_cpu=False)
+    def plain(workload):
+        ln = run_plain(args, ws, rank, local, workload, with_e2e=True, with_cpu=False)
         return {k: ln[k] for k in ("value", "unit", "ms_per_step", "config", "roofline", "kernels_ms", "gpu_launches",
                                    "clocks", "e2e")}
 
@@ -816,7 +817,8 @@ def run_forms(args, ws, rank, local) -> dict:
         out["cost_in_forward_runs"] = ln["adjoint"]["cost_in_forward_runs"]
         return out
 
-    guarded("plain_c3", plain_c3)
+    guarded("plain_c1", lambda: plain("c1"))
+    guarded("plain_c3", lambda: plain("c3"))
     guarded("batched", batched)
     guarded("adjoint", adjoint_form)
     return forms

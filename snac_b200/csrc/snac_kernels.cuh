@@ -1213,8 +1213,11 @@ __device__ __forceinline__ void k_heat_flux_body(const Mesh& m, const Fields& F,
     heat_flux_tet<ONE>(m, F, cfg, s, T, T0, g);
 }
 
+#ifndef SNAC_HEAT_MINB
+#define SNAC_HEAT_MINB 6  // resident blocks per SM asked of the heat-flux kernel (80 registers; measured best)
+#endif
 template <bool ONE>
-__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_heat_flux(Mesh m, Fields F, Config cfg,
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_HEAT_MINB) k_heat_flux(Mesh m, Fields F, Config cfg,
                                                                            int count_step) {
     if (count_step && blockIdx.x == 0 && threadIdx.x == 0) {  // the step's first kernel: timeStep++, currentTime += dt
         F.sc->time_step += 1;
