@@ -409,8 +409,8 @@ int op_fused(snac_gpu* h) {
 }
 
 int op_min_length_scale_sync(snac_gpu* h) {
-    k_min_length_scale_sync<<<(unsigned)((h->mesh.ne + 127) / 128), 128, 0, h->stream>>>(h->mesh, fields(h), h->cfg,
-                                                                                       h->wave_speed);
+    k_min_length_scale_sync<<<(unsigned)((h->mesh.ne + MINLS_THREADS - 1) / MINLS_THREADS), MINLS_THREADS, 0,
+                              h->stream>>>(h->mesh, fields(h), h->cfg, h->wave_speed);
     h->launches++;
     return launch_check_named(h, "k_min_length_scale_sync");
 }

@@ -1299,17 +1299,21 @@ __device__ __forceinline__ void sync_one(const Config& cfg, DevScalars* sc, doub
 // The minimum length scale of the new coordinates and Sync in one launch:
 // the last block to finish (counted in DevScalars, reset by that block) runs
 // Sync on the completed reductions.
-__global__ void __launch_bounds__(128) k_min_length_scale_sync(Mesh m, Fields F, Config cfg, double wave_speed) {
+constexpr int MINLS_THREADS = 128;  // one thread per hex
+__global__ void __launch_bounds__(MINLS_THREADS) k_min_length_scale_sync(Mesh m, Fields F, Config cfg,
+                                                                         double wave_speed) {
     double ls = hex_min_length_scale(m, F, blockIdx.x);
     for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
     // the block's minimum in one atomic (fewer atomics on the one address),
     // fenced so that it is visible device-wide before the block is counted
-    __shared__ double wmin[4];
+    __shared__ double wmin[MINLS_THREADS / 32];
     __shared__ bool last;
     if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = ls;
     __syncthreads();
     if (threadIdx.x == 0) {
-        const double b = fmin(fmin(wmin[0], wmin[1]), fmin(wmin[2], wmin[3]));
+        double b = wmin[0];
+#pragma unroll
+        for (int w = 1; w < MINLS_THREADS / 32; w++) b = fmin(b, wmin[w]);
         atomicMin(&F.sc->minls_bits, (unsigned long long)__double_as_longlong(b));
         __threadfence();
         last = atomicAdd(&F.sc->blocks_done, 1u) == gridDim.x - 1;
