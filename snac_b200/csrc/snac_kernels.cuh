@@ -56,7 +56,7 @@ struct Fields {
     double* vol;             // [ne*10][2] volume, old volume (Maxwell)
     double* hflux;           // rows (t, 0..5): face energy terms (q.n A/6), Cp rho V/8, thermal stress
     double* tpre;            // [nn] temperature before the BCs (temperature + density)
-    double* fterm;           // stress.n.A/6 of each face (Force.c:154-165), laid out by fterm_at()
+    double* fterm;           // rows (t, face, xyz): stress.n.A/6 of each face (Force.c:154-165)
     double* fgrav;           // rows (t): g rho V / 8 (Force.c:173)
     double* fmass;           // rows (t, face) (constant dt) or (t): inertial-mass term (Force.c:107-140)
     const uchar4* bc;        // per node: velocity-VC index of x, y, z and temperature-VC index (255 = free)
@@ -72,12 +72,6 @@ struct Fields {
     const double* visc_scale;        // [ne] or NULL
     DevScalars* sc;
 };
-
-// The per-face force terms: rows (t, face, component) of ner doubles each
-// (a warp's store or gather load touches one row at consecutive elements)
-__device__ __forceinline__ long long fterm_at(int t, int f, int c, long long e, long long R) {
-    return (long long)(t * 12 + f * 3 + c) * R + e;
-}
 
 #ifndef SNAC_VOLUME_ONLY
 #define SNAC_VOLUME_ONLY 1
@@ -607,6 +601,7 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
     if (s.active) {
         const double rho = cfg.has_density ? F.density[s.q] : M.density;
         const long long R = m.ner;
+        double* o = F.fterm + (long long)(s.t * 12) * R + s.e;  // rows (t, face, component)
 #pragma unroll
         for (int f = 0; f < 4; f++) {
             const V3& nr = gf.n[f];
@@ -614,9 +609,9 @@ __device__ __forceinline__ void stress_update(const Mesh& m, const Fields& F, co
             double t[3] = {(st[0] * nr.x + st[3] * nr.y + st[4] * nr.z) * A, (st[3] * nr.x + st[1] * nr.y + st[5] * nr.z) * A,
                            (st[4] * nr.x + st[5] * nr.y + st[2] * nr.z) * A};
             dvk_n(t, 6.0, Z6);
-            F.fterm[fterm_at(s.t, f, 0, s.e, R)] = t[0];
-            F.fterm[fterm_at(s.t, f, 1, s.e, R)] = t[1];
-            F.fterm[fterm_at(s.t, f, 2, s.e, R)] = t[2];
+            o[(f * 3 + 0) * R] = t[0];
+            o[(f * 3 + 1) * R] = t[1];
+            o[(f * 3 + 2) * R] = t[2];
         }
         const long long qt = (long long)s.t * R + s.e;  // row t
         const double factor4 = 1.0f / 4.0f;
@@ -1036,21 +1031,19 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 const int t = node_tet(ne, idx);
                 const int f = node_face(ne, idx);
                 const long long R = m.ner;
-                const double* o0 = F.fterm + fterm_at(t, f, 0, e, R);
-                const double* o1 = F.fterm + fterm_at(t, f, 1, e, R);
-                const double* o2 = F.fterm + fterm_at(t, f, 2, e, R);
+                const double* o = F.fterm + (t * 12 + f * 3) * R + e;
                 if (DTTYPE != SNAC_DT_CONSTANT && VONLY) {
                     const double V = F.fgrav[t * R + e];
                     imass += f4r * V;
-                    fx += *o0;
-                    fy += *o1;
-                    fz += *o2;
+                    fx += o[0];
+                    fy += o[R];
+                    fz += o[2 * R];
                     fy -= gr * V * 0.125;
                 } else {
                     imass += (DTTYPE == SNAC_DT_CONSTANT) ? F.fmass[(t * 4 + f) * R + e] : F.fmass[t * R + e];
-                    fx += *o0;
-                    fy += *o1;
-                    fz += *o2;
+                    fx += o[0];
+                    fy += o[R];
+                    fz += o[2 * R];
                     fy -= F.fgrav[t * R + e];
                 }
             }
