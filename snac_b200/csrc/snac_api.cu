@@ -98,14 +98,18 @@ struct snac_gpu {
     int parity = 0;
     long long time_step = 0;
     bool zero_done = false;
-    cudaGraphExec_t graph[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};  // [fused][parity]
+    cudaGraphExec_t graph[2][2][2] = {};  // [heat flux formed][fused][parity]
     bool pending = false;  // the element update of the last step is deferred into the next kernel
+    // temperature runs: the heat flux of the next step was formed at the end
+    // of the last graph step (k_heat_flux_min_length_scale); anything
+    // else that runs or changes the state clears it
+    bool hflux_ready = false;
     // kernel-by-kernel timing (snac_gpu_profile_step)
     snac_kernel_time* prof = nullptr;
     int prof_n = 0, prof_max = 0;
     cudaEvent_t prof_ev[64];
     long long launches = 0;
-    int steps_kernels[2] = {0, 0};
+    int steps_kernels[2][2] = {};  // kernels of a step graph [heat flux formed][fused]
     char err[512] = {0};
     long long err_index = -1;
 };
@@ -324,10 +328,11 @@ int op_fused_stress(snac_gpu* h) {
     return launch_check_named(h, "k_fused_stress");
 }
 
-int op_energy_nodes(snac_gpu* h) {
+int op_energy_nodes(snac_gpu* h, int count_step = 0) {
     if (!h->temperature) return 0;
-    k_heat_nodes<<<node_blocks(h->mesh), 128, 0, h->stream>>>(h->mesh, fields(h), h->cfg);
+    k_heat_nodes<<<node_blocks(h->mesh), 128, 0, h->stream>>>(h->mesh, fields(h), h->cfg, count_step);
     h->launches++;
+    if (count_step) h->time_step++;
     return launch_check_named(h, "k_heat_nodes");
 }
 
@@ -409,6 +414,20 @@ int op_fused(snac_gpu* h) {
 }
 
 int op_min_length_scale_sync(snac_gpu* h) {
+    if (h->temperature) {  // with the heat flux of the next step
+        if (h->mat)
+            k_heat_flux_min_length_scale<false><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(
+                h->mesh, fields(h), h->cfg);
+        else
+            k_heat_flux_min_length_scale<true><<<elem_blocks(h->mesh), ELEM_WARPS * 32, 0, h->stream>>>(
+                h->mesh, fields(h), h->cfg);
+        h->launches++;
+        int rc = launch_check_named(h, "k_heat_flux_min_length_scale");
+        if (rc) return rc;
+        k_slots_sync<<<1, 32, 0, h->stream>>>(h->cfg, h->sc, h->wave_speed);
+        h->launches++;
+        return launch_check_named(h, "k_slots_sync");
+    }
     k_min_length_scale_sync<<<(unsigned)((h->mesh.ne + MINLS_THREADS - 1) / MINLS_THREADS), MINLS_THREADS, 0,
                               h->stream>>>(h->mesh, fields(h), h->cfg, h->wave_speed);
     h->launches++;
@@ -439,24 +458,33 @@ int op_begin(snac_gpu* h) {
 // One step as a chain of launches.  Element update of step n and the first
 // element kernel of step n+1 share one launch when the previous step's
 // update is pending (fused), otherwise the step starts from scratch.
+// Temperature runs form the next step's heat flux in the step's last kernel;
+// a step whose heat flux is not ready (the first graph step, or one after a
+// state change) forms its own first.
 int record_step(snac_gpu* h, bool fused) {
     int rc;
+    const bool ready = h->temperature && h->hflux_ready;
     if (fused && h->temperature) {
-        // heat flux (opens the step), temperature update, then the pending
-        // element update fused with the stress update
-        if ((rc = op_energy_elements(h, 1))) return rc;
-        if ((rc = op_energy_nodes(h))) return rc;
+        // heat flux (opens the step; or the temperature update opens it when
+        // the flux is ready), temperature update, then the pending element
+        // update fused with the stress update
+        if (ready) {
+            if ((rc = op_energy_nodes(h, 1))) return rc;
+        } else {
+            if ((rc = op_energy_elements(h, 1))) return rc;
+            if ((rc = op_energy_nodes(h))) return rc;
+        }
         if ((rc = op_fused_stress(h))) return rc;
     } else if (fused) {
         if ((rc = op_fused(h))) return rc;  // element update + stress update
     } else {
         if ((rc = op_begin(h))) return rc;
-        if ((rc = op_energy_elements(h))) return rc;
+        if (!ready && (rc = op_energy_elements(h))) return rc;
         if ((rc = op_energy_nodes(h))) return rc;
         if ((rc = op_calc_stresses(h))) return rc;
     }
     if ((rc = op_loop_nodes(h))) return rc;
-    return op_min_length_scale_sync(h);
+    return op_min_length_scale_sync(h);  // temperature runs: with the next step's heat flux
 }
 
 // apply a deferred element update so that the state matches the reference's
@@ -508,8 +536,8 @@ int request_scalars(snac_gpu* h, long long ts) {
 // captured on first use; no status read
 int launch_step(snac_gpu* h) {
     if (int rc = request_scalars(h, h->time_step + 1)) return rc;
-    int p = h->parity, f = h->pending ? 1 : 0;
-    if (!h->graph[f][p]) {
+    int p = h->parity, f = h->pending ? 1 : 0, r = (h->temperature && h->hflux_ready) ? 1 : 0;
+    if (!h->graph[r][f][p]) {
         cudaGraph_t g;
         long long l0 = h->launches, ts0 = h->time_step;
         CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
@@ -517,18 +545,19 @@ int launch_step(snac_gpu* h) {
         cudaError_t e = cudaStreamEndCapture(h->stream, &g);
         if (rc) return rc;
         if (e != cudaSuccess) return set_err(h, SNAC_GPU_ECUDA, -1, "graph capture: %s", cudaGetErrorString(e));
-        CK(cudaGraphInstantiate(&h->graph[f][p], g, 0));
+        CK(cudaGraphInstantiate(&h->graph[r][f][p], g, 0));
         cudaGraphDestroy(g);
-        h->steps_kernels[f] = (int)(h->launches - l0);
+        h->steps_kernels[r][f] = (int)(h->launches - l0);
         h->launches = l0;  // counted again below, when the graph actually runs
         h->time_step = ts0;
         h->parity = p;
     }
-    CK(cudaGraphLaunch(h->graph[f][p], h->stream));
-    h->launches += h->steps_kernels[f];
+    CK(cudaGraphLaunch(h->graph[r][f][p], h->stream));
+    h->launches += h->steps_kernels[r][f];
     h->time_step++;
     h->parity ^= 1;
     h->pending = true;
+    h->hflux_ready = h->temperature;
     return 0;
 }
 
@@ -915,6 +944,7 @@ static int create_model(const snac_gpu_desc* d_in, snac_gpu** out, cudaStream_t 
     memset(&sc, 0, sizeof sc);
     sc.dt = d->dt;
     sc.minls_bits = 0x7ff0000000000000ull;
+    for (auto& b : sc.minls_slot) b = 0x7ff0000000000000ull;
     if (d->constitutive == SNAC_RHEOLOGY_VISCOPLASTIC) {  // viscoplastic/InitialConditions.c:49-90
         double dtm = 0;
         for (int p = 0; p < d->n_materials; p++) {
@@ -963,9 +993,10 @@ void snac_gpu_destroy(snac_gpu* h) {
     if (!h) return;
     snac_gpu_output_close(h);
     if (h->stream) cudaStreamSynchronize(h->stream);
-    for (auto& gf : h->graph)
-        for (auto& g : gf)
-            if (g) cudaGraphExecDestroy(g);
+    for (auto& gr : h->graph)
+        for (auto& gf : gr)
+            for (auto& g : gf)
+                if (g) cudaGraphExecDestroy(g);
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->pst, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
                     h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr, h->topo_scratch};
@@ -977,6 +1008,7 @@ void snac_gpu_destroy(snac_gpu* h) {
 
 int snac_gpu_time_step_zero(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     if (h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "time step zero already done");
     // Context.c:999-1020: tet density = phase density (the element scalar stress is an output only)
     if (h->has_density) {
@@ -1037,6 +1069,7 @@ int snac_gpu_time_steps(snac_gpu* h, int nsteps, void* flush, size_t flush_bytes
 
 int snac_gpu_begin_step(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     if (int rc = request_scalars(h, h->time_step + 1)) return rc;
     if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
     int rc = flush_pending(h);
@@ -1044,34 +1077,40 @@ int snac_gpu_begin_step(snac_gpu* h) {
 }
 int snac_gpu_loop_elements_energy(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     return rc ? rc : op_energy_elements(h);
 }
 int snac_gpu_loop_nodes_energy(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     return rc ? rc : op_energy_nodes(h);
 }
 int snac_gpu_calc_stresses(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     if (!rc) rc = op_calc_stresses(h);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_loop_nodes_momentum(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     if (!rc) rc = op_loop_nodes(h);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_loop_elements_momentum(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     if (!rc) rc = op_update_elements(h, h->time_step == 0);
     return rc ? rc : read_status(h);
 }
 int snac_gpu_sync(snac_gpu* h) {
     if (!h) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     int rc = flush_pending(h);
     if (!rc) rc = op_sync_full(h);
     return rc ? rc : read_status(h);
@@ -1079,6 +1118,7 @@ int snac_gpu_sync(snac_gpu* h) {
 
 int snac_gpu_upload(snac_gpu* h, const snac_state_view* v) {
     if (!h || !v) return SNAC_GPU_EINVAL;
+    h->hflux_ready = false;  // the state or the step sequence changes
     if (int rc = flush_pending(h)) return rc;
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT;
     int rc;
@@ -1174,6 +1214,7 @@ int snac_gpu_profile_step(snac_gpu* h, snac_kernel_time* out, int max) {
     if (!rc) {
         h->parity ^= 0;  // record_step already flipped the parity in the node loop
         h->pending = true;
+        h->hflux_ready = h->temperature;  // the step's last kernel formed the next heat flux
         CK(cudaStreamSynchronize(h->stream));
         for (int i = 0; i < h->prof_n; i++) {
             float ms = 0;
@@ -1470,6 +1511,7 @@ int batch_run(snac_gpu_batch* b, int nsteps) {
         h->time_step += nsteps;
         h->parity = b->parity;
         if (nsteps > 0) h->pending = true;
+        h->hflux_ready = false;  // the batched step forms each step's heat flux itself
     }
     return 0;
 }
@@ -1764,6 +1806,7 @@ int snap_copy(snac_gpu* h, bool save, Snap& z) {
     } else {
         h->pending = z.pending;
         h->time_step = z.time_step;
+        h->hflux_ready = false;  // the heat-flux rows are not part of a snapshot
     }
     return 0;
 }
@@ -2127,12 +2170,13 @@ int snac_gpu_output_open(snac_gpu* h, const char* output_path, unsigned rank, un
         return set_err(h, SNAC_GPU_ENOMEM, -1, "output staging: %s", cudaGetErrorString(e));
     }
     // the graphs hold the field pointers: re-capture them with the element-scalar buffer
-    for (auto& gf : h->graph)
-        for (auto& g : gf)
-            if (g) {
-                cudaGraphExecDestroy(g);
-                g = nullptr;
-            }
+    for (auto& gr : h->graph)
+        for (auto& gf : gr)
+            for (auto& g : gf)
+                if (g) {
+                    cudaGraphExecDestroy(g);
+                    g = nullptr;
+                }
     return 0;
 }
 

@@ -119,6 +119,9 @@ struct DevScalars {
     double inertial_density0;        // (lambda + 2 mu) / c^2 of phase 0 at the current speed of sound c (dynamic dt)
     unsigned blocks_done;            // blocks of k_min_length_scale_sync finished (0 between launches)
     unsigned pad;
+    // k_heat_flux_min_length_scale's per-block minima, spread over 32
+    // addresses (+inf between steps)
+    unsigned long long minls_slot[32];
 };
 
 __device__ __forceinline__ void report(DevScalars* sc, int code, long long index) {

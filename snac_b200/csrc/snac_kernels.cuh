@@ -1259,7 +1259,13 @@ __device__ __forceinline__ void k_heat_nodes_body(const Mesh& m, const Fields& F
     if (!isfinite(Tnew)) report(F.sc, SNAC_GPU_ENAN, n);
 }
 
-__global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg) {
+// count_step: the step's first kernel (its heat flux was formed at the end
+// of the previous step): timeStep++, currentTime += dt
+__global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg, int count_step) {
+    if (count_step && blockIdx.x == 0 && threadIdx.x == 0) {
+        F.sc->time_step += 1;
+        F.sc->current_time += F.sc->dt;
+    }
     k_heat_nodes_body(m, F, cfg, blockIdx.x);
 }
 
@@ -1316,6 +1322,72 @@ __global__ void __launch_bounds__(MINLS_THREADS) k_min_length_scale_sync(Mesh m,
         __threadfence();
         sync_one(cfg, F.sc, wave_speed);
         F.sc->blocks_done = 0u;
+    }
+}
+
+// Temperature runs: the minimum length scale of step n together with the
+// heat flux of step n+1 (Snac_HeatFlux, temperature/HeatFlux.c:60-200, and
+// its wall BC), which reads the same coordinates x^{n+1} and node
+// temperatures T^{n+1}: one geometry evaluation instead of two.  One thread
+// per tet, as k_heat_flux; each block's minimum goes to one of 32 slots
+// (non-returning atomics spread over addresses, so that the many small
+// blocks neither queue on one address nor wait for a counter), and
+// k_slots_sync then takes the minimum of the slots and runs Sync.  The tet's
+// share of the minimum is RN(V / max_f A_f) from the heat flux's own face areas:
+// max_f RN(RN(sqrt(s_f)) / 2) = RN(RN(sqrt(max_f s_f)) / 2), square root and
+// halving being monotonic and correctly rounded (faces with a NaN area are
+// skipped by both forms), so the minimum has the bits of
+// hex_min_length_scale.
+#ifndef SNAC_HEAT_MINLS_MINB
+#define SNAC_HEAT_MINLS_MINB 5  // resident blocks per SM asked of the kernel below
+#endif
+template <bool ONE>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_HEAT_MINLS_MINB)
+    k_heat_flux_min_length_scale(Mesh m, Fields F, Config cfg) {
+    TetSlot s = tet_slot(m, blockIdx.x);
+    V3 c[4], v[4];
+    double T[4], T0[4];
+    load_tet(m, F, s, c, v, T, T0);
+    TetGeom g;
+    tet_geometry(c, g);
+    heat_flux_tet<ONE>(m, F, cfg, s, T, T0, g);
+    double ls = 1.0e+27f;
+    if (s.active) {
+        double A = 0.0;
+#pragma unroll
+        for (int f = 0; f < 4; f++)
+            if (g.A[f] > A) A = g.A[f];
+        if (A) {
+            const double l = fabs(dv(g.V, A));
+            if (ls > l) ls = l;
+        }
+        if (g.V == 0.0) report(F.sc, SNAC_GPU_EVOLUME, s.e);
+    }
+    for (int o = 16; o > 0; o >>= 1) ls = fmin(ls, __shfl_xor_sync(FULL, ls, o));
+    __shared__ double wmin[ELEM_WARPS];
+    if ((threadIdx.x & 31) == 0) wmin[threadIdx.x >> 5] = ls;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double b = wmin[0];
+#pragma unroll
+        for (int w = 1; w < ELEM_WARPS; w++) b = fmin(b, wmin[w]);
+        atomicMin(&F.sc->minls_slot[blockIdx.x & 31], (unsigned long long)__double_as_longlong(b));
+    }
+}
+
+// One warp after k_heat_flux_min_length_scale: the minimum over its
+// slots (exact: min does not round), the slots reset, then Sync.
+__global__ void k_slots_sync(Config cfg, DevScalars* sc, double wave_speed) {
+    const int l = threadIdx.x;
+    unsigned long long v = sc->minls_slot[l];
+    sc->minls_slot[l] = 0x7ff0000000000000ull;
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long w = __shfl_xor_sync(FULL, v, o);
+        v = w < v ? w : v;
+    }
+    if (l == 0) {
+        if (v < sc->minls_bits) sc->minls_bits = v;
+        sync_one(cfg, sc, wave_speed);
     }
 }
 
