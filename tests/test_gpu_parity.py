@@ -205,6 +205,31 @@ def test_hook_by_hook_equals_graph_step():
         assert np.array_equal(getattr(sa, f), getattr(sb, f)), f
 
 
+def test_graph_steps_after_an_upload_form_a_fresh_heat_flux():
+    """Graph steps of a temperature run form the next step's heat flux in the
+    step's last kernel; an upload in between must not let the next step use
+    that flux of the old temperatures.  The graph steps after the upload give
+    the bits of hook-by-hook steps, which always form their own flux."""
+    make, _ = S.CASES["viscoplastic"]
+    out = []
+    for hooks in (False, True):
+        g = SnacContext(make())
+        g.time_step_zero()
+        g.step(10)
+        s = g.state()
+        s.temperature[:] = s.temperature * 1.01 + np.linspace(0.0, 5.0, s.temperature.size)
+        g.set_state(s, ["temperature"])
+        for _ in range(3):
+            if hooks:
+                g.solve()
+            else:
+                g.step(1)
+        out.append(g.state())
+        g.close()
+    for f in FIELDS:
+        assert np.array_equal(getattr(out[0], f), getattr(out[1], f)), f
+
+
 def test_run_to_run_bit_reproducible():
     make, steps = S.CASES["plastic"]
     out = []
