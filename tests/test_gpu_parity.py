@@ -411,23 +411,25 @@ def test_c2_full_size_1000_steps_bitwise_against_the_reference():
         assert_bitwise(g, c)
 
 
-def test_c3_full_size_20_steps_against_the_reference():
+def test_c3_full_size_100_steps_against_the_reference():
     """The Maxwell visco-plastic workload with temperature at full size (128 x 64 x 128,
-    ~1M hex) over 20 steps against the reference's own sources: within 1e-9 in
-    velocity, stress and temperature (device Arrhenius viscosity), 1e-6 in
-    the viscosity itself and where tets yield (plastic strain)."""
+    ~1M hex) against the reference's own sources, after 20 and after 100 steps:
+    within 1e-9 in velocity, stress, temperature and coordinates (device
+    Arrhenius viscosity), 1e-6 in the viscosity itself and where tets yield
+    (plastic strain)."""
     cfg = W.c3_viscoplastic()
     g = SnacContext(cfg)
     c = Checker(cfg, "reference_mt", threads=_host_threads())
     g.time_step_zero()
     c.time_step_zero()
-    g.step(20)
-    c.step(20)
-    sg, sc = g.state(), c.state()
-    for f in ("velocity", "stress", "temperature", "coord"):
-        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, (f, relerr(getattr(sg, f), getattr(sc, f)))
-    for f in ("viscosity", "plastic_strain"):
-        assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-6, (f, relerr(getattr(sg, f), getattr(sc, f)))
+    for n in (20, 80):
+        g.step(n)
+        c.step(n)
+        sg, sc = g.state(), c.state()
+        for f in ("velocity", "stress", "temperature", "coord"):
+            assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-9, (f, relerr(getattr(sg, f), getattr(sc, f)))
+        for f in ("viscosity", "plastic_strain"):
+            assert relerr(getattr(sg, f), getattr(sc, f)) <= 1e-6, (f, relerr(getattr(sg, f), getattr(sc, f)))
 
 
 def test_c3_full_size_first_steps_within_tolerance():
