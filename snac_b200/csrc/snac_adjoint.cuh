@@ -75,6 +75,9 @@ __device__ __forceinline__ void addc(D3& a, int d, double v) {
 }
 __device__ __forceinline__ double sgnd(double x) { return x < 0 ? -1.0 : (x > 0 ? 1.0 : 0.0); }
 
+#ifndef SNAC_ADJ_SMEM_REC
+#define SNAC_ADJ_SMEM_REC 1  // the forward record in shared memory (fewer spills; measured faster)
+#endif
 // ---- forward record of the constitutive update of one tet --------------------------------
 struct ConsRec {
     // visco-plastic Maxwell step
@@ -275,7 +278,14 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     double eps_p = (MC && s.active) ? S.eps_p[s.q] : 0.0;
     const double eps_p0 = eps_p;
 
+#if SNAC_ADJ_SMEM_REC
+    // the record lives in shared memory (dynamic, one per thread): its ~50
+    // doubles then hold no registers between the forward and the reverse
+    extern __shared__ __align__(16) unsigned char adj_smem[];
+    ConsRec& R = reinterpret_cast<ConsRec*>(adj_smem)[threadIdx.x];
+#else
     ConsRec R;
+#endif
     double st[6];
 #pragma unroll
     for (int a = 0; a < 6; a++) st[a] = s_pre[a];
@@ -826,8 +836,11 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     (void)eps_p0;
 }
 
+#ifndef SNAC_ADJ_MINB
+#define SNAC_ADJ_MINB 1  // resident blocks per SM asked of k_adj_tet
+#endif
 template <int PLUGIN>
-__global__ void __launch_bounds__(ELEM_WARPS * 32) k_adj_tet(Mesh m, Fields F, Config cfg, AdjState S, AdjBufs B,
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ADJ_MINB) k_adj_tet(Mesh m, Fields F, Config cfg, AdjState S, AdjBufs B,
                                                              int rotate, int first_rev, double dt) {
     adj_tet_body<PLUGIN>(m, F, cfg, S, B, rotate, first_rev, dt, blockIdx.x);
 }

@@ -1836,26 +1836,26 @@ int adjoint_supported(snac_gpu* h) {
     return 0;
 }
 
+template <int P>
+int adj_tet_launch_p(snac_gpu* h, const Fields& F, const AdjState& S, const AdjBufs& B, int rotate, int first_rev,
+                     double dt) {
+    const size_t smem = SNAC_ADJ_SMEM_REC ? (size_t)ELEM_WARPS * 32 * sizeof(ConsRec) : 0;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k_adj_tet<P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_adj_tet<P><<<elem_blocks(h->mesh), ELEM_WARPS * 32, smem, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate, first_rev,
+                                                                              dt);
+    return 0;
+}
+
 int adj_tet_launch(snac_gpu* h, const AdjState& S, const AdjBufs& B, int rotate, int first_rev, double dt) {
-    const unsigned nb = elem_blocks(h->mesh);
     const Fields F = fields(h);
+    int rc;
     switch (h->constitutive) {
-        case SNAC_RHEOLOGY_ELASTIC:
-            k_adj_tet<SNAC_RHEOLOGY_ELASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
-                                                                                  first_rev, dt);
-            break;
-        case SNAC_RHEOLOGY_PLASTIC:
-            k_adj_tet<SNAC_RHEOLOGY_PLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
-                                                                                  first_rev, dt);
-            break;
-        case SNAC_RHEOLOGY_MAXWELL:
-            k_adj_tet<SNAC_RHEOLOGY_MAXWELL><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B, rotate,
-                                                                                  first_rev, dt);
-            break;
-        default:
-            k_adj_tet<SNAC_RHEOLOGY_VISCOPLASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, S, B,
-                                                                                       rotate, first_rev, dt);
+        case SNAC_RHEOLOGY_ELASTIC: rc = adj_tet_launch_p<SNAC_RHEOLOGY_ELASTIC>(h, F, S, B, rotate, first_rev, dt); break;
+        case SNAC_RHEOLOGY_PLASTIC: rc = adj_tet_launch_p<SNAC_RHEOLOGY_PLASTIC>(h, F, S, B, rotate, first_rev, dt); break;
+        case SNAC_RHEOLOGY_MAXWELL: rc = adj_tet_launch_p<SNAC_RHEOLOGY_MAXWELL>(h, F, S, B, rotate, first_rev, dt); break;
+        default: rc = adj_tet_launch_p<SNAC_RHEOLOGY_VISCOPLASTIC>(h, F, S, B, rotate, first_rev, dt);
     }
+    if (rc) return rc;
     h->launches++;
     return launch_check_named(h, "k_adj_tet");
 }
