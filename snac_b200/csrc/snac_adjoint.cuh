@@ -51,7 +51,7 @@ struct AdjBufs {
     double4* xbar;   // [nn] adjoint of x (w unused)
     double4* vbar;   // [nn] adjoint of v
     double4* fbar;   // [nn] adjoint of the damped-force input F (xyz) and of the inertial mass (w)
-    double* cbuf;    // [nq][4][6] per-tet corner adjoints (x 3, v 3) for the node gather
+    double* cbuf;    // per-tet corner adjoints (x 3, v 3) for the node gather: rows (t, corner, component) of ner hexes
     double* sbar;    // [nq][6] adjoint of sigma_avg^{n-1}, handed to the next (earlier) step
     double* epbar;   // [nq] adjoint of eps_p
     double* pbar;    // [nq][3] adjoint of the cohesion, friction, viscosity scales
@@ -814,15 +814,18 @@ __device__ __forceinline__ void adj_tet_body(const Mesh& m, const Fields& F, con
     }
 
     if (s.active) {
-        double* o = B.cbuf + s.q * 24;
+        // tet-major rows, as the forward's force terms: the node gather reads
+        // one row at consecutive hexes
+        const long long R = m.ner;
+        double* o = B.cbuf + (long long)(s.t * 24) * R + s.e;
 #pragma unroll
         for (int k = 0; k < 4; k++) {
-            o[k * 6 + 0] = cb[k].x;
-            o[k * 6 + 1] = cb[k].y;
-            o[k * 6 + 2] = cb[k].z;
-            o[k * 6 + 3] = vb[k].x;
-            o[k * 6 + 4] = vb[k].y;
-            o[k * 6 + 5] = vb[k].z;
+            o[(k * 6 + 0) * R] = cb[k].x;
+            o[(k * 6 + 1) * R] = cb[k].y;
+            o[(k * 6 + 2) * R] = cb[k].z;
+            o[(k * 6 + 3) * R] = vb[k].x;
+            o[(k * 6 + 4) * R] = vb[k].y;
+            o[(k * 6 + 5) * R] = vb[k].z;
         }
         // pass 0 leaves the adjoint of the stress the state held
 #pragma unroll
@@ -865,13 +868,14 @@ __global__ void __launch_bounds__(128) k_adj_nodes(Mesh m, Fields F, AdjState cu
             for (int idx = 0; idx < 5; idx++) {
                 const int t = node_tet(ne, idx);
                 const int qn = (node_face(ne, idx) + 3) & 3;  // face f is opposite local node (f+3)%4
-                const double* o = B.cbuf + (e * NT + t) * 24 + qn * 6;
+                const long long R = m.ner;
+                const double* o = B.cbuf + (long long)(t * 24 + qn * 6) * R + e;
                 xb.x += o[0];
-                xb.y += o[1];
-                xb.z += o[2];
-                vb.x += o[3];
-                vb.y += o[4];
-                vb.z += o[5];
+                xb.y += o[R];
+                xb.z += o[2 * R];
+                vb.x += o[3 * R];
+                vb.y += o[4 * R];
+                vb.z += o[5 * R];
             }
         }
     }

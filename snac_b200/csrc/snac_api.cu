@@ -1911,7 +1911,7 @@ int adj_work_alloc(snac_gpu* h, AdjWork& w) {
     const long long nn = h->mesh.nn, nq = h->mesh.ne * NT, nt = (long long)h->mesh.nnx * h->mesh.nnz;
     int rc;
     if ((rc = dalloc(h, &w.B.xbar, nn)) || (rc = dalloc(h, &w.B.vbar, nn)) || (rc = dalloc(h, &w.B.fbar, nn)) ||
-        (rc = dalloc(h, &w.B.cbuf, nq * 24)) || (rc = dalloc(h, &w.B.sbar, nq * 6)) || (rc = dalloc(h, &w.B.epbar, nq)) ||
+        (rc = dalloc(h, &w.B.cbuf, h->mesh.ner * NT * 24)) || (rc = dalloc(h, &w.B.sbar, nq * 6)) || (rc = dalloc(h, &w.B.epbar, nq)) ||
         (rc = dalloc(h, &w.B.pbar, nq * 3)) || (rc = dalloc(h, &w.terms, nt)) || (rc = dalloc(h, &w.grads, 3 * h->mesh.ne)))
         return rc;
     if (h->constitutive == SNAC_RHEOLOGY_MAXWELL && (rc = dalloc(h, &w.B.vobar, nq))) return rc;
