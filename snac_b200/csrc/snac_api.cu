@@ -355,7 +355,7 @@ int op_calc_stresses(snac_gpu* h) {
 
 int op_loop_nodes(snac_gpu* h) {
     Fields F = fields(h);
-    unsigned nb = node_blocks(h->mesh);
+    const unsigned nb = node_blocks(h->mesh);
     const bool vo = h->cfg.vonly != 0;
     switch (h->cfg.dt_type) {
         case SNAC_DT_CONSTANT:

@@ -1004,23 +1004,71 @@ __device__ __noinline__ V3 traction_force(const double4* pos, int nx, int ny, in
 
 // VONLY: cfg.vonly (a template argument, so that the gather loop of each
 // instance is straight-line code)
+// The tail of the node loop for node n with its summed force and inertial
+// mass: force-BC plugins, FLAC local damping with the pre-update velocity
+// (UpdateNode.c:102-104), v and x update, BC override; returns the node's
+// max-BC-speed candidate.
+__device__ __forceinline__ double node_update(const Mesh& m, const Fields& F, const Config& cfg, long long n, int i,
+                                              int j, int k, double fx, double fy, double fz, double imass) {
+    const double dt = F.sc->dt;
+    if (cfg.winkler && cfg.gravity > 0.0 && j == 0) {
+        const WinklerArgs a{F.pos, F.mat, F.mats, F.residual_fr, F.sc->time_step, cfg.pisos, cfg.gravity, cfg.rzbo};
+        const V3 r = winkler_force(a, m.nx, m.ny, m.nz, n, i, k, V3{fx, fy, fz});
+        fx = r.x;
+        fy = r.y;
+        fz = r.z;
+    }
+    if (cfg.traction && i == m.nnx - 1) {
+        const V3 r = traction_force(F.pos, m.nx, m.ny, m.nz, j, k, V3{fx, fy, fz});
+        fx = r.x;
+        fy = r.y;
+        fz = r.z;
+    }
+    double4 w = F.vel[n];
+    const double demf = cfg.demf;
+    auto sgn = [](double x) { return x < 0 ? -1.0f : x > 0 ? +1.0f : 0.0f; };
+    fx -= demf * sgn(w.x) * fabs(fx);
+    fy -= demf * sgn(w.y) * fabs(fy);
+    fz -= demf * sgn(w.z) * fabs(fz);
+    double dw[3] = {dt * fx, dt * fy, dt * fz};
+    dvz_n(dw, imass, recip(imass));
+    w.x += dw[0];
+    w.y += dw[1];
+    w.z += dw[2];
+    uchar4 b = F.bc[n];
+    if (b.x != 255) w.x = F.vbc_val[b.x * 3 + 0];
+    if (b.y != 255) w.y = F.vbc_val[b.y * 3 + 1];
+    if (b.z != 255) w.z = F.vbc_val[b.z * 3 + 2];
+    double4 p = F.pos[n];
+    p.x += dt * w.x;
+    p.y += dt * w.y;
+    p.z += dt * w.z;
+    F.pos_next[n] = p;
+    F.vel[n] = w;
+    F.force[n] = make_double4(fx, fy, fz, imass);
+    if (!(isfinite(w.x) && isfinite(w.y) && isfinite(w.z))) report(F.sc, SNAC_GPU_ENAN, n);
+    return (b.x != 255 || b.y != 255 || b.z != 255) ? sqrt(w.x * w.x + w.y * w.y + w.z * w.z) : 0.0;
+}
+
+// Snac_Force (Force.c:53-188) for node n: the 8 incident hexes in
+// HexaEL.c:529-573 order, 5 tets each (NodeToTetra/NodeToSurface); absent
+// hexes are skipped (Force.c:92).  With cfg.vonly the fgrav row holds the
+// tet volume: (g rho) V / 8 and (1/4 rho_i) V are formed here exactly as the
+// element kernel forms them.
+// VONLY: cfg.vonly (a template argument, so that the gather loop of each
+// instance is straight-line code)
 template <int DTTYPE, bool VONLY>
 __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F, const Config& cfg, int lb) {
     long long n = (long long)lb * blockDim.x + threadIdx.x;
     bool active = n < m.nn;
     double vcand = 0.0;
     if (active) {
-        const double dt = F.sc->dt;
         int i, j, k;
         split3(n, m.nnx, m.nny, i, j, k);
         double fx = 0.0, fy = 0.0, fz = 0.0, imass = 0.0f;
-        // with cfg.vonly the fgrav row holds the tet volume: (g rho) V / 8 and
-        // (1/4 rho_i) V are formed here exactly as the element kernel forms them
         const double gr = VONLY ? cfg.gravity * cfg.m0.density : 0.0;
         const double f4r =
             VONLY ? (1.0f / 4.0f) * (DTTYPE == SNAC_DT_DYNAMIC ? F.sc->inertial_density0 : cfg.m0.density) : 0.0;
-        // Snac_Force: the 8 incident hexes in HexaEL.c:529-573 order, 5 tets each
-        // (NodeToTetra/NodeToSurface); absent hexes are skipped (Force.c:92)
 #pragma unroll
         for (int ne = 0; ne < 8; ne++) {
             int ei = i - 1 + (ne & 1), ej = j - 1 + ((ne >> 1) & 1), ek = k - 1 + ((ne >> 2) & 1);
@@ -1048,44 +1096,7 @@ __device__ __forceinline__ void k_loop_nodes_body(const Mesh& m, const Fields& F
                 }
             }
         }
-        if (cfg.winkler && cfg.gravity > 0.0 && j == 0) {
-            const WinklerArgs a{F.pos, F.mat, F.mats, F.residual_fr, F.sc->time_step, cfg.pisos, cfg.gravity, cfg.rzbo};
-            const V3 r = winkler_force(a, m.nx, m.ny, m.nz, n, i, k, V3{fx, fy, fz});
-            fx = r.x;
-            fy = r.y;
-            fz = r.z;
-        }
-        if (cfg.traction && i == m.nnx - 1) {
-            const V3 r = traction_force(F.pos, m.nx, m.ny, m.nz, j, k, V3{fx, fy, fz});
-            fx = r.x;
-            fy = r.y;
-            fz = r.z;
-        }
-        // FLAC local damping with the pre-update velocity, then v and x
-        double4 w = F.vel[n];
-        const double demf = cfg.demf;
-        auto sgn = [](double x) { return x < 0 ? -1.0f : x > 0 ? +1.0f : 0.0f; };
-        fx -= demf * sgn(w.x) * fabs(fx);
-        fy -= demf * sgn(w.y) * fabs(fy);
-        fz -= demf * sgn(w.z) * fabs(fz);
-        double dw[3] = {dt * fx, dt * fy, dt * fz};
-        dvz_n(dw, imass, recip(imass));
-        w.x += dw[0];
-        w.y += dw[1];
-        w.z += dw[2];
-        uchar4 b = F.bc[n];
-        if (b.x != 255) w.x = F.vbc_val[b.x * 3 + 0];
-        if (b.y != 255) w.y = F.vbc_val[b.y * 3 + 1];
-        if (b.z != 255) w.z = F.vbc_val[b.z * 3 + 2];
-        double4 p = F.pos[n];
-        p.x += dt * w.x;
-        p.y += dt * w.y;
-        p.z += dt * w.z;
-        F.pos_next[n] = p;
-        F.vel[n] = w;
-        F.force[n] = make_double4(fx, fy, fz, imass);
-        if (!(isfinite(w.x) && isfinite(w.y) && isfinite(w.z))) report(F.sc, SNAC_GPU_ENAN, n);
-        if (b.x != 255 || b.y != 255 || b.z != 255) vcand = sqrt(w.x * w.x + w.y * w.y + w.z * w.z);
+        vcand = node_update(m, F, cfg, n, i, j, k, fx, fy, fz, imass);
     }
     // max |v| over velocity-BC nodes for Sync (exact: max does not round)
     for (int o = 16; o > 0; o >>= 1) vcand = fmax(vcand, __shfl_xor_sync(FULL, vcand, o));
