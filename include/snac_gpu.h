@@ -259,6 +259,26 @@ int  snac_gpu_sync(snac_gpu* h);
 /* ---- state transfer -------------------------------------------------------- */
 int  snac_gpu_upload(snac_gpu* h, const snac_state_view* v);
 int  snac_gpu_download(snac_gpu* h, const snac_state_view* v);
+/* One step of a model whose state the host keeps: the fields `in` names are
+ * uploaded, one step runs (snac_gpu_step), and the fields `out` names are
+ * downloaded; the result has the bits of snac_gpu_upload(in) +
+ * snac_gpu_step(h, 1) + snac_gpu_download(out).  Replaces, for a host that
+ * owns the Snac context's arrays between steps, the per-step transfers
+ * around _Snac_Context_Solve (Context.c:1063-1099) and Sync (:1208-1268).
+ *   - The transfers overlap the kernels and each other: the mesh is cut
+ *     along k into `chunks` slabs (at most 64; 0: one per 8 MiB of tet
+ *     stresses, 1 to 16); each slab's kernels
+ *     start when its upload has arrived, and its download starts when its
+ *     last kernel is done.  The overlap needs page-locked host arrays
+ *     (cudaHostAlloc / cudaHostRegister); pageable ones give the same
+ *     result without it.
+ *   - `in` and `out` may name the same arrays (the step updates them in
+ *     place); NULL members are not transferred.
+ *   - Models with topography diffusion or open dump files, or an `out`
+ *     asking for force or inertial mass, run the three calls in sequence.
+ *   - Device memory: node staging of 14 doubles per node, allocated on the
+ *     first call, with two streams and the slab events. */
+int  snac_gpu_step_host(snac_gpu* h, const snac_state_view* in, const snac_state_view* out, int chunks);
 int  snac_gpu_scalars(snac_gpu* h, snac_scalars* out);
 int  snac_gpu_set_dt(snac_gpu* h, double dt);   /* _Snac_Context_SetDt, Context.c:1047-1053 */
 

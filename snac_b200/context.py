@@ -58,6 +58,8 @@ def load_library(path: str = LIB_PATH):
     lib.snac_gpu_upload.restype = C.c_int
     lib.snac_gpu_download.argtypes = [vp, C.POINTER(StateView)]
     lib.snac_gpu_download.restype = C.c_int
+    lib.snac_gpu_step_host.argtypes = [vp, C.POINTER(StateView), C.POINTER(StateView), C.c_int]
+    lib.snac_gpu_step_host.restype = C.c_int
     lib.snac_gpu_scalars.argtypes = [vp, C.POINTER(Scalars)]
     lib.snac_gpu_scalars.restype = C.c_int
     lib.snac_gpu_set_dt.argtypes = [vp, C.c_double]
@@ -238,6 +240,23 @@ class SnacContext:
     def set_state(self, s: State, fields: Optional[list] = None):
         v = s.view(fields)
         self._check(self.lib.snac_gpu_upload(self.h, C.byref(v)))
+
+    def step_host(self, s_in: State, s_out: State, fields_in: Optional[list] = None,
+                  fields_out: Optional[list] = None, chunks: int = 0) -> State:
+        """One step of a host-held state: upload `fields_in` of s_in, one step,
+        download `fields_out` into s_out (same bits as set_state + step(1) +
+        state), with the transfers overlapped slab by slab (snac_gpu_step_host).
+        Without an explicit list, the step's state moves: coordinates,
+        velocities, stresses, the hooks' per-tet state and the temperature."""
+        default = ["coord", "velocity", "stress", "plastic_strain", "viscosity"]
+        if self.cfg.temperature:
+            default.append("temperature")
+        if self.keeps_plastic_strain_tensor:
+            default.append("plastic_strain_tensor")
+        vi = s_in.view(fields_in if fields_in is not None else default)
+        vo = s_out.view(fields_out if fields_out is not None else default)
+        self._check(self.lib.snac_gpu_step_host(self.h, C.byref(vi), C.byref(vo), int(chunks)))
+        return s_out
 
     def scalars(self) -> Scalars:
         o = Scalars()

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -50,6 +51,20 @@ struct OutputState {
     bool dump = false, cp = false;
     int err = 0;
     int want = 0;             // the last element-scalar request sent to the device
+};
+
+// Streams, events and node staging of snac_gpu_step_host (created on its
+// first call): uploads run on `in`, downloads on `out`, kernels on the
+// handle's stream, ordered slab by slab through the events.
+constexpr int STEP_HOST_MAX_CHUNKS = 64;
+struct HostStep {
+    cudaStream_t in = nullptr, out = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr, nodes_in = nullptr;
+    cudaEvent_t ev_in[STEP_HOST_MAX_CHUNKS] = {}, ev_nodes[STEP_HOST_MAX_CHUNKS] = {},
+                ev_elems[STEP_HOST_MAX_CHUNKS] = {};
+    double* stage_in = nullptr;   // [nn][3] coordinates, [nn][3] velocities, [nn] temperatures, as the host holds them
+    double* stage_out = nullptr;  // the same rows
+    bool ready = false;
 };
 
 struct snac_gpu {
@@ -94,6 +109,7 @@ struct snac_gpu {
     double* residual_fr = nullptr;  // [nn] Winkler residual force
     double* topo_scratch = nullptr;  // [nnx * nnz] topography-diffusion scratch
     OutputState* out = nullptr;
+    HostStep* hs = nullptr;  // snac_gpu_step_host's streams and staging
     // host mirror of the step bookkeeping
     int parity = 0;
     long long time_step = 0;
@@ -590,6 +606,108 @@ int node_out(snac_gpu* h, const double4* src, double* dst, int what) {
     return 0;
 }
 
+// ---- slab launches of snac_gpu_step_host -----------------------------------------
+// Element slabs are block ranges [b0, b1) of the whole-mesh element launch,
+// node slabs block ranges of the node launch; an empty range launches nothing.
+int op_calc_stresses_slab(snac_gpu* h, const Fields& F, int b0, int b1) {
+    if (b1 <= b0) return 0;
+    const unsigned nb = (unsigned)(b1 - b0);
+    const Config& c = h->cfg;
+    cudaStream_t st = h->stream;
+#define SLAB_STRESS(P)                                                                              \
+    do {                                                                                             \
+        if (h->mat) k_calc_stresses_slab<P, false><<<nb, ELEM_WARPS * 32, 0, st>>>(h->mesh, F, c, b0); \
+        else k_calc_stresses_slab<P, true><<<nb, ELEM_WARPS * 32, 0, st>>>(h->mesh, F, c, b0);         \
+    } while (0)
+    switch (h->constitutive) {
+        case SNAC_RHEOLOGY_ELASTIC: SLAB_STRESS(SNAC_RHEOLOGY_ELASTIC); break;
+        case SNAC_RHEOLOGY_PLASTIC: SLAB_STRESS(SNAC_RHEOLOGY_PLASTIC); break;
+        case SNAC_RHEOLOGY_VISCOPLASTIC:
+            if (h->dp) SLAB_STRESS(SNAC_VP_DP);
+            else SLAB_STRESS(SNAC_RHEOLOGY_VISCOPLASTIC);
+            break;
+        case SNAC_RHEOLOGY_MAXWELL: SLAB_STRESS(SNAC_RHEOLOGY_MAXWELL); break;
+    }
+#undef SLAB_STRESS
+    h->launches++;
+    return launch_check_named(h, "k_calc_stresses_slab");
+}
+
+int op_loop_nodes_slab(snac_gpu* h, const Fields& F, int b0, int b1) {
+    if (b1 <= b0) return 0;
+    const unsigned nb = (unsigned)(b1 - b0);
+    const bool vo = h->cfg.vonly != 0;
+    cudaStream_t st = h->stream;
+    switch (h->cfg.dt_type) {
+        case SNAC_DT_CONSTANT:
+            k_loop_nodes_slab<SNAC_DT_CONSTANT, false><<<nb, 128, 0, st>>>(h->mesh, F, h->cfg, b0);
+            break;
+        case SNAC_DT_DYNAMIC:
+            if (vo) k_loop_nodes_slab<SNAC_DT_DYNAMIC, true><<<nb, 128, 0, st>>>(h->mesh, F, h->cfg, b0);
+            else k_loop_nodes_slab<SNAC_DT_DYNAMIC, false><<<nb, 128, 0, st>>>(h->mesh, F, h->cfg, b0);
+            break;
+        default:
+            if (vo) k_loop_nodes_slab<SNAC_DT_WAVE, true><<<nb, 128, 0, st>>>(h->mesh, F, h->cfg, b0);
+            else k_loop_nodes_slab<SNAC_DT_WAVE, false><<<nb, 128, 0, st>>>(h->mesh, F, h->cfg, b0);
+            break;
+    }
+    h->launches++;
+    return launch_check_named(h, "k_loop_nodes_slab");
+}
+
+int op_update_elements_slab(snac_gpu* h, const Fields& F, int b0, int b1) {
+    if (b1 <= b0) return 0;
+    const unsigned nb = (unsigned)(b1 - b0);
+    Config c = h->cfg;
+    c.time_step_zero = 0;
+    if (h->constitutive == SNAC_RHEOLOGY_MAXWELL)
+        k_update_elements_slab<SNAC_RHEOLOGY_MAXWELL><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c, b0);
+    else
+        k_update_elements_slab<SNAC_RHEOLOGY_ELASTIC><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, c, b0);
+    h->launches++;
+    return launch_check_named(h, "k_update_elements_slab");
+}
+
+int op_heat_flux_slab(snac_gpu* h, const Fields& F, int b0, int b1) {
+    if (b1 <= b0) return 0;
+    const unsigned nb = (unsigned)(b1 - b0);
+    if (h->mat)
+        k_heat_flux_slab<false><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, b0);
+    else
+        k_heat_flux_slab<true><<<nb, ELEM_WARPS * 32, 0, h->stream>>>(h->mesh, F, h->cfg, b0);
+    h->launches++;
+    return launch_check_named(h, "k_heat_flux_slab");
+}
+
+int op_heat_nodes_slab(snac_gpu* h, const Fields& F, int b0, int b1) {
+    if (b1 <= b0) return 0;
+    k_heat_nodes_slab<<<(unsigned)(b1 - b0), 128, 0, h->stream>>>(h->mesh, F, h->cfg, b0);
+    h->launches++;
+    return launch_check_named(h, "k_heat_nodes_slab");
+}
+
+int ensure_host_step(snac_gpu* h) {
+    if (h->hs && h->hs->ready) return 0;
+    if (h->hs) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_step_host: an earlier set-up of its streams failed");
+    HostStep* q = new HostStep();
+    h->hs = q;  // released by snac_gpu_destroy, also when set-up fails half way
+    CK(cudaStreamCreateWithFlags(&q->in, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&q->out, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&q->start, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&q->done, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&q->nodes_in, cudaEventDisableTiming));
+    for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++) {
+        CK(cudaEventCreateWithFlags(&q->ev_in[c], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&q->ev_nodes[c], cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&q->ev_elems[c], cudaEventDisableTiming));
+    }
+    int rc;
+    if ((rc = dalloc(h, &q->stage_in, (size_t)h->mesh.nn * 7))) return rc;
+    if ((rc = dalloc(h, &q->stage_out, (size_t)h->mesh.nn * 7))) return rc;
+    q->ready = true;
+    return 0;
+}
+
 // hydroStaticIC/VariableConditions.c:43-152 on one rank: lithostatic
 // pressure integrated down each element column; densities are the phase
 // densities (tet densities are still zero at this point of the reference's IC).
@@ -997,6 +1115,20 @@ void snac_gpu_destroy(snac_gpu* h) {
         for (auto& gf : gr)
             for (auto& g : gf)
                 if (g) cudaGraphExecDestroy(g);
+    if (HostStep* q = h->hs) {
+        for (cudaStream_t st : {q->in, q->out})
+            if (st) cudaStreamSynchronize(st);
+        for (cudaEvent_t e : {q->start, q->done, q->nodes_in})
+            if (e) cudaEventDestroy(e);
+        for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++)
+            for (cudaEvent_t e : {q->ev_in[c], q->ev_nodes[c], q->ev_elems[c]})
+                if (e) cudaEventDestroy(e);
+        for (cudaStream_t st : {q->in, q->out})
+            if (st) cudaStreamDestroy(st);
+        if (q->stage_in) cudaFree(q->stage_in);
+        if (q->stage_out) cudaFree(q->stage_out);
+        delete q;
+    }
     void* bufs[] = {h->pos[0], h->pos[1], h->vel, h->force, h->stress, h->eps_p, h->pst, h->visc, h->density, h->vol,
                     h->hflux, h->tpre, h->fterm, h->fgrav, h->fmass, h->bc, h->vbc_val, h->tbc_val, h->mat, h->mats, h->coh_scale, h->fric_scale,
                     h->visc_scale, h->sc, h->stage, h->escal, h->residual_fr, h->topo_scratch};
@@ -1160,6 +1292,234 @@ int snac_gpu_download(snac_gpu* h, const snac_state_view* v) {
     if (v->plastic_strain && !h->eps_p) memset(v->plastic_strain, 0, nq * sizeof(double));
     if (v->viscosity && !h->visc) memset(v->viscosity, 0, nq * sizeof(double));
     if (want_pst && !h->pst) memset(v->plastic_strain_tensor, 0, nq * 6 * sizeof(double));
+    return 0;
+}
+
+// One step with the state in host memory, as snac_gpu_upload + snac_gpu_step(1)
+// + snac_gpu_download, with the transfers overlapped slab by slab.  The mesh
+// is cut along k (the slowest index of hexes and nodes) into `chunks` slabs
+// of whole element blocks, and into as many node slabs of whole node blocks,
+// node slab c ending below the first k-plane of element slab c + 1.  The step
+// is a chain of stages that alternate between the two kinds of slab: the
+// momentum step is stress update (hexes) -> force gather and node update
+// (nodes) -> element update with the minimum length scale (hexes); models
+// with temperature put heat flux (hexes) -> temperature update (nodes) in
+// front.  A hex stage's slab reads the nodes of its k-planes and the next
+// one, so it waits until the node stage before it has finished those nodes;
+// a node stage's slab gathers from every hex of its planes and the planes
+// below, so it waits until the hex stage before it has finished those hexes.
+// A node slab only writes its own nodes, and by then no later slab of the
+// earlier stages reads them.  The node state and the per-slab hex state are
+// uploaded ahead on one stream, kernels run on the handle's stream, and each
+// slab's results go back on a third stream once its last stage is done, so
+// the host link carries both directions at once.  Every hex and node goes
+// through the kernel bodies of the whole-mesh step and the reductions
+// (max |v|, minimum length scale) are exact, so the result has the bits of
+// the three calls.
+// Queues the slab pipeline of one step (see snac_gpu_step_host) on the
+// handle's stream and the two transfer streams; the handle's stream ends
+// after every transfer of the step.
+static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_state_view* out, int S) {
+    int rc = 0;
+    HostStep* q = h->hs;
+    const Mesh& m = h->mesh;
+    const long long ne = m.ne, nn = m.nn;
+    const long long LE = (long long)m.nx * m.ny, P = (long long)m.nnx * m.nny;  // hexes per k-layer, nodes per k-plane
+    std::vector<long long> E(S + 1), N(S + 1);
+    for (int c = 0; c < S; c++) {
+        E[c] = ne * c / S / ELEM_PER_BLOCK * ELEM_PER_BLOCK;
+        N[c] = std::min(nn, E[c] / LE * P) / 128 * 128;
+    }
+    E[S] = ne;
+    N[S] = nn;
+    // nodes [0, need_nodes(c)) hold every node element slab c touches
+    auto need_nodes = [&](int c) -> long long {
+        if (E[c + 1] <= E[c]) return 0;
+        const long long k = (E[c + 1] - 1) / LE;
+        return std::min(nn, (k + 2) * P);
+    };
+    // hexes [0, need_elems(d)) hold every hex incident to node slab d
+    auto need_elems = [&](int d) -> long long {
+        if (N[d + 1] <= N[d]) return 0;
+        const long long k = (N[d + 1] - 1) / P;
+        return std::min(ne, (k + 1) * LE);
+    };
+    const bool want_pst = out->plastic_strain_tensor != nullptr;
+    const bool give_pst = in->plastic_strain_tensor != nullptr;
+    const size_t D = sizeof(double);
+    auto elems_in = [&](long long e0, long long e1) -> int {
+        if (e1 <= e0) return 0;
+        const long long a = e0 * NT, n = (e1 - e0) * NT;
+        if (in->stress) CK(cudaMemcpyAsync(h->stress + a * 6, in->stress + a * 6, n * 6 * D, cudaMemcpyHostToDevice, q->in));
+        if (in->plastic_strain && h->eps_p)
+            CK(cudaMemcpyAsync(h->eps_p + a, in->plastic_strain + a, n * D, cudaMemcpyHostToDevice, q->in));
+        if (in->viscosity && h->visc)
+            CK(cudaMemcpyAsync(h->visc + a, in->viscosity + a, n * D, cudaMemcpyHostToDevice, q->in));
+        if (give_pst && h->pst)
+            CK(cudaMemcpyAsync(h->pst + a * 6, in->plastic_strain_tensor + a * 6, n * 6 * D, cudaMemcpyHostToDevice, q->in));
+        return 0;
+    };
+    auto elems_out = [&](long long e0, long long e1) -> int {
+        if (e1 <= e0) return 0;
+        const long long a = e0 * NT, n = (e1 - e0) * NT;
+        if (out->stress) CK(cudaMemcpyAsync(out->stress + a * 6, h->stress + a * 6, n * 6 * D, cudaMemcpyDeviceToHost, q->out));
+        if (out->plastic_strain && h->eps_p)
+            CK(cudaMemcpyAsync(out->plastic_strain + a, h->eps_p + a, n * D, cudaMemcpyDeviceToHost, q->out));
+        if (out->viscosity && h->visc)
+            CK(cudaMemcpyAsync(out->viscosity + a, h->visc + a, n * D, cudaMemcpyDeviceToHost, q->out));
+        if (want_pst && h->pst)
+            CK(cudaMemcpyAsync(out->plastic_strain_tensor + a * 6, h->pst + a * 6, n * 6 * D, cudaMemcpyDeviceToHost, q->out));
+        return 0;
+    };
+
+    // the stages of the step; even entries are hex stages, odd ones node stages
+    enum Stage { HEAT_FLUX, HEAT_NODES, STRESS, MOMENTUM_NODES, UPDATE };
+    std::vector<Stage> stages;
+    if (h->temperature) stages = {HEAT_FLUX, HEAT_NODES};
+    stages.insert(stages.end(), {STRESS, MOMENTUM_NODES, UPDATE});
+    const int ns = (int)stages.size();
+
+    const int p = h->parity;
+    const Fields F0 = fields_at(h, p);      // this step: coordinates in pos[p], moved into pos[p ^ 1]
+    const Fields F1 = fields_at(h, p ^ 1);  // the element update reads the moved coordinates
+    double* const si = q->stage_in;         // [coordinates | velocities | temperatures]
+    double* const so = q->stage_out;
+    CK(cudaEventRecord(q->start, h->stream));  // after anything the handle ran before
+    CK(cudaStreamWaitEvent(q->in, q->start, 0));
+    CK(cudaStreamWaitEvent(q->out, q->start, 0));
+    // uploads, all queued at once: the node state first, then the hex state slab by slab
+    if (in->coord) CK(cudaMemcpyAsync(si, in->coord, nn * 3 * D, cudaMemcpyHostToDevice, q->in));
+    if (in->velocity) CK(cudaMemcpyAsync(si + nn * 3, in->velocity, nn * 3 * D, cudaMemcpyHostToDevice, q->in));
+    if (in->temperature) CK(cudaMemcpyAsync(si + nn * 6, in->temperature, nn * D, cudaMemcpyHostToDevice, q->in));
+    CK(cudaEventRecord(q->nodes_in, q->in));
+    for (int c = 0; c < S; c++) {
+        if ((rc = elems_in(E[c], E[c + 1]))) return rc;
+        CK(cudaEventRecord(q->ev_in[c], q->in));
+    }
+    if ((rc = op_begin(h))) return rc;  // timeStep++, currentTime += dt
+    CK(cudaStreamWaitEvent(h->stream, q->nodes_in, 0));
+    if (in->coord || in->velocity || in->temperature) {
+        k_unpack_node_state<<<(unsigned)((nn + 255) / 256), 256, 0, h->stream>>>(
+            h->pos[p], in->coord ? si : nullptr, in->temperature ? si + nn * 6 : nullptr, h->vel,
+            in->velocity ? si + nn * 3 : nullptr, nn);
+        h->launches++;
+        if ((rc = launch_check_named(h, "k_unpack_node_state"))) return rc;
+    }
+
+    // Kernels in dependency order: the deepest stage that can take its next
+    // slab goes first, so that a slab's last stage (and its download) is not
+    // queued behind hex slabs still waiting for their uploads.
+    std::vector<int> done(ns, 0);
+    auto ready = [&](int s) -> bool {
+        const int i = done[s];
+        if (i >= S) return false;
+        if (s == 0) return true;
+        if (stages[s] == HEAT_NODES || stages[s] == MOMENTUM_NODES) return E[done[s - 1]] >= need_elems(i);
+        return N[done[s - 1]] >= need_nodes(i) && done[s - 2] > i;
+    };
+    int total = 0;
+    while (total < ns * S) {
+        int s = ns - 1;
+        while (s > 0 && !ready(s)) s--;
+        const int i = done[s];
+        if (s == 0) {
+            if (i >= S)  // every bound above is met once all hex slabs of stage 0 are done
+                return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_step_host: slab schedule stalled");
+            CK(cudaStreamWaitEvent(h->stream, q->ev_in[i], 0));
+        }
+        const int b0 = (int)(E[i] / ELEM_PER_BLOCK), b1 = (int)((E[i + 1] + ELEM_PER_BLOCK - 1) / ELEM_PER_BLOCK);
+        const int n0 = (int)(N[i] / 128), n1 = (int)((N[i + 1] + 127) / 128);
+        switch (stages[s]) {
+            case HEAT_FLUX: rc = op_heat_flux_slab(h, F0, b0, b1); break;
+            case HEAT_NODES: rc = op_heat_nodes_slab(h, F0, n0, n1); break;
+            case STRESS: rc = op_calc_stresses_slab(h, F0, b0, b1); break;
+            case MOMENTUM_NODES: rc = op_loop_nodes_slab(h, F0, n0, n1); break;
+            case UPDATE: rc = op_update_elements_slab(h, F1, b0, b1); break;
+        }
+        if (rc) return rc;
+        if (stages[s] == MOMENTUM_NODES && N[i + 1] > N[i] && (out->coord || out->velocity || out->temperature)) {
+            const long long a = N[i], n = N[i + 1] - N[i];
+            k_pack_node_state<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
+                h->pos[p ^ 1] + a, out->coord ? so + a * 3 : nullptr, out->temperature ? so + nn * 6 + a : nullptr,
+                h->vel + a, out->velocity ? so + nn * 3 + a * 3 : nullptr, n);
+            h->launches++;
+            if ((rc = launch_check_named(h, "k_pack_node_state"))) return rc;
+            CK(cudaEventRecord(q->ev_nodes[i], h->stream));
+            CK(cudaStreamWaitEvent(q->out, q->ev_nodes[i], 0));
+            if (out->coord) CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (out->velocity)
+                CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (out->temperature)
+                CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
+        }
+        if (stages[s] == UPDATE) {
+            CK(cudaEventRecord(q->ev_elems[i], h->stream));
+            CK(cudaStreamWaitEvent(q->out, q->ev_elems[i], 0));
+            if ((rc = elems_out(E[i], E[i + 1]))) return rc;
+        }
+        done[s]++;
+        total++;
+    }
+    if ((rc = op_sync(h))) return rc;  // Sync: the next dt from this step's reductions
+    CK(cudaEventRecord(q->done, q->out));
+    CK(cudaStreamWaitEvent(h->stream, q->done, 0));
+    return 0;
+}
+
+int snac_gpu_step_host(snac_gpu* h, const snac_state_view* in, const snac_state_view* out, int chunks) {
+    if (!h || !in || !out) return SNAC_GPU_EINVAL;
+    if (chunks < 0 || chunks > STEP_HOST_MAX_CHUNKS)
+        return set_err(h, SNAC_GPU_EINVAL, -1, "snac_gpu_step_host: chunks = %d, allowed 0 (default) to %d", chunks,
+                       STEP_HOST_MAX_CHUNKS);
+    if (!h->zero_done) return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_time_step_zero must come first");
+    // Topography diffusion (a wavefront over the whole top surface), dump
+    // files, kernel timing and node fields the step does not move take the
+    // three calls.
+    const bool slabs = !topo_on(h->cfg) && !h->out && h->own_stream && !h->prof && !out->force && !out->inertial_mass;
+    if (!slabs) {
+        int rc = snac_gpu_upload(h, in);
+        if (!rc) rc = snac_gpu_step(h, 1);
+        if (!rc) rc = snac_gpu_download(h, out);
+        return rc;
+    }
+    int rc = ensure_host_step(h);
+    if (rc) return rc;
+    HostStep* q = h->hs;
+    h->hflux_ready = false;  // this step forms its own heat flux
+    if ((rc = flush_pending(h))) return rc;
+    // the caller's views as this handle reads them (a version-1 view has no
+    // plastic-strain tensor)
+    snac_state_view vi{}, vo{};
+    const size_t vbytes = h->abi >= 2 ? sizeof(snac_state_view) : offsetof(snac_state_view, plastic_strain_tensor);
+    memcpy(&vi, in, vbytes);
+    memcpy(&vo, out, vbytes);
+    // default: one slab per 8 MiB of stresses (the bulk of the transfers),
+    // 1 to 16 slabs; smaller slabs cost more in per-slab latency than they
+    // save in pipeline fill
+    const long long stress_bytes = h->mesh.ne * NT * 6 * (long long)sizeof(double);
+    const int S = chunks ? chunks : (int)std::max(1LL, std::min(16LL, (stress_bytes + (4LL << 20)) / (8LL << 20)));
+    {
+        // every return below waits for this call's copies first: the caller
+        // may release its host buffers once the call has returned
+        struct Drain {
+            HostStep* q;
+            cudaStream_t s;
+            ~Drain() {
+                cudaStreamSynchronize(q->in);
+                cudaStreamSynchronize(q->out);
+                cudaStreamSynchronize(s);
+            }
+        } drain{q, h->stream};
+        if ((rc = record_host_step(h, &vi, &vo, S))) return rc;
+    }
+    h->parity ^= 1;
+    h->pending = false;
+    CK(cudaStreamSynchronize(h->stream));
+    if ((rc = read_status(h))) return rc;
+    const long long nq = h->mesh.ne * NT;
+    if (out->plastic_strain && !h->eps_p) memset(out->plastic_strain, 0, nq * sizeof(double));
+    if (out->viscosity && !h->visc) memset(out->viscosity, 0, nq * sizeof(double));
+    if (vo.plastic_strain_tensor && !h->pst) memset(vo.plastic_strain_tensor, 0, nq * 6 * sizeof(double));
     return 0;
 }
 

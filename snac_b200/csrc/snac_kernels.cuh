@@ -1112,6 +1112,28 @@ __global__ void __launch_bounds__(128, SNAC_NODE_MINB) k_loop_nodes(Mesh m, Fiel
     k_loop_nodes_body<DTTYPE, VONLY>(m, F, cfg, blockIdx.x);
 }
 
+// Slab launches of the step with the state in host memory: the same bodies
+// over blocks [b0, b0 + gridDim.x) of the whole-mesh launch, so a slab's
+// hexes (nodes) get exactly the arithmetic of the whole-mesh kernels.
+template <int PLUGIN, bool ONE>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_calc_stresses_slab(Mesh m, Fields F, Config cfg,
+                                                                                        int b0) {
+    k_calc_stresses_body<PLUGIN, ONE>(m, F, cfg, b0 + (int)blockIdx.x);
+}
+
+// UpdateElement.c:54-269 with this step's dt and the minimum length scale
+// of the new geometry (the unfused element update)
+template <int PLUGIN>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_ELEM_MINB) k_update_elements_slab(Mesh m, Fields F, Config cfg,
+                                                                                          int b0) {
+    k_update_elements_body<PLUGIN>(m, F, cfg, 0, b0 + (int)blockIdx.x);
+}
+
+template <int DTTYPE, bool VONLY>
+__global__ void __launch_bounds__(128, SNAC_NODE_MINB) k_loop_nodes_slab(Mesh m, Fields F, Config cfg, int b0) {
+    k_loop_nodes_body<DTTYPE, VONLY>(m, F, cfg, b0 + (int)blockIdx.x);
+}
+
 // ======================================================================================
 // Snac_EP_LoopElementsEnergy: Snac_HeatFlux (temperature/HeatFlux.c:60-200) and
 // SnacTemperature_HeatFluxBC (temperature/VariableConditions.c:280-413)
@@ -1278,6 +1300,19 @@ __global__ void __launch_bounds__(128) k_heat_nodes(Mesh m, Fields F, Config cfg
         F.sc->current_time += F.sc->dt;
     }
     k_heat_nodes_body(m, F, cfg, blockIdx.x);
+}
+
+// Slab launches of the energy hooks for the step with the state in host
+// memory (see k_calc_stresses_slab): blocks [b0, b0 + gridDim.x) of the
+// whole-mesh launch; the step was counted by its first kernel.
+template <bool ONE>
+__global__ void __launch_bounds__(ELEM_WARPS * 32, SNAC_HEAT_MINB) k_heat_flux_slab(Mesh m, Fields F, Config cfg,
+                                                                                   int b0) {
+    k_heat_flux_body<ONE>(m, F, cfg, b0 + (int)blockIdx.x);
+}
+
+__global__ void __launch_bounds__(128) k_heat_nodes_slab(Mesh m, Fields F, Config cfg, int b0) {
+    k_heat_nodes_body(m, F, cfg, b0 + (int)blockIdx.x);
 }
 
 // ======================================================================================
@@ -1591,6 +1626,50 @@ __global__ void k_unpack_nodes(double4* __restrict__ dst, const double* __restri
         d[2] = src[n * 3 + 2];
     } else {
         d[3] = src[n];
+    }
+}
+
+// The node state of nodes [0, nn) between the host's rows (3 doubles of
+// coordinates, 3 of velocity, 1 of temperature per node) and the device's
+// double4 rows (pos: x, y, z, T; vel: vx, vy, vz and the previous T, which
+// stays); pos and vel always hold nn rows, a null host row (c, t, v) is
+// skipped.
+__global__ void k_unpack_node_state(double4* __restrict__ pos, const double* __restrict__ c,
+                                    const double* __restrict__ t, double4* __restrict__ vel,
+                                    const double* __restrict__ v, long long nn) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    double* p = reinterpret_cast<double*>(pos + n);
+    if (c) {
+        p[0] = c[n * 3 + 0];
+        p[1] = c[n * 3 + 1];
+        p[2] = c[n * 3 + 2];
+    }
+    if (t) p[3] = t[n];
+    if (v) {
+        double* w = reinterpret_cast<double*>(vel + n);
+        w[0] = v[n * 3 + 0];
+        w[1] = v[n * 3 + 1];
+        w[2] = v[n * 3 + 2];
+    }
+}
+
+__global__ void k_pack_node_state(const double4* __restrict__ pos, double* __restrict__ c, double* __restrict__ t,
+                                  const double4* __restrict__ vel, double* __restrict__ v, long long nn) {
+    long long n = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= nn) return;
+    const double4 x = pos[n];
+    if (c) {
+        c[n * 3 + 0] = x.x;
+        c[n * 3 + 1] = x.y;
+        c[n * 3 + 2] = x.z;
+    }
+    if (t) t[n] = x.w;
+    if (v) {
+        const double4 w = vel[n];
+        v[n * 3 + 0] = w.x;
+        v[n * 3 + 1] = w.y;
+        v[n * 3 + 2] = w.z;
     }
 }
 
