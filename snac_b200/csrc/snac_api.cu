@@ -60,8 +60,7 @@ constexpr int STEP_HOST_MAX_CHUNKS = 64;
 struct HostStep {
     cudaStream_t in = nullptr, out = nullptr;
     cudaEvent_t start = nullptr, done = nullptr, nodes_in = nullptr;
-    cudaEvent_t ev_in[STEP_HOST_MAX_CHUNKS] = {}, ev_nodes[STEP_HOST_MAX_CHUNKS] = {},
-                ev_elems[STEP_HOST_MAX_CHUNKS] = {};
+    cudaEvent_t ev_in[STEP_HOST_MAX_CHUNKS] = {}, ev_elems[STEP_HOST_MAX_CHUNKS] = {};
     double* stage_in = nullptr;   // [nn][3] coordinates, [nn][3] velocities, [nn] temperatures, as the host holds them
     double* stage_out = nullptr;  // the same rows
     bool ready = false;
@@ -698,7 +697,6 @@ int ensure_host_step(snac_gpu* h) {
     CK(cudaEventCreateWithFlags(&q->nodes_in, cudaEventDisableTiming));
     for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++) {
         CK(cudaEventCreateWithFlags(&q->ev_in[c], cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&q->ev_nodes[c], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&q->ev_elems[c], cudaEventDisableTiming));
     }
     int rc;
@@ -1121,7 +1119,7 @@ void snac_gpu_destroy(snac_gpu* h) {
         for (cudaEvent_t e : {q->start, q->done, q->nodes_in})
             if (e) cudaEventDestroy(e);
         for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++)
-            for (cudaEvent_t e : {q->ev_in[c], q->ev_nodes[c], q->ev_elems[c]})
+            for (cudaEvent_t e : {q->ev_in[c], q->ev_elems[c]})
                 if (e) cudaEventDestroy(e);
         for (cudaStream_t st : {q->in, q->out})
             if (st) cudaStreamDestroy(st);
@@ -1437,24 +1435,27 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
             case UPDATE: rc = op_update_elements_slab(h, F1, b0, b1); break;
         }
         if (rc) return rc;
-        if (stages[s] == MOMENTUM_NODES && N[i + 1] > N[i] && (out->coord || out->velocity || out->temperature)) {
+        const bool node_rows = out->coord || out->velocity || out->temperature;
+        if (stages[s] == MOMENTUM_NODES && N[i + 1] > N[i] && node_rows) {
             const long long a = N[i], n = N[i + 1] - N[i];
             k_pack_node_state<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
                 h->pos[p ^ 1] + a, out->coord ? so + a * 3 : nullptr, out->temperature ? so + nn * 6 + a : nullptr,
                 h->vel + a, out->velocity ? so + nn * 3 + a * 3 : nullptr, n);
             h->launches++;
             if ((rc = launch_check_named(h, "k_pack_node_state"))) return rc;
-            CK(cudaEventRecord(q->ev_nodes[i], h->stream));
-            CK(cudaStreamWaitEvent(q->out, q->ev_nodes[i], 0));
-            if (out->coord) CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
-            if (out->velocity)
-                CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
-            if (out->temperature)
-                CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
         }
         if (stages[s] == UPDATE) {
+            // node slab i is packed by now (this element slab needed it moved):
+            // one wait for both downloads of the slab
             CK(cudaEventRecord(q->ev_elems[i], h->stream));
             CK(cudaStreamWaitEvent(q->out, q->ev_elems[i], 0));
+            const long long a = N[i], n = N[i + 1] - N[i];
+            if (n > 0 && out->coord)
+                CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (n > 0 && out->velocity)
+                CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (n > 0 && out->temperature)
+                CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
             if ((rc = elems_out(E[i], E[i + 1]))) return rc;
         }
         done[s]++;
