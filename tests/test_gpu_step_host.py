@@ -153,3 +153,28 @@ def test_refuses_bad_arguments():
                 ctx.step_host(s, s, chunks=chunks)
             assert e.value.code == -1
         ctx.step_host(s, s, chunks=64)
+
+
+def test_non_finite_state_is_reported_as_by_the_three_calls():
+    """a NaN uploaded with the state: the status snac_gpu_upload +
+    snac_gpu_step + snac_gpu_download give, with an element or node index
+    (the first of the tets or nodes that see it to report; the fault is
+    made on the host, nothing faults on the GPU)"""
+    make, _ = S.CASES["plastic"]
+    errs = []
+    for host_step in (False, True):
+        with SnacContext(make()) as ctx:
+            ctx.time_step_zero()
+            ctx.step(3)
+            s = ctx.state()
+            s.velocity[17, 2] = np.nan
+            with pytest.raises(SnacError) as e:
+                if host_step:
+                    ctx.step_host(s, s, chunks=4)
+                else:
+                    ctx.set_state(s, MOVED)
+                    ctx.step(1)
+                    ctx.state(s)
+            errs.append((e.value.code, e.value.index))
+    assert errs[0][0] == errs[1][0] == -4  # ENAN
+    assert errs[0][1] >= 0 and errs[1][1] >= 0
