@@ -266,7 +266,7 @@ int  snac_gpu_download(snac_gpu* h, const snac_state_view* v);
  * owns the Snac context's arrays between steps, the per-step transfers
  * around _Snac_Context_Solve (Context.c:1063-1099) and Sync (:1208-1268).
  *   - The transfers overlap the kernels and each other: the mesh is cut
- *     along k into `chunks` slabs (at most 64; 0: one per 8 MiB of tet
+ *     along k into `chunks` slabs (at most 64; 0: one per 6 MiB of tet
  *     stresses, 1 to 16); each slab's kernels
  *     start when its upload has arrived, and its download starts when its
  *     last kernel is done.  The overlap needs page-locked host arrays

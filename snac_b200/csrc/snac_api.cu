@@ -59,7 +59,7 @@ struct OutputState {
 constexpr int STEP_HOST_MAX_CHUNKS = 64;
 struct HostStep {
     cudaStream_t in = nullptr, out = nullptr;
-    cudaEvent_t start = nullptr, done = nullptr, nodes_in = nullptr;
+    cudaEvent_t start = nullptr, done = nullptr, nodes_in = nullptr, nodes_rest = nullptr;
     cudaEvent_t ev_in[STEP_HOST_MAX_CHUNKS] = {}, ev_elems[STEP_HOST_MAX_CHUNKS] = {};
     double* stage_in = nullptr;   // [nn][3] coordinates, [nn][3] velocities, [nn] temperatures, as the host holds them
     double* stage_out = nullptr;  // the same rows
@@ -695,6 +695,7 @@ int ensure_host_step(snac_gpu* h) {
     CK(cudaEventCreateWithFlags(&q->start, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&q->done, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&q->nodes_in, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&q->nodes_rest, cudaEventDisableTiming));
     for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++) {
         CK(cudaEventCreateWithFlags(&q->ev_in[c], cudaEventDisableTiming));
         CK(cudaEventCreateWithFlags(&q->ev_elems[c], cudaEventDisableTiming));
@@ -1116,7 +1117,7 @@ void snac_gpu_destroy(snac_gpu* h) {
     if (HostStep* q = h->hs) {
         for (cudaStream_t st : {q->in, q->out})
             if (st) cudaStreamSynchronize(st);
-        for (cudaEvent_t e : {q->start, q->done, q->nodes_in})
+        for (cudaEvent_t e : {q->start, q->done, q->nodes_in, q->nodes_rest})
             if (e) cudaEventDestroy(e);
         for (int c = 0; c < STEP_HOST_MAX_CHUNKS; c++)
             for (cudaEvent_t e : {q->ev_in[c], q->ev_elems[c]})
@@ -1385,29 +1386,52 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
     CK(cudaEventRecord(q->start, h->stream));  // after anything the handle ran before
     CK(cudaStreamWaitEvent(q->in, q->start, 0));
     CK(cudaStreamWaitEvent(q->out, q->start, 0));
-    // uploads, all queued at once: the node state first, then the hex state slab by slab
-    if (in->coord) CK(cudaMemcpyAsync(si, in->coord, nn * 3 * D, cudaMemcpyHostToDevice, q->in));
-    if (in->velocity) CK(cudaMemcpyAsync(si + nn * 3, in->velocity, nn * 3 * D, cudaMemcpyHostToDevice, q->in));
-    if (in->temperature) CK(cudaMemcpyAsync(si + nn * 6, in->temperature, nn * D, cudaMemcpyHostToDevice, q->in));
+    // Uploads, all queued at once: the node rows the first two hex slabs
+    // read, those two slabs, the other node rows, then the other hex slabs;
+    // the first downloads wait for the second slab, so it arrives early.
+    const bool node_in = in->coord || in->velocity || in->temperature;
+    const long long n_head = std::max(need_nodes(0), need_nodes(std::min(1, S - 1)));
+    auto nodes_up = [&](long long a, long long b) -> int {
+        if (b <= a) return 0;
+        if (in->coord) CK(cudaMemcpyAsync(si + a * 3, in->coord + a * 3, (b - a) * 3 * D, cudaMemcpyHostToDevice, q->in));
+        if (in->velocity)
+            CK(cudaMemcpyAsync(si + (nn + a) * 3, in->velocity + a * 3, (b - a) * 3 * D, cudaMemcpyHostToDevice, q->in));
+        if (in->temperature)
+            CK(cudaMemcpyAsync(si + nn * 6 + a, in->temperature + a, (b - a) * D, cudaMemcpyHostToDevice, q->in));
+        return 0;
+    };
+    auto nodes_unpack = [&](long long a, long long b) -> int {
+        if (b <= a || !node_in) return 0;
+        k_unpack_node_state<<<(unsigned)((b - a + 255) / 256), 256, 0, h->stream>>>(
+            h->pos[p] + a, in->coord ? si + a * 3 : nullptr, in->temperature ? si + nn * 6 + a : nullptr, h->vel + a,
+            in->velocity ? si + (nn + a) * 3 : nullptr, b - a);
+        h->launches++;
+        return launch_check_named(h, "k_unpack_node_state");
+    };
+    if ((rc = nodes_up(0, n_head))) return rc;
     CK(cudaEventRecord(q->nodes_in, q->in));
     for (int c = 0; c < S; c++) {
+        if (c == std::min(2, S)) {
+            if ((rc = nodes_up(n_head, nn))) return rc;
+            CK(cudaEventRecord(q->nodes_rest, q->in));
+        }
         if ((rc = elems_in(E[c], E[c + 1]))) return rc;
         CK(cudaEventRecord(q->ev_in[c], q->in));
     }
+    if (S <= 2) {  // (then the first two slabs read every node: nothing left)
+        if ((rc = nodes_up(n_head, nn))) return rc;
+        CK(cudaEventRecord(q->nodes_rest, q->in));
+    }
     if ((rc = op_begin(h))) return rc;  // timeStep++, currentTime += dt
     CK(cudaStreamWaitEvent(h->stream, q->nodes_in, 0));
-    if (in->coord || in->velocity || in->temperature) {
-        k_unpack_node_state<<<(unsigned)((nn + 255) / 256), 256, 0, h->stream>>>(
-            h->pos[p], in->coord ? si : nullptr, in->temperature ? si + nn * 6 : nullptr, h->vel,
-            in->velocity ? si + nn * 3 : nullptr, nn);
-        h->launches++;
-        if ((rc = launch_check_named(h, "k_unpack_node_state"))) return rc;
-    }
+    if ((rc = nodes_unpack(0, n_head))) return rc;
+    bool rest_unpacked = false;  // nodes [n_head, nn): before hex slab 2 of the first stage
 
     // Kernels in dependency order: the deepest stage that can take its next
     // slab goes first, so that a slab's last stage (and its download) is not
     // queued behind hex slabs still waiting for their uploads.
     std::vector<int> done(ns, 0);
+    long long nodes_back = 0;  // node rows [0, nodes_back) queued for download
     auto ready = [&](int s) -> bool {
         const int i = done[s];
         if (i >= S) return false;
@@ -1423,6 +1447,11 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
         if (s == 0) {
             if (i >= S)  // every bound above is met once all hex slabs of stage 0 are done
                 return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_step_host: slab schedule stalled");
+            if (!rest_unpacked && (i >= 2 || need_nodes(i) > n_head)) {
+                CK(cudaStreamWaitEvent(h->stream, q->nodes_rest, 0));
+                if ((rc = nodes_unpack(n_head, nn))) return rc;
+                rest_unpacked = true;
+            }
             CK(cudaStreamWaitEvent(h->stream, q->ev_in[i], 0));
         }
         const int b0 = (int)(E[i] / ELEM_PER_BLOCK), b1 = (int)((E[i + 1] + ELEM_PER_BLOCK - 1) / ELEM_PER_BLOCK);
@@ -1445,17 +1474,22 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
             if ((rc = launch_check_named(h, "k_pack_node_state"))) return rc;
         }
         if (stages[s] == UPDATE) {
-            // node slab i is packed by now (this element slab needed it moved):
-            // one wait for both downloads of the slab
+            // node slabs <= i are packed by now (this element slab needed them
+            // moved): one wait for the slab's downloads; the node rows go back
+            // every fourth slab, in fewer and larger copies
             CK(cudaEventRecord(q->ev_elems[i], h->stream));
             CK(cudaStreamWaitEvent(q->out, q->ev_elems[i], 0));
-            const long long a = N[i], n = N[i + 1] - N[i];
-            if (n > 0 && out->coord)
-                CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
-            if (n > 0 && out->velocity)
-                CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
-            if (n > 0 && out->temperature)
-                CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
+            if ((i + 1) % 4 == 0 || i == S - 1) {
+                const long long a = nodes_back, n = N[i + 1] - nodes_back;
+                if (n > 0 && out->coord)
+                    CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+                if (n > 0 && out->velocity)
+                    CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost,
+                                       q->out));
+                if (n > 0 && out->temperature)
+                    CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
+                nodes_back = N[i + 1];
+            }
             if ((rc = elems_out(E[i], E[i + 1]))) return rc;
         }
         done[s]++;
@@ -1494,11 +1528,11 @@ int snac_gpu_step_host(snac_gpu* h, const snac_state_view* in, const snac_state_
     const size_t vbytes = h->abi >= 2 ? sizeof(snac_state_view) : offsetof(snac_state_view, plastic_strain_tensor);
     memcpy(&vi, in, vbytes);
     memcpy(&vo, out, vbytes);
-    // default: one slab per 8 MiB of stresses (the bulk of the transfers),
+    // default: one slab per 6 MiB of stresses (the bulk of the transfers),
     // 1 to 16 slabs; smaller slabs cost more in per-slab latency than they
     // save in pipeline fill
     const long long stress_bytes = h->mesh.ne * NT * 6 * (long long)sizeof(double);
-    const int S = chunks ? chunks : (int)std::max(1LL, std::min(16LL, (stress_bytes + (4LL << 20)) / (8LL << 20)));
+    const int S = chunks ? chunks : (int)std::max(1LL, std::min(16LL, (stress_bytes + (3LL << 20)) / (6LL << 20)));
     {
         // every return below waits for this call's copies first: the caller
         // may release its host buffers once the call has returned
