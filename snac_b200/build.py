@@ -30,6 +30,7 @@ def nvcc() -> str:
 
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")) + glob.glob(os.path.join(CSRC, "*.cuh")) +
+                  glob.glob(os.path.join(CSRC, "*.h")) +
                   [os.path.join(ROOT, "include", "snac_gpu.h")])
 
 

@@ -23,6 +23,7 @@
 #include "snac_adjoint.cuh"
 #include "snac_batch.cuh"
 #include "snac_output.cuh"
+#include "snac_slab_plan.h"
 #include "snac_kernels.cuh"
 
 using namespace snac;
@@ -1323,26 +1324,14 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
     HostStep* q = h->hs;
     const Mesh& m = h->mesh;
     const long long ne = m.ne, nn = m.nn;
-    const long long LE = (long long)m.nx * m.ny, P = (long long)m.nnx * m.nny;  // hexes per k-layer, nodes per k-plane
-    std::vector<long long> E(S + 1), N(S + 1);
-    for (int c = 0; c < S; c++) {
-        E[c] = ne * c / S / ELEM_PER_BLOCK * ELEM_PER_BLOCK;
-        N[c] = std::min(nn, E[c] / LE * P) / 128 * 128;
-    }
-    E[S] = ne;
-    N[S] = nn;
-    // nodes [0, need_nodes(c)) hold every node element slab c touches
-    auto need_nodes = [&](int c) -> long long {
-        if (E[c + 1] <= E[c]) return 0;
-        const long long k = (E[c + 1] - 1) / LE;
-        return std::min(nn, (k + 2) * P);
-    };
-    // hexes [0, need_elems(d)) hold every hex incident to node slab d
-    auto need_elems = [&](int d) -> long long {
-        if (N[d + 1] <= N[d]) return 0;
-        const long long k = (N[d + 1] - 1) / P;
-        return std::min(ne, (k + 1) * LE);
-    };
+    // the stages of the step, alternating hex and node stages (snac_slab_plan.h)
+    enum Stage { HEAT_FLUX, HEAT_NODES, STRESS, MOMENTUM_NODES, UPDATE };
+    std::vector<Stage> stages;
+    if (h->temperature) stages = {HEAT_FLUX, HEAT_NODES};
+    stages.insert(stages.end(), {STRESS, MOMENTUM_NODES, UPDATE});
+    const SlabPlan plan = plan_slabs(m.nx, m.ny, m.nz, S, (int)stages.size(), ELEM_PER_BLOCK, 128);
+    const std::vector<long long>& E = plan.E;
+    const std::vector<long long>& N = plan.N;
     const bool want_pst = out->plastic_strain_tensor != nullptr;
     const bool give_pst = in->plastic_strain_tensor != nullptr;
     const size_t D = sizeof(double);
@@ -1371,13 +1360,6 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
         return 0;
     };
 
-    // the stages of the step; even entries are hex stages, odd ones node stages
-    enum Stage { HEAT_FLUX, HEAT_NODES, STRESS, MOMENTUM_NODES, UPDATE };
-    std::vector<Stage> stages;
-    if (h->temperature) stages = {HEAT_FLUX, HEAT_NODES};
-    stages.insert(stages.end(), {STRESS, MOMENTUM_NODES, UPDATE});
-    const int ns = (int)stages.size();
-
     const int p = h->parity;
     const Fields F0 = fields_at(h, p);      // this step: coordinates in pos[p], moved into pos[p ^ 1]
     const Fields F1 = fields_at(h, p ^ 1);  // the element update reads the moved coordinates
@@ -1390,7 +1372,7 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
     // read, those two slabs, the other node rows, then the other hex slabs;
     // the first downloads wait for the second slab, so it arrives early.
     const bool node_in = in->coord || in->velocity || in->temperature;
-    const long long n_head = std::max(need_nodes(0), need_nodes(std::min(1, S - 1)));
+    const long long n_head = plan.n_head;
     auto nodes_up = [&](long long a, long long b) -> int {
         if (b <= a) return 0;
         if (in->coord) CK(cudaMemcpyAsync(si + a * 3, in->coord + a * 3, (b - a) * 3 * D, cudaMemcpyHostToDevice, q->in));
@@ -1425,35 +1407,31 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
     if ((rc = op_begin(h))) return rc;  // timeStep++, currentTime += dt
     CK(cudaStreamWaitEvent(h->stream, q->nodes_in, 0));
     if ((rc = nodes_unpack(0, n_head))) return rc;
-    bool rest_unpacked = false;  // nodes [n_head, nn): before hex slab 2 of the first stage
 
-    // Kernels in dependency order: the deepest stage that can take its next
-    // slab goes first, so that a slab's last stage (and its download) is not
-    // queued behind hex slabs still waiting for their uploads.
-    std::vector<int> done(ns, 0);
-    long long nodes_back = 0;  // node rows [0, nodes_back) queued for download
-    auto ready = [&](int s) -> bool {
-        const int i = done[s];
-        if (i >= S) return false;
-        if (s == 0) return true;
-        if (stages[s] == HEAT_NODES || stages[s] == MOMENTUM_NODES) return E[done[s - 1]] >= need_elems(i);
-        return N[done[s - 1]] >= need_nodes(i) && done[s - 2] > i;
-    };
-    int total = 0;
-    while (total < ns * S) {
-        int s = ns - 1;
-        while (s > 0 && !ready(s)) s--;
-        const int i = done[s];
-        if (s == 0) {
-            if (i >= S)  // every bound above is met once all hex slabs of stage 0 are done
-                return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_step_host: slab schedule stalled");
-            if (!rest_unpacked && (i >= 2 || need_nodes(i) > n_head)) {
-                CK(cudaStreamWaitEvent(h->stream, q->nodes_rest, 0));
-                if ((rc = nodes_unpack(n_head, nn))) return rc;
-                rest_unpacked = true;
-            }
-            CK(cudaStreamWaitEvent(h->stream, q->ev_in[i], 0));
+    const bool node_rows = out->coord || out->velocity || out->temperature;
+    int kernels = 0;
+    for (const SlabOp& o : plan.ops) {
+        if (o.kind == SlabOp::UNPACK_REST) {  // nodes [n_head, nn), before hex slab 2 of the first stage
+            CK(cudaStreamWaitEvent(h->stream, q->nodes_rest, 0));
+            if ((rc = nodes_unpack(n_head, nn))) return rc;
+            continue;
         }
+        if (o.kind == SlabOp::NODES_BACK) {  // node slabs up to this one are packed
+            const long long a = o.a, n = o.b - o.a;
+            if (n > 0 && out->coord)
+                CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (n > 0 && out->velocity)
+                CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
+            if (n > 0 && out->temperature)
+                CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
+            continue;
+        }
+        if (o.kind == SlabOp::HEXES_BACK) {
+            if ((rc = elems_out(E[o.slab], E[o.slab + 1]))) return rc;
+            continue;
+        }
+        const int s = o.stage, i = o.slab;
+        if (s == 0) CK(cudaStreamWaitEvent(h->stream, q->ev_in[i], 0));
         const int b0 = (int)(E[i] / ELEM_PER_BLOCK), b1 = (int)((E[i + 1] + ELEM_PER_BLOCK - 1) / ELEM_PER_BLOCK);
         const int n0 = (int)(N[i] / 128), n1 = (int)((N[i + 1] + 127) / 128);
         switch (stages[s]) {
@@ -1464,7 +1442,7 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
             case UPDATE: rc = op_update_elements_slab(h, F1, b0, b1); break;
         }
         if (rc) return rc;
-        const bool node_rows = out->coord || out->velocity || out->temperature;
+        kernels++;
         if (stages[s] == MOMENTUM_NODES && N[i + 1] > N[i] && node_rows) {
             const long long a = N[i], n = N[i + 1] - N[i];
             k_pack_node_state<<<(unsigned)((n + 255) / 256), 256, 0, h->stream>>>(
@@ -1473,28 +1451,15 @@ static int record_host_step(snac_gpu* h, const snac_state_view* in, const snac_s
             h->launches++;
             if ((rc = launch_check_named(h, "k_pack_node_state"))) return rc;
         }
-        if (stages[s] == UPDATE) {
-            // node slabs <= i are packed by now (this element slab needed them
-            // moved): one wait for the slab's downloads; the node rows go back
-            // every fourth slab, in fewer and larger copies
+        if (stages[s] == UPDATE) {  // the slab's downloads (the plan's next ops) wait for this
             CK(cudaEventRecord(q->ev_elems[i], h->stream));
             CK(cudaStreamWaitEvent(q->out, q->ev_elems[i], 0));
-            if ((i + 1) % 4 == 0 || i == S - 1) {
-                const long long a = nodes_back, n = N[i + 1] - nodes_back;
-                if (n > 0 && out->coord)
-                    CK(cudaMemcpyAsync(out->coord + a * 3, so + a * 3, n * 3 * D, cudaMemcpyDeviceToHost, q->out));
-                if (n > 0 && out->velocity)
-                    CK(cudaMemcpyAsync(out->velocity + a * 3, so + nn * 3 + a * 3, n * 3 * D, cudaMemcpyDeviceToHost,
-                                       q->out));
-                if (n > 0 && out->temperature)
-                    CK(cudaMemcpyAsync(out->temperature + a, so + nn * 6 + a, n * D, cudaMemcpyDeviceToHost, q->out));
-                nodes_back = N[i + 1];
-            }
-            if ((rc = elems_out(E[i], E[i + 1]))) return rc;
         }
-        done[s]++;
-        total++;
     }
+    if (kernels != (int)stages.size() * S)  // the plan always finishes every slab of every stage
+        return set_err(h, SNAC_GPU_ESTATE, -1, "snac_gpu_step_host: slab plan has %d of %d slab kernels", kernels,
+                       (int)stages.size() * S);
+    (void)ne;
     if ((rc = op_sync(h))) return rc;  // Sync: the next dt from this step's reductions
     CK(cudaEventRecord(q->done, q->out));
     CK(cudaStreamWaitEvent(h->stream, q->done, 0));
